@@ -1,0 +1,241 @@
+/*
+ * pfem2.h -- C ABI of the B200-native PFEM2 time-step library (libpfem2b.so).
+ *
+ * The reference (andreyypopov/pfem2) exposes its hot path as the member
+ * functions of `class pfem2Solver` (TurekBenchmarkCuda/pfem2particle.h:126-233,
+ * TurekBenchmark/pfem2particle.h:139-243, tubePoiseuille3D/pfem2particle.h).
+ * Every function below replaces one of those members (cited beside it); the
+ * header-only C++ class in pfem2_solver.hpp forwards the reference's member
+ * names to these entry points so a case driver keeps its run() order:
+ *
+ *     correct_particles_velocities -> move_particles ->
+ *     distribute_particle_velocities_to_grid -> fem_step -> calculate_loads
+ *
+ * Conventions
+ *  - Plain pointers and sizes only; every entry point returns pfem2_status.
+ *  - A context owns all device memory and one CUDA stream. Calls on one
+ *    context are not re-entrant; distinct contexts are independent.
+ *  - A context holds a BATCH of independent flow instances (a single case is
+ *    a batch of one). Cells, vertices (= Q1 DoFs) and particles of all
+ *    instances are concatenated; per-instance arrays passed to or returned by
+ *    the API use the instance's own local numbering.
+ *  - Vertex order inside a cell and face numbering follow deal.II
+ *    (lexicographic): vertex v has reference coordinate bit d of v along axis
+ *    d; face f lies on axis f/2 at side f%2.
+ *  - Host buffers passed in are copied; nothing is retained after return.
+ */
+#ifndef PFEM2_H
+#define PFEM2_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define PFEM2_ABI_VERSION 1
+
+typedef enum {
+  PFEM2_OK = 0,
+  PFEM2_INVALID_ARG = 1,
+  PFEM2_CUDA_ERROR = 2,
+  PFEM2_NOT_CONVERGED = 3,      /* a Krylov solve hit max_iter (reference only prints this) */
+  PFEM2_TIMEOUT = 4,            /* a bounded device-side wait gave up */
+  PFEM2_PARTICLE_OVERFLOW = 5,  /* particle / per-cell / far-mover capacity exceeded */
+  PFEM2_NO_DEVICE = 6,
+  PFEM2_BAD_STATE = 7,          /* call order violated (e.g. step before setup) */
+  PFEM2_MESH_ERROR = 8          /* inverted cell, bad connectivity */
+} pfem2_status;
+
+typedef enum {
+  PFEM2_PREC_FP64 = 0,   /* everything FP64 ("plain" path) */
+  PFEM2_PREC_MIXED = 1   /* FP32 particles/assembly/inner Krylov, FP64 refinement, dots, loads */
+} pfem2_precision;
+
+typedef enum {
+  PFEM2_FIELD_VX = 0, PFEM2_FIELD_VY = 1, PFEM2_FIELD_VZ = 2, PFEM2_FIELD_P = 3,
+  PFEM2_FIELD_OLD_VX = 4, PFEM2_FIELD_OLD_VY = 5, PFEM2_FIELD_OLD_VZ = 6, PFEM2_FIELD_OLD_P = 7,
+  PFEM2_FIELD_PRED_VX = 8, PFEM2_FIELD_PRED_VY = 9, PFEM2_FIELD_PRED_VZ = 10,
+  PFEM2_FIELD_NODE_WEIGHT = 11,  /* sum of shape values from the last projection */
+  PFEM2_N_FIELDS = 12
+} pfem2_field;
+
+typedef enum {
+  PFEM2_BC_CONSTANT = 0,   /* value */
+  PFEM2_BC_PARABOLA = 1    /* value * 4 (s-a)(b-s)/(b-a)^2, s = vertex coordinate `axis` */
+} pfem2_bc_kind;
+
+typedef enum {
+  PFEM2_SOLVER_CG = 0,
+  PFEM2_SOLVER_BICGSTAB = 1
+} pfem2_solver_kind;
+
+/* One Dirichlet condition: all vertices of boundary faces with `boundary_id`.
+ * Conditions of a field are applied in array order; a vertex on several
+ * listed boundaries takes the last one (as successive
+ * MatrixTools::apply_boundary_values calls do, cylinder2D/cylinder2D.cc:459-466). */
+typedef struct {
+  int32_t boundary_id;
+  int32_t kind;      /* pfem2_bc_kind */
+  int32_t axis;      /* PARABOLA only */
+  int32_t pad_;
+  double value;
+  double a, b;       /* PARABOLA only */
+} pfem2_dirichlet;
+
+#define PFEM2_MAX_BC 8
+
+/* Physics, boundary conditions and solver controls of one instance.
+ * Field index for bc arrays: 0..dim-1 = velocity components, 3 = pressure. */
+typedef struct {
+  double mu, rho, dt;
+  int32_t n_dirichlet[4];
+  pfem2_dirichlet dirichlet[4][PFEM2_MAX_BC];
+  /* Boundary ids (bit mask) that are inflow/outflow sections: the prediction
+   * stress face terms and the pressure flux face term are integrated there
+   * (cylinder2D/cylinder2D.cc:432-447,582-597; tubePoiseuille3D/tube.cc:253-273,496-510). */
+  uint32_t open_boundary_mask;
+  /* Neumann pressure term G * n_x integrated over open faces
+   * (tubePoiseuille3D/tube.cc:509 uses G = -10); 0 in 2D cases. */
+  double open_boundary_pressure_flux;
+  /* Boundary ids whose vertices are set to zero velocity right after the
+   * particle->grid projection (wallsAndBodyDoFs, TurekBenchmarkCuda/pfem2particle.cu:866-869). */
+  uint32_t zero_after_projection_mask;
+  /* Loads (calculate_loads): obstacle patch id, reference diameter and mean
+   * velocity for the coefficients, and the two probe vertices of the
+   * pressure difference (-1 = unused), TurekBenchmark/pfem2particle.cpp:920-970. */
+  int32_t load_patch_id;
+  int32_t probe_a, probe_b;
+  int32_t outer_corrections;      /* nOuterCorr (cylinder2D/cylinder2D.cc:395) */
+  double load_diam, load_umean;
+  /* Krylov controls: SolverControl(max_iter, tol) with the absolute
+   * unpreconditioned residual norm as in deal.II (cylinder2D/cylinder2D.cc:736-779). */
+  double vel_tol, p_tol;
+  int32_t max_iter;
+  int32_t vel_solver;             /* pfem2_solver_kind */
+  int32_t p_solver;               /* pfem2_solver_kind */
+  int32_t reassemble_every_step;  /* 1: rebuild matrices each step like the reference */
+} pfem2_case;
+
+/* A mesh of one instance (host arrays, copied by pfem2_add_instance). */
+typedef struct {
+  int32_t n_vertices;
+  int32_t n_cells;
+  const double* vertices;          /* [n_vertices][dim] */
+  const int32_t* cells;            /* [n_cells][2^dim], deal.II vertex order */
+  const int32_t* face_boundary_id; /* [n_cells][2*dim], -1 = interior face */
+} pfem2_mesh_view;
+
+typedef struct {
+  int32_t dim;                     /* 2 or 3 */
+  int32_t precision;               /* pfem2_precision */
+  int32_t device;                  /* CUDA ordinal */
+  int32_t movement_steps;          /* PARTICLES_MOVEMENT_STEPS (pfem2particle.h:4) */
+  int32_t max_particles_per_cell_part; /* MAX_PARTICLES_PER_CELL_PART (pfem2particle.h:5) */
+  int32_t particles_per_cell_max;  /* per-cell capacity of the rebin pass (0 = auto) */
+  double particle_capacity_factor; /* particle storage = factor * seeded count (0 = 2.0) */
+  int32_t far_mover_capacity;      /* particles that leave the 1-ring of their cell in one step (0 = auto) */
+  int32_t use_graph;               /* capture pfem2_step as a CUDA graph */
+} pfem2_config;
+
+typedef struct pfem2_ctx pfem2_ctx;
+
+typedef struct {
+  int32_t n_particles;
+  int32_t n_deleted_last_move;     /* left the mesh or found in no patch cell */
+  int32_t n_removed_last_check;    /* over MAX_PARTICLES_PER_CELL_PART */
+  int32_t n_reseeded_last_check;   /* one per empty sub-cell */
+  int32_t n_far_movers_last_move;
+  int32_t iters[7];                /* last Krylov iterations: pred x,y,z, p, corr x,y,z */
+  double residual[7];              /* last absolute residual norms */
+  int32_t refinements_p;           /* FP64 refinement sweeps of the last pressure solve */
+  int32_t pad_;
+} pfem2_stats;
+
+/* ---- lifecycle (pfem2Solver::pfem2Solver, build_grid, setup_system) ---- */
+pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out);
+pfem2_status pfem2_destroy(pfem2_ctx* ctx);
+/* Adds one instance (build_grid; cases' GridIn / GridGenerator calls). */
+pfem2_status pfem2_add_instance(pfem2_ctx* ctx, const pfem2_mesh_view* mesh,
+                                const pfem2_case* cs, int32_t* instance_out);
+/* Builds DoF maps, sparsity, boundary tables, vertex->cell maps and assembles
+ * the step-invariant matrices (setup_system, TurekBenchmarkCuda/TurekBenchmark.cc:282-403;
+ * pfem2ParticleHandler::initialize_maps, TurekBenchmark/pfem2particle.cpp:215-219). */
+pfem2_status pfem2_setup(pfem2_ctx* ctx);
+
+/* ---- the pfem2Solver member functions ---- */
+/* seed_particles (TurekBenchmark/pfem2particle.cpp:701-721,774-790): q[d]
+ * particles per axis per cell at sub-cell centres, plus a uniform jitter of
+ * +-jitter (reference units) from a counter-based SplitMix64 stream keyed by
+ * (seed, global particle ordinal, axis). instance < 0: all instances. */
+pfem2_status pfem2_seed(pfem2_ctx* ctx, int32_t instance, const uint32_t q[3],
+                        uint64_t seed, double jitter);
+/* correct_particles_velocities (TurekBenchmark/pfem2particle.cpp:792-811). */
+pfem2_status pfem2_correct(pfem2_ctx* ctx);
+/* move_particles incl. point location and check_cell_for_empty_parts
+ * (TurekBenchmark/pfem2particle.cpp:813-856, :276-507, :723-772). */
+pfem2_status pfem2_move(pfem2_ctx* ctx);
+/* move_particles without the final check (advection + location + re-sort). */
+pfem2_status pfem2_advect(pfem2_ctx* ctx);
+/* check_cells_for_empty_parts alone (TurekBenchmarkCuda/pfem2particle.cu:360-416). */
+pfem2_status pfem2_check_empty(pfem2_ctx* ctx);
+/* distribute_particle_velocities_to_grid (TurekBenchmark/pfem2particle.cpp:858-918). */
+pfem2_status pfem2_project(pfem2_ctx* ctx);
+/* fem_step / assemble_system: prediction, pressure Poisson, correction
+ * (cylinder2D/cylinder2D.cc:385-731, tubePoiseuille3D/tube.cc:165-715). */
+pfem2_status pfem2_fem_step(pfem2_ctx* ctx);
+/* calculate_loads (TurekBenchmark/pfem2particle.cpp:920-970): out[5] =
+ * {Cx_nu, Cx_p, Cy_nu, Cy_p, p(probe_a) - p(probe_b)} (2D). In 3D out =
+ * {Fx_p, Fy_p, Fz_p, 0, p(probe_a) - p(probe_b)} (tubePoiseuille3D/pfem2particle.cpp:693-737). */
+pfem2_status pfem2_loads(pfem2_ctx* ctx, int32_t instance, int32_t patch_id, double out[5]);
+/* One whole time step: correct -> move -> project -> fem_step, with fused
+ * kernels (and a CUDA graph if cfg.use_graph); advances time by dt. */
+pfem2_status pfem2_step(pfem2_ctx* ctx);
+/* Same as pfem2_step, then loads of every instance into out[5*n_instances]
+ * and a host read of all instances' nodal fields listed in `fields`
+ * (n_fields entries) into `host_fields` (instance-major, field, vertex). */
+pfem2_status pfem2_step_and_read(pfem2_ctx* ctx, double* loads_out,
+                                 const int32_t* fields, int32_t n_fields,
+                                 double* host_fields);
+
+/* ---- state access (public data members of pfem2Solver) ---- */
+pfem2_status pfem2_get_field(pfem2_ctx* ctx, int32_t instance, int32_t field, double* host);
+pfem2_status pfem2_set_field(pfem2_ctx* ctx, int32_t instance, int32_t field, const double* host);
+pfem2_status pfem2_particle_count(pfem2_ctx* ctx, int32_t instance, int32_t* n);
+/* Particles of an instance in storage order (sorted by cell): local cell id,
+ * reference coordinates [n][dim] and velocity [n][dim]. */
+pfem2_status pfem2_get_particles(pfem2_ctx* ctx, int32_t instance, int32_t* cell,
+                                 double* xi, double* u);
+/* Replaces the particles of ALL instances: n particles with instance-local
+ * cells given per instance by counts[n_instances] (instance-major order);
+ * the library sorts them (stable) by cell. */
+pfem2_status pfem2_set_particles(pfem2_ctx* ctx, const int32_t* counts, const int32_t* cell,
+                                 const double* xi, const double* u);
+pfem2_status pfem2_get_stats(pfem2_ctx* ctx, pfem2_stats* out);
+pfem2_status pfem2_get_time(pfem2_ctx* ctx, double* time, int32_t* timestep_number);
+pfem2_status pfem2_synchronize(pfem2_ctx* ctx);
+/* Device kernel launches issued by this context so far (for accounting). */
+pfem2_status pfem2_launch_count(pfem2_ctx* ctx, int64_t* n);
+/* Device time (ms) of named stages accumulated since the last reset: stage
+ * 0 correct+move, 1 rebin/check, 2 project, 3 assembly, 4 solves, 5 loads. */
+pfem2_status pfem2_stage_times(pfem2_ctx* ctx, double* ms6, int32_t reset);
+/* Enable per-stage CUDA-event timing (off by default; costs a few events/step). */
+pfem2_status pfem2_enable_stage_timing(pfem2_ctx* ctx, int32_t on);
+/* The CUDA stream (cudaStream_t) all work of the context is issued on. */
+pfem2_status pfem2_get_stream(pfem2_ctx* ctx, void** stream);
+const char* pfem2_last_error(void);
+int32_t pfem2_abi_version(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFEM2_H */

@@ -1,0 +1,859 @@
+// capi.cu -- the C ABI of libpfem2b (include/pfem2.h): context, mesh
+// preprocessing (setup_system / initialize_maps), the pfem2Solver member
+// functions and the whole-step path with its CUDA graphs.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "ctx.h"
+
+namespace pfem2 {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& s) { g_last_error = s; }
+
+pfem2_status cuda_status(cudaError_t e, const char* where) {
+  set_error(std::string(where) + ": " + cudaGetErrorString(e));
+  return PFEM2_CUDA_ERROR;
+}
+
+template <typename T>
+static pfem2_status dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * n);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
+  e = cudaMemset(*p, 0, sizeof(T) * n);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMemset");
+  return PFEM2_OK;
+}
+
+template <typename T>
+static pfem2_status upload(T** p, const std::vector<T>& v) {
+  pfem2_status s = dalloc(p, v.size());
+  if (s != PFEM2_OK) return s;
+  if (!v.empty()) PFEM2_CUDA(cudaMemcpy(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return PFEM2_OK;
+}
+
+#define PFEM2_TRY(x)                         \
+  do {                                       \
+    pfem2_status s_ = (x);                   \
+    if (s_ != PFEM2_OK) return s_;           \
+  } while (0)
+
+// host pinned mirror of the step counters (deferred error reporting)
+struct StepMirror {
+  int counters[CNT_N];
+  int np[2];
+};
+
+static double bc_value(const pfem2_dirichlet& d, const double* x) {
+  if (d.kind == PFEM2_BC_PARABOLA) {
+    const double s = x[d.axis], L = d.b - d.a;
+    return d.value * 4.0 * (s - d.a) * (d.b - s) / (L * L);
+  }
+  return d.value;
+}
+
+// --------------------------------------------------------------- setup
+static pfem2_status do_setup(Ctx& c) {
+  const int dim = c.dim, NV = 1 << dim, NF = 2 * dim;
+  // offsets
+  int v = 0, cc = 0;
+  for (auto& in : c.inst) {
+    in.v_off = v;
+    in.nv_pad = (in.nv + kSlice - 1) / kSlice * kSlice;
+    in.c_off = cc;
+    v += in.nv_pad;
+    cc += in.nc;
+  }
+  c.nv = v;
+  c.nc = cc;
+  const int nv = c.nv, nc = c.nc;
+  std::vector<double> X((size_t)nv * dim, 0.0);
+  std::vector<int> cv((size_t)nc * NV), cinst(nc), vinst(nv, 0);
+  std::vector<signed char> fb((size_t)nc * NF);
+  for (size_t i = 0; i < c.inst.size(); ++i) {
+    auto& in = c.inst[i];
+    std::copy(in.X.begin(), in.X.end(), X.begin() + (size_t)in.v_off * dim);
+    for (int k = 0; k < in.nv_pad; ++k) vinst[in.v_off + k] = (int)i;
+    for (int k = 0; k < in.nc; ++k) {
+      cinst[in.c_off + k] = (int)i;
+      for (int b = 0; b < NV; ++b) {
+        int g = in.cells[(size_t)k * NV + b];
+        if (g < 0 || g >= in.nv) {
+          set_error("mesh: vertex index out of range");
+          return PFEM2_MESH_ERROR;
+        }
+        cv[(size_t)(in.c_off + k) * NV + b] = g + in.v_off;
+      }
+      for (int f = 0; f < NF; ++f) {
+        int b = in.fb[(size_t)k * NF + f];
+        if (b < -1 || b > 127) {
+          set_error("mesh: boundary id must be in [-1, 127]");
+          return PFEM2_MESH_ERROR;
+        }
+        fb[(size_t)(in.c_off + k) * NF + f] = (signed char)b;
+      }
+    }
+  }
+  // vertex -> cells (ascending cell index), local index, centre directions
+  std::vector<int> v2c_ptr(nv + 1, 0);
+  for (int k = 0; k < nc * NV; ++k) v2c_ptr[cv[k] + 1]++;
+  for (int i = 0; i < nv; ++i) v2c_ptr[i + 1] += v2c_ptr[i];
+  c.ninc = v2c_ptr[nv];
+  std::vector<int> v2c_cell(c.ninc), fill(nv, 0);
+  std::vector<unsigned char> v2c_loc(c.ninc);
+  for (int ce = 0; ce < nc; ++ce)
+    for (int b = 0; b < NV; ++b) {
+      int g = cv[(size_t)ce * NV + b];
+      int k = v2c_ptr[g] + fill[g]++;
+      v2c_cell[k] = ce;
+      v2c_loc[k] = (unsigned char)b;
+    }
+  for (int i = 0; i < nv; ++i)
+    if (v2c_ptr[i + 1] - v2c_ptr[i] > kMaxPatch) {
+      set_error("mesh: more than 32 cells around a vertex");
+      return PFEM2_MESH_ERROR;
+    }
+  std::vector<double> v2c_dir((size_t)c.ninc * dim);
+  std::vector<float> v2c_dirf((size_t)c.ninc * dim);
+  for (int i = 0; i < nv; ++i)
+    for (int k = v2c_ptr[i]; k < v2c_ptr[i + 1]; ++k) {
+      int ce = v2c_cell[k];
+      double ctr[3] = {0, 0, 0}, nn = 0;
+      for (int b = 0; b < NV; ++b)
+        for (int a = 0; a < dim; ++a) ctr[a] += X[(size_t)cv[(size_t)ce * NV + b] * dim + a];
+      for (int a = 0; a < dim; ++a) {
+        ctr[a] = ctr[a] / NV - X[(size_t)i * dim + a];
+        nn += ctr[a] * ctr[a];
+      }
+      nn = std::sqrt(nn);
+      for (int a = 0; a < dim; ++a) {
+        v2c_dir[(size_t)k * dim + a] = ctr[a] / nn;
+        v2c_dirf[(size_t)k * dim + a] = (float)(ctr[a] / nn);
+      }
+    }
+  // 1-ring of each cell (cells sharing a vertex), ascending
+  std::vector<int> ring_ptr(nc + 1, 0), ring_cell;
+  ring_cell.reserve((size_t)nc * (dim == 2 ? 9 : 27));
+  std::vector<int> tmp;
+  c.ring_max = 0;
+  for (int ce = 0; ce < nc; ++ce) {
+    tmp.clear();
+    for (int b = 0; b < NV; ++b) {
+      int g = cv[(size_t)ce * NV + b];
+      for (int k = v2c_ptr[g]; k < v2c_ptr[g + 1]; ++k) tmp.push_back(v2c_cell[k]);
+    }
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    ring_cell.insert(ring_cell.end(), tmp.begin(), tmp.end());
+    ring_ptr[ce + 1] = (int)ring_cell.size();
+    c.ring_max = std::max(c.ring_max, (int)tmp.size());
+  }
+  // sparsity: per row diagonal first, then ascending columns; SELL-32
+  std::vector<std::vector<int>> rows(nv);
+  int maxlen = 1;
+  for (int i = 0; i < nv; ++i) {
+    tmp.clear();
+    for (int k = v2c_ptr[i]; k < v2c_ptr[i + 1]; ++k)
+      for (int b = 0; b < NV; ++b) tmp.push_back(cv[(size_t)v2c_cell[k] * NV + b]);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    auto& r = rows[i];
+    r.push_back(i);
+    for (int j : tmp)
+      if (j != i) r.push_back(j);
+    maxlen = std::max(maxlen, (int)r.size());
+  }
+  c.nslices = nv / kSlice;
+  std::vector<int> sl_ptr(c.nslices + 1, 0), sl_len(c.nslices);
+  for (int s = 0; s < c.nslices; ++s) {
+    int L = 1;
+    for (int l = 0; l < kSlice; ++l) L = std::max(L, (int)rows[s * kSlice + l].size());
+    sl_len[s] = L;
+    sl_ptr[s + 1] = sl_ptr[s] + L * kSlice;
+  }
+  c.nell = sl_ptr[c.nslices];
+  c.h_sl_ptr = sl_ptr;
+  std::vector<int> sl_col(c.nell);
+  std::vector<std::map<int, int>> where(0);
+  c.nnz = 0;
+  for (int s = 0; s < c.nslices; ++s)
+    for (int l = 0; l < kSlice; ++l) {
+      int row = s * kSlice + l;
+      auto& r = rows[row];
+      c.nnz += (int)r.size();
+      for (int j = 0; j < sl_len[s]; ++j) sl_col[sl_ptr[s] + j * kSlice + l] = j < (int)r.size() ? r[j] : row;
+    }
+  std::vector<int> inc_slot((size_t)c.ninc * NV);
+  for (int i = 0; i < nv; ++i) {
+    auto& r = rows[i];
+    int s = i / kSlice, l = i % kSlice;
+    for (int k = v2c_ptr[i]; k < v2c_ptr[i + 1]; ++k)
+      for (int b = 0; b < NV; ++b) {
+        int col = cv[(size_t)v2c_cell[k] * NV + b];
+        int j = (int)(std::find(r.begin(), r.end(), col) - r.begin());
+        inc_slot[(size_t)k * NV + b] = sl_ptr[s] + j * kSlice + l;
+      }
+  }
+  // Dirichlet tables and zero-after-projection flags
+  std::vector<unsigned char> isd[4];
+  std::vector<double> dval[4];
+  for (int f = 0; f < 4; ++f) {
+    isd[f].assign(nv, 0);
+    dval[f].assign(nv, 0.0);
+  }
+  std::vector<unsigned char> zflag(nv, 0);
+  for (auto& in : c.inst) {
+    for (int k = in.nv; k < in.nv_pad; ++k)
+      for (int f = 0; f < 4; ++f) isd[f][in.v_off + k] = 1;
+    for (int f = 0; f < 4; ++f) {
+      if (f >= dim && f < 3) continue;
+      for (int k = 0; k < in.cs.n_dirichlet[f]; ++k) {
+        const pfem2_dirichlet& d = in.cs.dirichlet[f][k];
+        for (int ce = in.c_off; ce < in.c_off + in.nc; ++ce)
+          for (int fc = 0; fc < NF; ++fc) {
+            if (fb[(size_t)ce * NF + fc] != d.boundary_id) continue;
+            for (int b = 0; b < NV; ++b) {
+              if (((b >> (fc / 2)) & 1) != fc % 2) continue;
+              int g = cv[(size_t)ce * NV + b];
+              isd[f][g] = 1;
+              dval[f][g] = bc_value(d, &X[(size_t)g * dim]);
+            }
+          }
+      }
+    }
+    if (in.cs.zero_after_projection_mask)
+      for (int ce = in.c_off; ce < in.c_off + in.nc; ++ce)
+        for (int fc = 0; fc < NF; ++fc) {
+          int b = fb[(size_t)ce * NF + fc];
+          if (b < 0 || b > 31 || !((in.cs.zero_after_projection_mask >> b) & 1u)) continue;
+          for (int vb = 0; vb < NV; ++vb)
+            if (((vb >> (fc / 2)) & 1) == fc % 2) zflag[cv[(size_t)ce * NV + vb]] = 1;
+        }
+  }
+  // instance table
+  c.h_inst.resize(c.inst.size());
+  std::vector<double> tols(2 * c.inst.size());
+  std::vector<int> maxit(c.inst.size());
+  for (size_t i = 0; i < c.inst.size(); ++i) {
+    auto& in = c.inst[i];
+    DevInst& d = c.h_inst[i];
+    d.mu = in.cs.mu; d.rho = in.cs.rho; d.dt = in.cs.dt; d.open_flux = in.cs.open_boundary_pressure_flux;
+    d.open_mask = in.cs.open_boundary_mask;
+    d.q[0] = d.q[1] = d.q[2] = 1;
+    d.max_per_part = c.cfg.max_particles_per_cell_part;
+    d.v_off = in.v_off; d.nv_pad = in.nv_pad; d.c_off = in.c_off; d.nc = in.nc;
+    tols[i] = in.cs.vel_tol;
+    tols[c.inst.size() + i] = in.cs.p_tol;
+    maxit[i] = in.cs.max_iter > 0 ? in.cs.max_iter : 10000;
+  }
+  // uploads
+  PFEM2_TRY(upload(&c.X, X));
+  PFEM2_TRY(upload(&c.cv, cv));
+  PFEM2_TRY(upload(&c.fb, fb));
+  PFEM2_TRY(upload(&c.cell_inst, cinst));
+  PFEM2_TRY(upload(&c.vert_inst, vinst));
+  PFEM2_TRY(upload(&c.v2c_ptr, v2c_ptr));
+  PFEM2_TRY(upload(&c.v2c_cell, v2c_cell));
+  PFEM2_TRY(upload(&c.v2c_loc, v2c_loc));
+  PFEM2_TRY(upload(&c.v2c_dir, v2c_dir));
+  if (c.mixed) {
+    float* p = nullptr;
+    PFEM2_TRY(upload(&p, v2c_dirf));
+    c.v2c_dir_r = p;
+  } else {
+    c.v2c_dir_r = c.v2c_dir;
+  }
+  PFEM2_TRY(upload(&c.ring_ptr, ring_ptr));
+  PFEM2_TRY(upload(&c.ring_cell, ring_cell));
+  PFEM2_TRY(upload(&c.sl_ptr, sl_ptr));
+  PFEM2_TRY(upload(&c.sl_len, sl_len));
+  PFEM2_TRY(upload(&c.sl_col, sl_col));
+  PFEM2_TRY(upload(&c.inc_slot, inc_slot));
+  for (int f = 0; f < 4; ++f) {
+    PFEM2_TRY(upload(&c.isdir[f], isd[f]));
+    PFEM2_TRY(upload(&c.dirval[f], dval[f]));
+    PFEM2_TRY(dalloc(&c.shift[f], nv));
+  }
+  PFEM2_TRY(upload(&c.zero_flag, zflag));
+  PFEM2_TRY(upload(&c.d_inst, c.h_inst));
+  {
+    double* t = nullptr;
+    PFEM2_TRY(upload(&t, tols));
+    c.sys_scalars = t;
+    PFEM2_TRY(upload(&c.d_sysinfo, maxit));
+  }
+  for (int k = 0; k < kNumSys; ++k) {
+    PFEM2_TRY(dalloc(&c.A64[k], c.nell));
+    PFEM2_TRY(dalloc(&c.A32[k], c.nell));
+    PFEM2_TRY(dalloc(&c.dinv64[k], nv));
+    PFEM2_TRY(dalloc(&c.dinv32[k], nv));
+  }
+  for (int f = 0; f < PFEM2_N_FIELDS; ++f) PFEM2_TRY(dalloc(&c.F[f], nv));
+  for (int k = 0; k < 3; ++k) {
+    PFEM2_TRY(dalloc(&c.corr[k], nv));
+    PFEM2_TRY(dalloc(&c.rhs[k], nv));
+  }
+  const size_t rs = c.mixed ? 4 : 8;
+  {
+    void* p;
+    PFEM2_CUDA(cudaMalloc(&p, rs * 3 * nv));
+    PFEM2_CUDA(cudaMemset(p, 0, rs * 3 * nv));
+    c.Vr = p;
+    PFEM2_CUDA(cudaMalloc(&p, rs * 3 * nv));
+    PFEM2_CUDA(cudaMemset(p, 0, rs * 3 * nv));
+    c.dVr = p;
+    PFEM2_CUDA(cudaMalloc(&p, rs * (size_t)nc * NV * (dim + 1)));
+    PFEM2_CUDA(cudaMemset(p, 0, rs * (size_t)nc * NV * (dim + 1)));
+    c.partial = p;
+  }
+  for (int b = 0; b < 2; ++b) PFEM2_TRY(dalloc(&c.cell_start[b], nc + 1));
+  PFEM2_TRY(dalloc(&c.cell_count, nc));
+  PFEM2_TRY(dalloc(&c.d_np, 2));
+  PFEM2_TRY(dalloc(&c.d_counters, CNT_N));
+  c.far_cap = c.cfg.far_mover_capacity > 0 ? std::min(c.cfg.far_mover_capacity, 4096) : 4096;
+  PFEM2_TRY(dalloc(&c.far_keys, c.far_cap));
+  c.scan_tmp_n = (nc + 4095) / 4096 + 1;
+  PFEM2_TRY(dalloc(&c.scan_tmp, c.scan_tmp_n));
+  PFEM2_TRY(dalloc(&c.barrier, 2));
+  PFEM2_TRY(dalloc(&c.d_err, 1));
+  c.list_cap = c.cfg.particles_per_cell_max > 0 ? c.cfg.particles_per_cell_max : (dim == 2 ? 512 : 1024);
+  PFEM2_TRY(krylov_setup(c));
+  PFEM2_TRY(assemble_matrices(c));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  PFEM2_CUDA(cudaGetLastError());
+  c.setup_done = true;
+  return PFEM2_OK;
+}
+
+static pfem2_status alloc_particles(Ctx& c, size_t seeded) {
+  double f = c.cfg.particle_capacity_factor > 0 ? c.cfg.particle_capacity_factor : 2.0;
+  size_t cap = (size_t)std::ceil(seeded * f) + 1024;
+  if (cap > (size_t)2000000000) cap = 2000000000;
+  if ((int)cap <= c.pcap) return PFEM2_OK;
+  const size_t rs = c.mixed ? 4 : 8;
+  for (int b = 0; b < 2; ++b) {
+    if (c.pcell[b]) cudaFree(c.pcell[b]);
+    if (c.pxi[b]) cudaFree(c.pxi[b]);
+    if (c.pu[b]) cudaFree(c.pu[b]);
+    PFEM2_CUDA(cudaMalloc(&c.pcell[b], sizeof(int) * cap));
+    PFEM2_CUDA(cudaMalloc(&c.pxi[b], rs * c.dim * cap));
+    PFEM2_CUDA(cudaMalloc(&c.pu[b], rs * c.dim * cap));
+  }
+  if (c.newcell) cudaFree(c.newcell);
+  PFEM2_CUDA(cudaMalloc(&c.newcell, sizeof(int) * cap));
+  c.pcap = (int)cap;
+  c.graph_valid = false;
+  return PFEM2_OK;
+}
+
+// deferred checks of the counters of the last particle pass
+static pfem2_status check_counters(Ctx& c, bool sync) {
+  if (sync) PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  int cnt[CNT_N];
+  int np[2];
+  PFEM2_CUDA(cudaMemcpy(cnt, c.d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+  PFEM2_CUDA(cudaMemcpy(np, c.d_np, sizeof(np), cudaMemcpyDeviceToHost));
+  c.stats.n_particles = np[c.cur];
+  c.stats.n_deleted_last_move = cnt[CNT_DELETED];
+  c.stats.n_removed_last_check = cnt[CNT_REMOVED];
+  c.stats.n_reseeded_last_check = cnt[CNT_RESEEDED];
+  c.stats.n_far_movers_last_move = cnt[CNT_FAR];
+  if (cnt[CNT_LIST_OVERFLOW]) {
+    set_error("rebin: more incoming particles than the per-cell capacity (particles_per_cell_max)");
+    return PFEM2_PARTICLE_OVERFLOW;
+  }
+  if (cnt[CNT_FAR_OVERFLOW]) {
+    set_error("advect: more far movers than far_mover_capacity");
+    return PFEM2_PARTICLE_OVERFLOW;
+  }
+  if (np[c.cur] > c.pcap) {
+    set_error("rebin: particle storage capacity exceeded");
+    return PFEM2_PARTICLE_OVERFLOW;
+  }
+  return PFEM2_OK;
+}
+
+// ------------------------------------------------------------ FEM step
+static pfem2_status fem_step_launch(Ctx& c) {
+  for (int d = 0; d < c.dim; ++d)
+    PFEM2_CUDA(cudaMemcpyAsync(c.F[PFEM2_FIELD_OLD_VX + d], c.F[PFEM2_FIELD_VX + d], sizeof(double) * c.nv,
+                               cudaMemcpyDeviceToDevice, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(c.F[PFEM2_FIELD_OLD_P], c.F[PFEM2_FIELD_P], sizeof(double) * c.nv,
+                             cudaMemcpyDeviceToDevice, c.stream));
+  if (c.inst[0].cs.reassemble_every_step) PFEM2_TRY(assemble_matrices(c));
+  int nouter = std::max(1, c.inst[0].cs.outer_corrections);
+  for (int oc = 0; oc < nouter; ++oc) {
+    PFEM2_TRY(launch_rhs_prediction(c));
+    PFEM2_TRY(krylov_solve(c, 0));
+    PFEM2_TRY(launch_rhs_pressure(c));
+    PFEM2_TRY(krylov_solve(c, 1));
+    PFEM2_TRY(launch_rhs_correction(c));
+    PFEM2_TRY(krylov_solve(c, 2));
+    PFEM2_TRY(launch_finish_fem(c));
+  }
+  return PFEM2_OK;
+}
+
+static pfem2_status step_launch(Ctx& c) {
+  PFEM2_TRY(launch_advect(c, true));
+  PFEM2_TRY(launch_rebin(c, true, true, true));
+  PFEM2_TRY(launch_project(c, true));
+  PFEM2_TRY(fem_step_launch(c));
+  return PFEM2_OK;
+}
+
+}  // namespace pfem2
+
+using namespace pfem2;
+
+struct pfem2_ctx {
+  Ctx c;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_launches[2] = {0, 0};
+  bool graph_failed = false;
+};
+
+#define CTX_CHECK(ctx)                              \
+  do {                                              \
+    if (!(ctx)) {                                   \
+      set_error("null context");                    \
+      return PFEM2_INVALID_ARG;                     \
+    }                                               \
+  } while (0)
+#define SETUP_CHECK(ctx)                            \
+  do {                                              \
+    CTX_CHECK(ctx);                                 \
+    if (!(ctx)->c.setup_done) {                     \
+      set_error("pfem2_setup has not run");         \
+      return PFEM2_BAD_STATE;                       \
+    }                                               \
+  } while (0)
+#define SEED_CHECK(ctx)                             \
+  do {                                              \
+    SETUP_CHECK(ctx);                               \
+    if (!(ctx)->c.seeded) {                         \
+      set_error("no particles (seed first)");       \
+      return PFEM2_BAD_STATE;                       \
+    }                                               \
+  } while (0)
+
+extern "C" {
+
+const char* pfem2_last_error(void) { return g_last_error.c_str(); }
+int32_t pfem2_abi_version(void) { return PFEM2_ABI_VERSION; }
+
+pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
+  if (!cfg || !out) { set_error("null argument"); return PFEM2_INVALID_ARG; }
+  if (cfg->dim != 2 && cfg->dim != 3) { set_error("dim must be 2 or 3"); return PFEM2_INVALID_ARG; }
+  if (cfg->movement_steps < 1 || cfg->max_particles_per_cell_part < 1) {
+    set_error("movement_steps and max_particles_per_cell_part must be >= 1");
+    return PFEM2_INVALID_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return PFEM2_NO_DEVICE;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) { set_error("bad device ordinal"); return PFEM2_INVALID_ARG; }
+  pfem2_ctx* x = new (std::nothrow) pfem2_ctx();
+  if (!x) { set_error("out of host memory"); return PFEM2_INVALID_ARG; }
+  Ctx& c = x->c;
+  c.cfg = *cfg;
+  c.dim = cfg->dim;
+  c.mixed = cfg->precision == PFEM2_PREC_MIXED;
+  c.device = cfg->device;
+  PFEM2_CUDA(cudaSetDevice(c.device));
+  cudaDeviceProp prop;
+  PFEM2_CUDA(cudaGetDeviceProperties(&prop, c.device));
+  c.num_sms = prop.multiProcessorCount;
+  PFEM2_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 8; ++k) PFEM2_CUDA(cudaEventCreate(&c.ev[k]));
+  *out = x;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_destroy(pfem2_ctx* x) {
+  if (!x) return PFEM2_OK;
+  Ctx& c = x->c;
+  cudaSetDevice(c.device);
+  cudaStreamSynchronize(c.stream);
+  for (int k = 0; k < 2; ++k)
+    if (x->graph[k]) cudaGraphExecDestroy(x->graph[k]);
+  // device memory is released with the context's allocations; free the big ones
+  void* ptrs[] = {c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
+                  c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.d_inst,
+                  c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.cell_count, c.d_np, c.d_counters,
+                  c.far_keys, c.scan_tmp, c.barrier, c.d_err, c.newcell};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (c.mixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);
+  for (int k = 0; k < kNumSys; ++k) {
+    cudaFree(c.A64[k]); cudaFree(c.A32[k]); cudaFree(c.dinv64[k]); cudaFree(c.dinv32[k]);
+  }
+  for (int f = 0; f < 4; ++f) { cudaFree(c.isdir[f]); cudaFree(c.dirval[f]); cudaFree(c.shift[f]); }
+  for (int f = 0; f < PFEM2_N_FIELDS; ++f) cudaFree(c.F[f]);
+  for (int k = 0; k < 3; ++k) { cudaFree(c.corr[k]); cudaFree(c.rhs[k]); }
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(c.pcell[b]); cudaFree(c.pxi[b]); cudaFree(c.pu[b]); cudaFree(c.cell_start[b]);
+  }
+  for (int k = 0; k < 8; ++k) cudaEventDestroy(c.ev[k]);
+  cudaStreamDestroy(c.stream);
+  delete x;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_add_instance(pfem2_ctx* x, const pfem2_mesh_view* mesh, const pfem2_case* cs, int32_t* inst_out) {
+  CTX_CHECK(x);
+  Ctx& c = x->c;
+  if (c.setup_done) { set_error("instances must be added before pfem2_setup"); return PFEM2_BAD_STATE; }
+  if (!mesh || !cs || !mesh->vertices || !mesh->cells || !mesh->face_boundary_id || mesh->n_cells <= 0 ||
+      mesh->n_vertices <= 0) {
+    set_error("invalid mesh view");
+    return PFEM2_INVALID_ARG;
+  }
+  if (!(cs->dt > 0) || !(cs->rho > 0) || !(cs->mu >= 0)) { set_error("invalid case parameters"); return PFEM2_INVALID_ARG; }
+  for (int f = 0; f < 4; ++f)
+    if (cs->n_dirichlet[f] < 0 || cs->n_dirichlet[f] > PFEM2_MAX_BC) { set_error("bad n_dirichlet"); return PFEM2_INVALID_ARG; }
+  const int dim = c.dim, NV = 1 << dim, NF = 2 * dim;
+  HostInst in;
+  in.nv = mesh->n_vertices;
+  in.nc = mesh->n_cells;
+  in.cs = *cs;
+  in.X.assign(mesh->vertices, mesh->vertices + (size_t)in.nv * dim);
+  in.cells.assign(mesh->cells, mesh->cells + (size_t)in.nc * NV);
+  in.fb.assign(mesh->face_boundary_id, mesh->face_boundary_id + (size_t)in.nc * NF);
+  c.inst.push_back(std::move(in));
+  if (inst_out) *inst_out = (int32_t)c.inst.size() - 1;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_setup(pfem2_ctx* x) {
+  CTX_CHECK(x);
+  Ctx& c = x->c;
+  if (c.setup_done) { set_error("pfem2_setup called twice"); return PFEM2_BAD_STATE; }
+  if (c.inst.empty()) { set_error("no instances"); return PFEM2_BAD_STATE; }
+  PFEM2_CUDA(cudaSetDevice(c.device));
+  return do_setup(c);
+}
+
+pfem2_status pfem2_seed(pfem2_ctx* x, int32_t instance, const uint32_t q[3], uint64_t seed, double jitter) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (!q || q[0] < 1 || q[1] < 1 || (c.dim == 3 && q[2] < 1)) { set_error("bad q"); return PFEM2_INVALID_ARG; }
+  int nb = (q[0] + 1) * (q[1] + 1) * (c.dim == 3 ? q[2] + 1 : 1);
+  if (nb > 256) { set_error("q too large: at most 256 sub-cell buckets per cell"); return PFEM2_INVALID_ARG; }
+  if (instance >= (int)c.inst.size()) { set_error("bad instance"); return PFEM2_INVALID_ARG; }
+  PFEM2_CUDA(cudaSetDevice(c.device));
+  for (size_t i = 0; i < c.inst.size(); ++i)
+    if (instance < 0 || (int)i == instance) {
+      for (int d = 0; d < 3; ++d) c.inst[i].q[d] = (d < c.dim) ? q[d] : 1;
+      for (int d = 0; d < 3; ++d) c.h_inst[i].q[d] = (int)c.inst[i].q[d];
+    }
+  for (auto& in : c.inst)
+    if (in.q[0] == 0) { set_error("every instance needs particles: seed all instances"); return PFEM2_BAD_STATE; }
+  PFEM2_CUDA(cudaMemcpy(c.d_inst, c.h_inst.data(), sizeof(DevInst) * c.h_inst.size(), cudaMemcpyHostToDevice));
+  size_t total = 0;
+  for (auto& in : c.inst) total += (size_t)in.nc * in.q[0] * in.q[1] * in.q[2];
+  PFEM2_TRY(alloc_particles(c, total));
+  c.cur = 0;
+  PFEM2_TRY(launch_seed(c, instance, q, seed, jitter));
+  c.seeded = true;
+  c.stats.n_particles = (int)total;
+  x->graph_failed = false;
+  for (int k = 0; k < 2; ++k)
+    if (x->graph[k]) { cudaGraphExecDestroy(x->graph[k]); x->graph[k] = nullptr; }
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_correct(pfem2_ctx* x) {
+  SEED_CHECK(x);
+  PFEM2_TRY(launch_correct(x->c));
+  PFEM2_CUDA(cudaStreamSynchronize(x->c.stream));
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_advect(pfem2_ctx* x) {
+  SEED_CHECK(x);
+  PFEM2_TRY(launch_advect(x->c, false));
+  PFEM2_TRY(launch_rebin(x->c, false, false, true));
+  PFEM2_CUDA(cudaGetLastError());
+  return check_counters(x->c, true);
+}
+
+pfem2_status pfem2_check_empty(pfem2_ctx* x) {
+  SEED_CHECK(x);
+  PFEM2_CUDA(cudaMemsetAsync(x->c.d_counters, 0, sizeof(int) * CNT_N, x->c.stream));
+  PFEM2_TRY(launch_rebin(x->c, true, false, false));
+  PFEM2_CUDA(cudaGetLastError());
+  return check_counters(x->c, true);
+}
+
+pfem2_status pfem2_move(pfem2_ctx* x) {
+  SEED_CHECK(x);
+  PFEM2_TRY(launch_advect(x->c, false));
+  PFEM2_TRY(launch_rebin(x->c, true, false, true));
+  PFEM2_CUDA(cudaGetLastError());
+  return check_counters(x->c, true);
+}
+
+pfem2_status pfem2_project(pfem2_ctx* x) {
+  SEED_CHECK(x);
+  PFEM2_TRY(launch_project(x->c, false));
+  PFEM2_CUDA(cudaStreamSynchronize(x->c.stream));
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_fem_step(pfem2_ctx* x) {
+  SETUP_CHECK(x);
+  PFEM2_TRY(fem_step_launch(x->c));
+  PFEM2_CUDA(cudaStreamSynchronize(x->c.stream));
+  PFEM2_CUDA(cudaGetLastError());
+  return krylov_read_stats(x->c);
+}
+
+static pfem2_status run_step(pfem2_ctx* x) {
+  Ctx& c = x->c;
+  const int par = c.cur;
+  if (c.cfg.use_graph && !x->graph_failed) {
+    if (!x->graph[par]) {
+      cudaGraph_t g;
+      cudaError_t e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return cuda_status(e, "cudaStreamBeginCapture");
+      long long l0 = c.launches;
+      pfem2_status s = step_launch(c);
+      e = cudaStreamEndCapture(c.stream, &g);
+      c.cur = par;  // capture does not execute: restore the parity
+      x->graph_launches[par] = c.launches - l0;
+      c.launches = l0;
+      if (s != PFEM2_OK || e != cudaSuccess) {
+        cudaGetLastError();
+        x->graph_failed = true;
+        if (g) cudaGraphDestroy(g);
+      } else {
+        e = cudaGraphInstantiate(&x->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          x->graph[par] = nullptr;
+          x->graph_failed = true;
+        }
+      }
+    }
+    if (x->graph[par]) {
+      PFEM2_CUDA(cudaGraphLaunch(x->graph[par], c.stream));
+      c.cur = 1 - par;
+      c.launches += x->graph_launches[par];
+      return PFEM2_OK;
+    }
+  }
+  return step_launch(c);
+}
+
+pfem2_status pfem2_step(pfem2_ctx* x) {
+  SEED_CHECK(x);
+  Ctx& c = x->c;
+  PFEM2_TRY(run_step(x));
+  c.time += c.inst[0].cs.dt;
+  c.timestep += 1;
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_step_and_read(pfem2_ctx* x, double* loads_out, const int32_t* fields, int32_t n_fields,
+                                 double* host_fields) {
+  SEED_CHECK(x);
+  Ctx& c = x->c;
+  PFEM2_TRY(pfem2_step(x));
+  const int ni = (int)c.inst.size();
+  if (loads_out) {
+    double* d;
+    PFEM2_CUDA(cudaMallocAsync(&d, sizeof(double) * 5 * ni, c.stream));
+    for (int i = 0; i < ni; ++i) PFEM2_TRY(launch_loads(c, i, c.inst[i].cs.load_patch_id, d + 5 * i));
+    PFEM2_CUDA(cudaMemcpyAsync(loads_out, d, sizeof(double) * 5 * ni, cudaMemcpyDeviceToHost, c.stream));
+    PFEM2_CUDA(cudaFreeAsync(d, c.stream));
+  }
+  if (host_fields && fields) {
+    size_t off = 0;
+    for (int i = 0; i < ni; ++i)
+      for (int f = 0; f < n_fields; ++f) {
+        if (fields[f] < 0 || fields[f] >= PFEM2_N_FIELDS) { set_error("bad field"); return PFEM2_INVALID_ARG; }
+        PFEM2_CUDA(cudaMemcpyAsync(host_fields + off, c.F[fields[f]] + c.inst[i].v_off, sizeof(double) * c.inst[i].nv,
+                                   cudaMemcpyDeviceToHost, c.stream));
+        off += c.inst[i].nv;
+      }
+  }
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  for (int i = 0; i < ni && loads_out; ++i) {
+    const pfem2_case& cs = c.inst[i].cs;
+    double* o = loads_out + 5 * i;
+    double raw[5];
+    std::memcpy(raw, o, sizeof(raw));
+    if (c.dim == 2) {
+      const double s = cs.rho * cs.load_umean * cs.load_umean * cs.load_diam;
+      for (int k = 0; k < 4; ++k) o[k] = s != 0 ? 2.0 * raw[k] / s : 0.0;
+    } else {
+      o[3] = 0.0;
+    }
+    o[4] = 0.0;
+  }
+  if (loads_out) {
+    // probe pressure difference
+    for (int i = 0; i < ni; ++i) {
+      const pfem2_case& cs = c.inst[i].cs;
+      double pa = 0, pb = 0;
+      if (cs.probe_a >= 0) PFEM2_CUDA(cudaMemcpy(&pa, c.F[PFEM2_FIELD_P] + c.inst[i].v_off + cs.probe_a, 8, cudaMemcpyDeviceToHost));
+      if (cs.probe_b >= 0) PFEM2_CUDA(cudaMemcpy(&pb, c.F[PFEM2_FIELD_P] + c.inst[i].v_off + cs.probe_b, 8, cudaMemcpyDeviceToHost));
+      loads_out[5 * i + 4] = pa - pb;
+    }
+  }
+  return check_counters(c, false);
+}
+
+pfem2_status pfem2_loads(pfem2_ctx* x, int32_t instance, int32_t patch_id, double out[5]) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (instance < 0 || instance >= (int)c.inst.size() || !out) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  double* d;
+  PFEM2_CUDA(cudaMalloc(&d, sizeof(double) * 5));
+  PFEM2_TRY(launch_loads(c, instance, patch_id, d));
+  double raw[5];
+  PFEM2_CUDA(cudaMemcpyAsync(raw, d, sizeof(raw), cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  cudaFree(d);
+  const pfem2_case& cs = c.inst[instance].cs;
+  if (c.dim == 2) {
+    const double s = cs.rho * cs.load_umean * cs.load_umean * cs.load_diam;
+    for (int k = 0; k < 4; ++k) out[k] = s != 0 ? 2.0 * raw[k] / s : 0.0;
+  } else {
+    for (int k = 0; k < 3; ++k) out[k] = raw[k];
+    out[3] = 0.0;
+  }
+  double pa = 0, pb = 0;
+  const int vo = c.inst[instance].v_off;
+  if (cs.probe_a >= 0) PFEM2_CUDA(cudaMemcpy(&pa, c.F[PFEM2_FIELD_P] + vo + cs.probe_a, 8, cudaMemcpyDeviceToHost));
+  if (cs.probe_b >= 0) PFEM2_CUDA(cudaMemcpy(&pb, c.F[PFEM2_FIELD_P] + vo + cs.probe_b, 8, cudaMemcpyDeviceToHost));
+  out[4] = (cs.probe_a >= 0 ? pa : 0.0) - (cs.probe_b >= 0 ? pb : 0.0);
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_get_field(pfem2_ctx* x, int32_t instance, int32_t field, double* host) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (instance < 0 || instance >= (int)c.inst.size() || field < 0 || field >= PFEM2_N_FIELDS || !host) {
+    set_error("bad argument");
+    return PFEM2_INVALID_ARG;
+  }
+  PFEM2_CUDA(cudaMemcpyAsync(host, c.F[field] + c.inst[instance].v_off, sizeof(double) * c.inst[instance].nv,
+                             cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_set_field(pfem2_ctx* x, int32_t instance, int32_t field, const double* host) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (instance < 0 || instance >= (int)c.inst.size() || field < 0 || field >= PFEM2_N_FIELDS || !host) {
+    set_error("bad argument");
+    return PFEM2_INVALID_ARG;
+  }
+  PFEM2_CUDA(cudaMemcpyAsync(c.F[field] + c.inst[instance].v_off, host, sizeof(double) * c.inst[instance].nv,
+                             cudaMemcpyHostToDevice, c.stream));
+  PFEM2_TRY(launch_sync_real_fields(c));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_particle_count(pfem2_ctx* x, int32_t instance, int32_t* n) {
+  SEED_CHECK(x);
+  if (!n || instance < 0 || instance >= (int)x->c.inst.size()) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  int nn = 0;
+  PFEM2_TRY(read_particles(x->c, instance, nullptr, nullptr, nullptr, &nn));
+  *n = nn;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_get_particles(pfem2_ctx* x, int32_t instance, int32_t* cell, double* xi, double* u) {
+  SEED_CHECK(x);
+  if (!cell || !xi || !u || instance < 0 || instance >= (int)x->c.inst.size()) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  int n = 0;
+  return read_particles(x->c, instance, cell, xi, u, &n);
+}
+
+pfem2_status pfem2_set_particles(pfem2_ctx* x, const int32_t* counts, const int32_t* cell, const double* xi,
+                                 const double* u) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (!counts) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  size_t total = 0;
+  for (size_t i = 0; i < c.inst.size(); ++i) total += counts[i];
+  for (auto& in : c.inst)
+    if (in.q[0] == 0) { set_error("seed (to set q) before set_particles"); return PFEM2_BAD_STATE; }
+  PFEM2_TRY(alloc_particles(c, total));
+  c.cur = 0;
+  PFEM2_TRY(launch_set_particles(c, counts, cell, xi, u));
+  c.seeded = true;
+  for (int k = 0; k < 2; ++k)
+    if (x->graph[k]) { cudaGraphExecDestroy(x->graph[k]); x->graph[k] = nullptr; }
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_get_stats(pfem2_ctx* x, pfem2_stats* out) {
+  SETUP_CHECK(x);
+  if (!out) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  pfem2_status s1 = x->c.seeded ? check_counters(x->c, true) : PFEM2_OK;
+  pfem2_status s2 = krylov_read_stats(x->c);
+  *out = x->c.stats;
+  return s1 != PFEM2_OK ? s1 : s2;
+}
+
+pfem2_status pfem2_get_time(pfem2_ctx* x, double* t, int32_t* n) {
+  CTX_CHECK(x);
+  if (t) *t = x->c.time;
+  if (n) *n = x->c.timestep;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_synchronize(pfem2_ctx* x) {
+  CTX_CHECK(x);
+  PFEM2_CUDA(cudaStreamSynchronize(x->c.stream));
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_launch_count(pfem2_ctx* x, int64_t* n) {
+  CTX_CHECK(x);
+  if (n) *n = x->c.launches;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_stage_times(pfem2_ctx* x, double* ms6, int32_t reset) {
+  CTX_CHECK(x);
+  if (ms6) std::memcpy(ms6, x->c.stage_ms, sizeof(double) * 6);
+  if (reset) std::memset(x->c.stage_ms, 0, sizeof(x->c.stage_ms));
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_enable_stage_timing(pfem2_ctx* x, int32_t on) {
+  CTX_CHECK(x);
+  x->c.timing = on != 0;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_get_stream(pfem2_ctx* x, void** stream) {
+  CTX_CHECK(x);
+  if (stream) *stream = (void*)x->c.stream;
+  return PFEM2_OK;
+}
+
+}  // extern "C"

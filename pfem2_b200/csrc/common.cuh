@@ -1,0 +1,228 @@
+// common.cuh -- device helpers shared by the PFEM2 kernels (sm_100a).
+//
+// Q1 / Q1-hex shape functions, the multilinear cell map and its Newton
+// inverse in a cell-local frame, the counter-based SplitMix64 stream, the
+// bounded grid barrier and small warp utilities.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define PFEM2_FULL_MASK 0xffffffffu
+
+namespace pfem2 {
+
+template <int DIM> struct Dims {
+  static constexpr int NV = 1 << DIM;  // vertices per cell
+  static constexpr int NF = 2 * DIM;   // faces per cell
+};
+
+// FE_Q(1) shape values in deal.II lexicographic order:
+// N_v(xi) = prod_d (bit_d(v) ? xi_d : 1 - xi_d)
+template <int DIM, typename R>
+__device__ __forceinline__ void shape_values(const R* xi, R* N) {
+#pragma unroll
+  for (int v = 0; v < Dims<DIM>::NV; ++v) {
+    R s = R(1);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s *= ((v >> d) & 1) ? xi[d] : (R(1) - xi[d]);
+    N[v] = s;
+  }
+}
+
+template <int DIM, typename R>
+__device__ __forceinline__ void shape_grads_ref(const R* xi, R* dN) {
+#pragma unroll
+  for (int v = 0; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      R s = ((v >> d) & 1) ? R(1) : R(-1);
+#pragma unroll
+      for (int e = 0; e < DIM; ++e)
+        if (e != d) s *= ((v >> e) & 1) ? xi[e] : (R(1) - xi[e]);
+      dN[v * DIM + d] = s;
+    }
+}
+
+template <int DIM, typename R>
+__device__ __forceinline__ R det_inv(const R* J, R* Ji) {
+  if constexpr (DIM == 2) {
+    R det = J[0] * J[3] - J[1] * J[2];
+    R id = R(1) / det;
+    Ji[0] = J[3] * id; Ji[1] = -J[1] * id;
+    Ji[2] = -J[2] * id; Ji[3] = J[0] * id;
+    return det;
+  } else {
+    R a = J[0], b = J[1], c = J[2], d = J[3], e = J[4], f = J[5], g = J[6], h = J[7], i = J[8];
+    R A = e * i - f * h, B = -(d * i - f * g), Cc = d * h - e * g;
+    R det = a * A + b * B + c * Cc;
+    R id = R(1) / det;
+    Ji[0] = A * id; Ji[1] = -(b * i - c * h) * id; Ji[2] = (b * f - c * e) * id;
+    Ji[3] = B * id; Ji[4] = (a * i - c * g) * id;  Ji[5] = -(a * f - c * d) * id;
+    Ji[6] = Cc * id; Ji[7] = -(a * h - b * g) * id; Ji[8] = (a * e - b * d) * id;
+    return det;
+  }
+}
+
+// Cell geometry in the cell-local frame: D[v][a] = X_v - X_0 (D[0] = 0).
+template <int DIM, typename R> struct LocalCell {
+  R D[Dims<DIM>::NV][DIM];
+};
+
+template <int DIM, typename R>
+__device__ __forceinline__ void load_local_cell(const double* __restrict__ X, const int* __restrict__ cv, int c,
+                                                LocalCell<DIM, R>& L, double* x0) {
+  constexpr int NV = Dims<DIM>::NV;
+  int g0 = __ldg(cv + (size_t)c * NV);
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) x0[a] = __ldg(X + (size_t)g0 * DIM + a);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    int g = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) L.D[v][a] = R(__ldg(X + (size_t)g * DIM + a) - x0[a]);
+  }
+}
+
+// local position F(xi) - X_0 = sum_v N_v D_v
+template <int DIM, typename R>
+__device__ __forceinline__ void local_map(const LocalCell<DIM, R>& L, const R* xi, R* x) {
+  R N[Dims<DIM>::NV];
+  shape_values<DIM, R>(xi, N);
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) x[a] = R(0);
+#pragma unroll
+  for (int v = 1; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) x[a] += N[v] * L.D[v][a];
+}
+
+template <int DIM, typename R>
+__device__ __forceinline__ void local_jacobian(const LocalCell<DIM, R>& L, const R* xi, R* J) {
+  R dN[Dims<DIM>::NV * DIM];
+  shape_grads_ref<DIM, R>(xi, dN);
+#pragma unroll
+  for (int k = 0; k < DIM * DIM; ++k) J[k] = R(0);
+#pragma unroll
+  for (int v = 1; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) J[a * DIM + b] += L.D[v][a] * dN[v * DIM + b];
+}
+
+template <typename R> struct NewtonTol;
+template <> struct NewtonTol<double> {
+  static constexpr double step = 1e-12;
+  static constexpr int iters = 30;
+};
+template <> struct NewtonTol<float> {
+  static constexpr float step = 2e-6f;
+  static constexpr int iters = 12;
+};
+
+// Inverse of the multilinear map (MappingQ1::transform_real_to_unit_cell)
+// for a point given in the cell-local frame. Returns false when Newton fails
+// (the reference treats that as "not in this cell").
+template <int DIM, typename R>
+__device__ __forceinline__ bool local_inverse(const LocalCell<DIM, R>& L, const R* x, R* xi) {
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) xi[d] = R(0.5);
+  for (int it = 0; it < NewtonTol<R>::iters; ++it) {
+    R F[DIM], J[DIM * DIM], Ji[DIM * DIM];
+    local_map<DIM, R>(L, xi, F);
+    local_jacobian<DIM, R>(L, xi, J);
+    R det = det_inv<DIM, R>(J, Ji);
+    if (!(det > R(0))) return false;
+    R mx = R(0);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      R s = R(0);
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) s += Ji[a * DIM + b] * (F[b] - x[b]);
+      xi[a] -= s;
+      mx = fmax(mx, fabs(s));
+    }
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+      if (!(fabs(xi[a]) < R(1e6))) return false;
+    if (mx < NewtonTol<R>::step) return true;
+  }
+  return false;
+}
+
+template <int DIM, typename R>
+__device__ __forceinline__ bool inside_unit(const R* xi) {
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) ok = ok && (xi[d] >= R(0) && xi[d] <= R(1));
+  return ok;
+}
+
+// Counter-based SplitMix64 stream (identical to the oracle's).
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t ordinal, int axis) {
+  uint64_t key = seed * 0xD1B54A32D192ED03ULL + ordinal * 4ULL + (uint64_t)axis;
+  return (double)(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Bounded software grid barrier for cooperative (co-resident) grids.
+// Every wait is capped; on timeout the barrier sets *err and returns false,
+// and callers leave their loops so the kernel always terminates.
+struct GridBarrier {
+  unsigned* count;
+  unsigned* gen;
+  int* err;
+};
+
+#define PFEM2_BARRIER_SPIN_LIMIT (1u << 26)
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = gb.gen;
+    unsigned g = *vgen;
+    __threadfence();
+    unsigned arrived = atomicAdd(gb.count, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      *gb.count = 0;
+      __threadfence();
+      atomicAdd(gb.gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (*vgen == g) {
+        if (++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)gb.err) {
+          atomicExch(gb.err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+    s_ok = ok && (*(volatile int*)gb.err == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(PFEM2_FULL_MASK, v, o);
+  return v;
+}
+
+}  // namespace pfem2

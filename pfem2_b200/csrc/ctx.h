@@ -1,0 +1,202 @@
+// ctx.h -- host-side context of libpfem2b: device buffers of a batch of
+// PFEM2 instances and the launchers shared by the .cu translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pfem2.h"
+
+namespace pfem2 {
+
+constexpr int kSlice = 32;          // SELL slice height (rows per warp)
+constexpr int kMaxPatch = 32;       // max cells around a vertex
+constexpr int kMaxRing = 64;        // max cells sharing a vertex with a cell
+constexpr int kNumSys = 7;          // pred x,y,z, pressure, mass x,y,z
+
+// Per-instance parameters visible to kernels.
+struct DevInst {
+  double mu, rho, dt, open_flux;
+  unsigned open_mask;
+  int q[3];
+  int max_per_part;
+  int v_off, nv_pad, c_off, nc;
+};
+
+struct HostInst {
+  int nv = 0, nc = 0;
+  int v_off = 0, nv_pad = 0, c_off = 0;
+  pfem2_case cs{};
+  unsigned q[3] = {0, 0, 0};
+  std::vector<double> X;
+  std::vector<int> cells, fb;
+};
+
+// Krylov tile: a run of SELL slices of one system.
+struct Tile {
+  int sys;        // system id inside the phase
+  int comp;       // component slot (vector block)
+  int s0, s1;     // slice range
+};
+
+struct Ctx {
+  pfem2_config cfg{};
+  int dim = 2;
+  bool mixed = false;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::vector<HostInst> inst;
+  bool setup_done = false;
+  bool seeded = false;
+  double time = 0.0;
+  int timestep = 1;
+  long long launches = 0;
+
+  // sizes (nv includes per-instance padding to a multiple of kSlice)
+  int nv = 0, nc = 0, ninc = 0, nnz = 0, nslices = 0, nell = 0;
+
+  // mesh
+  double* X = nullptr;
+  int* cv = nullptr;
+  signed char* fb = nullptr;
+  int* cell_inst = nullptr;
+  int* vert_inst = nullptr;
+  int* v2c_ptr = nullptr;
+  int* v2c_cell = nullptr;
+  unsigned char* v2c_loc = nullptr;
+  double* v2c_dir = nullptr;
+  void* v2c_dir_r = nullptr;  // Real copy for the particle kernels
+  int* ring_ptr = nullptr;
+  int* ring_cell = nullptr;
+  DevInst* d_inst = nullptr;
+  std::vector<DevInst> h_inst;
+
+  // sparsity: CSR (setup, tests) and SELL-32 (solvers)
+  int* rp = nullptr;
+  int* ci = nullptr;
+  int* inc_slot = nullptr;  // [ninc][NV] -> SELL entry index
+  int* sl_ptr = nullptr;    // [nslices+1] entry offset of each slice
+  int* sl_len = nullptr;    // [nslices] entries per row in the slice
+  int* sl_col = nullptr;    // [nell] column (padding: the row itself with value 0)
+  std::vector<int> h_sl_ptr;
+
+  // matrices in SELL layout (values only), FP64 master + FP32 copy
+  double* A64[kNumSys] = {};
+  float* A32[kNumSys] = {};
+  double* dinv64[kNumSys] = {};
+  float* dinv32[kNumSys] = {};
+
+  // Dirichlet tables: fields 0..2 velocity, 3 pressure
+  unsigned char* isdir[4] = {};
+  double* dirval[4] = {};
+  double* shift[4] = {};
+  unsigned char* zero_flag = nullptr;
+
+  // nodal fields (FP64 masters) and Real mirrors for particle kernels
+  double* F[PFEM2_N_FIELDS] = {};
+  double* corr[3] = {};
+  double* rhs[3] = {};
+  void* Vr = nullptr;   // [dim][nv] Real
+  void* dVr = nullptr;  // [dim][nv] Real, V - V_old
+
+  // particles (SoA, double buffered)
+  int pcap = 0;
+  int* pcell[2] = {};
+  void* pxi[2] = {};
+  void* pu[2] = {};
+  int cur = 0;
+  int* newcell = nullptr;
+  int* cell_start[2] = {};
+  int* cell_count = nullptr;
+  int* d_np = nullptr;       // [2] particle count of buffer 0/1
+  int far_cap = 0;
+  unsigned long long* far_keys = nullptr;
+  int* d_counters = nullptr;  // see enum Counter
+  void* partial = nullptr;    // [nc][NV][dim+1] Real projection partials
+  int* scan_tmp = nullptr;
+  int scan_tmp_n = 0;
+  int ring_max = 0;
+  int list_cap = 0;           // per-cell incoming particle capacity in the rebin pass
+  int nbucket_max = 0;
+
+  // Krylov workspace
+  void* kws = nullptr;
+  size_t kws_bytes = 0;
+  Tile* d_tiles[2] = {};      // [0] 1 component phase, [1] dim component phase
+  int ntiles[2] = {};
+  int tile_slices = 8;
+  double* sys_scalars = nullptr;
+  double* tile_part = nullptr;
+  int* d_sysinfo = nullptr;
+  unsigned* barrier = nullptr;   // count, gen
+  int* d_err = nullptr;
+  int coop_blocks = 0;
+  int solve_threads = 256;
+
+  // graph
+  cudaGraphExec_t graph = nullptr;
+  bool graph_valid = false;
+  bool timing = false;
+  cudaEvent_t ev[8] = {};
+  double stage_ms[6] = {};
+
+  pfem2_stats stats{};
+};
+
+enum Counter {
+  CNT_DELETED = 0,
+  CNT_REMOVED = 1,
+  CNT_RESEEDED = 2,
+  CNT_FAR = 3,
+  CNT_LIST_OVERFLOW = 4,
+  CNT_CAP_OVERFLOW = 5,
+  CNT_FAR_OVERFLOW = 6,
+  CNT_ZERO_WEIGHT = 7,
+  CNT_N = 8
+};
+
+// error reporting
+void set_error(const std::string& s);
+pfem2_status cuda_status(cudaError_t e, const char* where);
+#define PFEM2_CUDA(call)                                              \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) return ::pfem2::cuda_status(e_, #call);    \
+  } while (0)
+
+inline int grid_for(const Ctx& c, long long n, int threads, int per_sm = 8) {
+  long long b = (n + threads - 1) / threads;
+  long long cap = (long long)c.num_sms * per_sm;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// launchers (particles.cu)
+pfem2_status launch_seed(Ctx& c, int instance, const uint32_t q[3], uint64_t seed, double jitter);
+pfem2_status launch_correct(Ctx& c);
+pfem2_status launch_advect(Ctx& c, bool fuse_correct);
+pfem2_status launch_rebin(Ctx& c, bool do_check, bool fuse_project, bool from_advect);
+pfem2_status launch_project(Ctx& c, bool partials_ready);
+pfem2_status launch_sync_real_fields(Ctx& c);
+pfem2_status launch_set_particles(Ctx& c, const int* counts, const int* cell, const double* xi, const double* u);
+pfem2_status read_particles(Ctx& c, int instance, int* cell, double* xi, double* u, int* n);
+
+// fem.cu
+pfem2_status assemble_matrices(Ctx& c);
+pfem2_status launch_rhs_prediction(Ctx& c);
+pfem2_status launch_rhs_pressure(Ctx& c);
+pfem2_status launch_rhs_correction(Ctx& c);
+pfem2_status launch_finish_fem(Ctx& c);
+pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev);
+
+// krylov.cu
+pfem2_status krylov_setup(Ctx& c);
+// which: 0 prediction (dim systems per instance), 1 pressure, 2 correction
+pfem2_status krylov_solve(Ctx& c, int which);
+pfem2_status krylov_read_stats(Ctx& c);
+
+}  // namespace pfem2

@@ -1,0 +1,984 @@
+// particles.cu -- particle kernels of the PFEM2 step (sm_100a).
+//
+// Layout: particles are SoA and sorted by cell (cell_start offsets), with
+// reference coordinates xi[d][cap] and carried velocity u[d][cap] in the
+// arithmetic type R (float for the mixed path, double for the plain path).
+//
+// Kernels and the reference routines they replace:
+//   k_seed          seed_particles / seed_particles_into_cell
+//                   (TurekBenchmark/pfem2particle.cpp:701-721,774-790)
+//   k_correct       correct_particles_velocities (:792-811)
+//   k_advect        move_particles sub-steps (:813-848) + point location
+//                   sort_particles_into_subdomains_and_cells (:276-507),
+//                   find_closest_vertex_of_cell (:142-166),
+//                   compare_particle_association (:268-274)
+//   k_rebin         the re-sort by cell plus check_cell_for_empty_parts
+//                   (:723-772), with the projection partials fused in
+//   k_project_*     distribute_particle_velocities_to_grid (:858-918)
+#include <algorithm>
+#include <cstdio>
+
+#include "common.cuh"
+#include "ctx.h"
+
+namespace pfem2 {
+
+constexpr int kRebinWarps = 8;
+constexpr int kMaxBuckets = 256;
+
+// ------------------------------------------------------------------ seed
+template <int DIM, typename R>
+__global__ void k_seed(int c0, int c1, int q0, int q1, int q2, int pbase, uint64_t seed, double jitter,
+                       const double* __restrict__ X, const int* __restrict__ cv, const double* __restrict__ V0,
+                       const double* __restrict__ V1, const double* __restrict__ V2, int* __restrict__ cell,
+                       R* __restrict__ xi, R* __restrict__ u, size_t cap, int* __restrict__ cell_start) {
+  constexpr int NV = Dims<DIM>::NV;
+  const int Q = q0 * q1 * q2;
+  const double h[3] = {1.0 / q0, 1.0 / q1, 1.0 / q2};
+  const double* V[3] = {V0, V1, V2};
+  for (int c = c0 + blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += gridDim.x * blockDim.x) {
+    const size_t pc = (size_t)pbase + (size_t)(c - c0) * Q;
+    cell_start[c] = (int)pc;
+    for (int t = 0; t < Q; ++t) {
+      int idx[3] = {t / (q1 * q2), (t / q2) % q1, t % q2};
+      uint64_t ord = (uint64_t)(c - c0) * Q + t;
+      double x[3];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        x[d] = (idx[d] + 1.0 / 2) * h[d];
+        if (jitter != 0.0) x[d] += jitter * (2.0 * uniform01(seed, ord, d) - 1.0);
+      }
+      double N[NV];
+      shape_values<DIM, double>(x, N);
+      double uu[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        int g = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) uu[d] = uu[d] + N[v] * V[d][g];
+      }
+      size_t p = pc + t;
+      cell[p] = c;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        xi[d * cap + p] = R(x[d]);
+        u[d * cap + p] = R(uu[d]);
+      }
+    }
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status seed_impl(Ctx& c, uint64_t seed, double jitter) {
+  int b = c.cur;
+  size_t total = 0;
+  for (auto& in : c.inst) total += (size_t)in.nc * in.q[0] * in.q[1] * (DIM == 3 ? in.q[2] : 1);
+  if (total > (size_t)c.pcap) {
+    set_error("seed: particle capacity exceeded");
+    return PFEM2_PARTICLE_OVERFLOW;
+  }
+  size_t pbase = 0;
+  for (auto& in : c.inst) {
+    int q2 = DIM == 3 ? (int)in.q[2] : 1;
+    int grid = grid_for(c, in.nc, 128, 16);
+    k_seed<DIM, R><<<grid, 128, 0, c.stream>>>(in.c_off, in.c_off + in.nc, in.q[0], in.q[1], q2, (int)pbase, seed,
+                                               jitter, c.X, c.cv, c.F[PFEM2_FIELD_VX], c.F[PFEM2_FIELD_VY],
+                                               c.F[PFEM2_FIELD_VZ], c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b],
+                                               (size_t)c.pcap, c.cell_start[b]);
+    c.launches++;
+    pbase += (size_t)in.nc * in.q[0] * in.q[1] * q2;
+  }
+  int tot = (int)total;
+  PFEM2_CUDA(cudaMemcpyAsync(c.cell_start[b] + c.nc, &tot, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(c.d_np + b, &tot, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
+}
+
+pfem2_status launch_seed(Ctx& c, int instance, const uint32_t q[3], uint64_t seed, double jitter) {
+  (void)instance;
+  if (c.dim == 2) return c.mixed ? seed_impl<2, float>(c, seed, jitter) : seed_impl<2, double>(c, seed, jitter);
+  return c.mixed ? seed_impl<3, float>(c, seed, jitter) : seed_impl<3, double>(c, seed, jitter);
+}
+
+// -------------------------------------------------------- real mirrors
+template <int DIM, typename R>
+__global__ void k_sync_real(int nv, const double* __restrict__ V0, const double* __restrict__ V1,
+                            const double* __restrict__ V2, const double* __restrict__ O0,
+                            const double* __restrict__ O1, const double* __restrict__ O2, R* __restrict__ Vr,
+                            R* __restrict__ dVr) {
+  const double* V[3] = {V0, V1, V2};
+  const double* O[3] = {O0, O1, O2};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      double v = V[d][i];
+      Vr[(size_t)d * nv + i] = R(v);
+      dVr[(size_t)d * nv + i] = R(v - O[d][i]);
+    }
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status sync_real_impl(Ctx& c) {
+  k_sync_real<DIM, R><<<grid_for(c, c.nv, 256), 256, 0, c.stream>>>(
+      c.nv, c.F[PFEM2_FIELD_VX], c.F[PFEM2_FIELD_VY], c.F[PFEM2_FIELD_VZ], c.F[PFEM2_FIELD_OLD_VX],
+      c.F[PFEM2_FIELD_OLD_VY], c.F[PFEM2_FIELD_OLD_VZ], (R*)c.Vr, (R*)c.dVr);
+  c.launches++;
+  return PFEM2_OK;
+}
+
+pfem2_status launch_sync_real_fields(Ctx& c) {
+  if (c.dim == 2) return c.mixed ? sync_real_impl<2, float>(c) : sync_real_impl<2, double>(c);
+  return c.mixed ? sync_real_impl<3, float>(c) : sync_real_impl<3, double>(c);
+}
+
+// --------------------------------------------------------------- correct
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_correct(const int* __restrict__ cell, const R* __restrict__ xi,
+                                                 R* __restrict__ u, size_t cap, const int* __restrict__ d_np,
+                                                 const int* __restrict__ cv, const R* __restrict__ dV, int nv) {
+  constexpr int NV = Dims<DIM>::NV;
+  const int n = min(*d_np, (int)cap);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int c = cell[p];
+    R x[DIM], up[DIM], N[NV];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      x[d] = xi[d * cap + p];
+      up[d] = u[d * cap + p];
+    }
+    shape_values<DIM, R>(x, N);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      int g = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dV + (size_t)d * nv + g);
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) u[d * cap + p] = up[d];
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status correct_impl(Ctx& c) {
+  int b = c.cur;
+  k_correct<DIM, R><<<grid_for(c, c.pcap, 256, 8), 256, 0, c.stream>>>(
+      c.pcell[b], (const R*)c.pxi[b], (R*)c.pu[b], (size_t)c.pcap, c.d_np + b, c.cv, (const R*)c.dVr, c.nv);
+  c.launches++;
+  return PFEM2_OK;
+}
+
+pfem2_status launch_correct(Ctx& c) {
+  if (c.dim == 2) return c.mixed ? correct_impl<2, float>(c) : correct_impl<2, double>(c);
+  return c.mixed ? correct_impl<3, float>(c) : correct_impl<3, double>(c);
+}
+
+// ---------------------------------------------------------------- advect
+// One thread per particle; all PARTICLES_MOVEMENT_STEPS sub-steps run in
+// registers (the nodal field is fixed during move_particles). After each
+// sub-step the particle is located like the reference does: current cell
+// first, then the patch of the "closest" vertex in alignment order; a
+// particle found nowhere is deleted (newcell = -1).
+template <int DIM, typename R, bool FUSE>
+__global__ void __launch_bounds__(256) k_advect(
+    const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
+    const int* __restrict__ d_np, const double* __restrict__ X, const int* __restrict__ cv,
+    const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
+    const int* __restrict__ cell_inst, const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
+    const R* __restrict__ v2c_dir, const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell,
+    unsigned long long* __restrict__ far_keys, int far_cap, int* __restrict__ counters) {
+  constexpr int NV = Dims<DIM>::NV;
+  const int n = min(*d_np, (int)cap);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int c0 = cell[p];
+    int c = c0;
+    R x[DIM], up[DIM], N[NV];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      x[d] = xi[d * cap + p];
+      up[d] = u[d * cap + p];
+    }
+    if (FUSE) {
+      shape_values<DIM, R>(x, N);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        int g = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
+      }
+    }
+    const R dts = R(inst[__ldg(cell_inst + c0)].dt / S);
+    LocalCell<DIM, R> L;
+    double x0[DIM];
+    load_local_cell<DIM, R>(X, cv, c, L, x0);
+    bool alive = true;
+    for (int s = 0; s < S && alive; ++s) {
+      shape_values<DIM, R>(x, N);
+      R uf[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) uf[d] = R(0);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        int g = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * __ldg(Vr + (size_t)d * nv + g);
+      }
+      R xo[DIM], xn[DIM], x2[DIM];
+      local_map<DIM, R>(L, x, xo);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xn[d] = xo[d] + uf[d] * dts;
+      if (local_inverse<DIM, R>(L, xn, x2) && inside_unit<DIM, R>(x2)) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) x[d] = x2[d];
+        continue;
+      }
+      // closest vertex of the old cell seen along the velocity
+      R un = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) un += uf[d] * uf[d];
+      un = sqrt(un);
+      R best = R(0);
+      int bv = 0;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        R t[DIM], tn = R(0), dot = R(0);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          t[d] = L.D[v][d] - xo[d];
+          tn += t[d] * t[d];
+        }
+        tn = sqrt(tn);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dot += (uf[d] / un) * (t[d] / tn);
+        if (v == 0) best = dot;
+        else if (dot > best) { best = dot; bv = v; }
+      }
+      const int gv = __ldg(cv + (size_t)c * NV + bv);
+      R vp[DIM], vpn = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        vp[d] = xn[d] - L.D[bv][d];
+        vpn += vp[d] * vp[d];
+      }
+      vpn = sqrt(vpn);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vp[d] /= vpn;
+      const int k0 = __ldg(v2c_ptr + gv);
+      int nk = __ldg(v2c_ptr + gv + 1) - k0;
+      if (nk > kMaxPatch) nk = kMaxPatch;
+      R key[kMaxPatch];
+      int perm[kMaxPatch];
+      for (int i = 0; i < nk; ++i) {
+        R sdot = R(0);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) sdot += __ldg(v2c_dir + (size_t)(k0 + i) * DIM + d) * vp[d];
+        key[i] = sdot;
+        // stable insertion by descending alignment (std::sort is an
+        // insertion sort, hence stable, for patches of <= 16 cells)
+        int j = i - 1;
+        while (j >= 0 && sdot > key[perm[j]]) {
+          perm[j + 1] = perm[j];
+          --j;
+        }
+        perm[j + 1] = i;
+      }
+      bool found = false;
+      for (int i = 0; i < nk && !found; ++i) {
+        const int cc = __ldg(v2c_cell + k0 + perm[i]);
+        LocalCell<DIM, R> Lc;
+        double xc[DIM];
+        load_local_cell<DIM, R>(X, cv, cc, Lc, xc);
+        R t[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) t[d] = xn[d] + R(x0[d] - xc[d]);
+        if (local_inverse<DIM, R>(Lc, t, x2) && inside_unit<DIM, R>(x2)) {
+          found = true;
+          c = cc;
+          L = Lc;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            x0[d] = xc[d];
+            x[d] = x2[d];
+          }
+        }
+      }
+      if (!found) alive = false;
+    }
+    if (!alive) {
+      c = -1;
+      atomicAdd(counters + CNT_DELETED, 1);
+    } else if (c != c0) {
+      // a particle that left the 1-ring of its old cell goes to the far list
+      bool near = false;
+      for (int r = __ldg(ring_ptr + c0); r < __ldg(ring_ptr + c0 + 1); ++r)
+        if (__ldg(ring_cell + r) == c) { near = true; break; }
+      if (!near) {
+        int slot = atomicAdd(counters + CNT_FAR, 1);
+        if (slot < far_cap) far_keys[slot] = ((unsigned long long)(unsigned)c << 32) | (unsigned)p;
+        else atomicExch(counters + CNT_FAR_OVERFLOW, 1);
+      }
+    }
+    newcell[p] = c;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      xi[d * cap + p] = x[d];
+      u[d * cap + p] = up[d];
+    }
+  }
+}
+
+// single-CTA bitonic sort of the (cell, particle) keys of the far movers
+__global__ void k_far_sort(unsigned long long* keys, const int* __restrict__ counters, int cap) {
+  extern __shared__ unsigned long long sk[];
+  int n = counters[CNT_FAR];
+  if (n > cap) n = cap;
+  if (n <= 1) return;
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) sk[i] = i < n ? keys[i] : ~0ull;
+  __syncthreads();
+  for (int k = 2; k <= m; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        int l = i ^ j;
+        if (l > i) {
+          bool up = (i & k) == 0;
+          unsigned long long a = sk[i], b = sk[l];
+          if ((a > b) == up) { sk[i] = b; sk[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) keys[i] = sk[i];
+}
+
+template <int DIM, typename R>
+static pfem2_status advect_impl(Ctx& c, bool fuse) {
+  int b = c.cur;
+  int grid = grid_for(c, c.pcap, 256, 8);
+  int S = c.cfg.movement_steps;
+  if (fuse)
+    k_advect<DIM, R, true><<<grid, 256, 0, c.stream>>>(
+        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b, c.X, c.cv, (const R*)c.Vr,
+        (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
+        c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+  else
+    k_advect<DIM, R, false><<<grid, 256, 0, c.stream>>>(
+        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b, c.X, c.cv, (const R*)c.Vr,
+        (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
+        c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+  c.launches++;
+  k_far_sort<<<1, 1024, sizeof(unsigned long long) * c.far_cap, c.stream>>>(c.far_keys, c.d_counters, c.far_cap);
+  c.launches++;
+  return PFEM2_OK;
+}
+
+pfem2_status launch_advect(Ctx& c, bool fuse) {
+  PFEM2_CUDA(cudaMemsetAsync(c.d_counters, 0, sizeof(int) * CNT_N, c.stream));
+  if (c.dim == 2) return c.mixed ? advect_impl<2, float>(c, fuse) : advect_impl<2, double>(c, fuse);
+  return c.mixed ? advect_impl<3, float>(c, fuse) : advect_impl<3, double>(c, fuse);
+}
+
+// ----------------------------------------------------------------- rebin
+// One warp per target cell. Pass 0 counts, pass 1 writes. The incoming
+// particles of cell c are gathered from the old segments of the cells
+// sharing a vertex with c (ascending cell id, segment order), so the
+// result is a stable sort by cell of the old storage order; particles that
+// left that 1-ring come from the sorted far list and are merged by index.
+// With CHECK the per-sub-cell counts are walked in that order: a particle
+// whose bucket already holds MAX_PARTICLES_PER_CELL_PART is removed, and
+// every empty sub-cell receives one particle at its centre, appended in
+// (i,j,k) order with the interpolated nodal velocity.
+template <int DIM, typename R>
+struct ProjAcc {
+  R a[Dims<DIM>::NV][DIM + 1];
+};
+
+template <int DIM, typename R>
+__device__ __forceinline__ void proj_add(ProjAcc<DIM, R>& acc, const R* x, const R* uu) {
+  R N[Dims<DIM>::NV];
+  shape_values<DIM, R>(x, N);
+#pragma unroll
+  for (int v = 0; v < Dims<DIM>::NV; ++v) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) acc.a[v][d] += N[v] * uu[d];
+    acc.a[v][DIM] += N[v];
+  }
+}
+
+template <int DIM, typename R>
+__device__ __forceinline__ void proj_store(ProjAcc<DIM, R>& acc, R* __restrict__ partial, int c, int lane) {
+  constexpr int K = Dims<DIM>::NV * (DIM + 1);
+#pragma unroll
+  for (int v = 0; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+    for (int k = 0; k <= DIM; ++k) acc.a[v][k] = warp_sum(acc.a[v][k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+      for (int k = 0; k <= DIM; ++k) partial[(size_t)c * K + v * (DIM + 1) + k] = acc.a[v][k];
+  }
+}
+
+// sub-cell index of check_cell_for_empty_parts: unsigned(xi / h), which is q
+// for xi == 1 (a bucket of its own, as in the reference); clamped to [0, q]
+__device__ __forceinline__ int sub_bucket(double xi, double h, int q) {
+  double t = xi / h;
+  if (!(t >= 0.0)) t = 0.0;
+  if (t > (double)q) t = (double)q;
+  return (int)(unsigned)t;
+}
+
+__device__ __forceinline__ int far_lower_bound(const unsigned long long* keys, int n, unsigned long long k) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (keys[mid] < k) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+template <int DIM, typename R, int PASS, bool CHECK, bool PROJ>
+__global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
+    const int* __restrict__ old_start, const int* __restrict__ newcell, const R* __restrict__ oxi,
+    const R* __restrict__ ou, size_t cap, int* __restrict__ ncell, R* __restrict__ nxi, R* __restrict__ nu,
+    const int* __restrict__ new_start, int* __restrict__ cell_count, int nc, const int* __restrict__ ring_ptr,
+    const int* __restrict__ ring_cell, const unsigned long long* __restrict__ far_keys, int far_cap,
+    const DevInst* __restrict__ inst, const int* __restrict__ cell_inst, const int* __restrict__ cv,
+    const R* __restrict__ Vr, int nv, R* __restrict__ partial, int list_cap, int* __restrict__ counters) {
+  constexpr int NV = Dims<DIM>::NV;
+  extern __shared__ int smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* list = smem + warp * (list_cap + kMaxBuckets);
+  int* bcnt = list + list_cap;
+  const unsigned lt = lanemask_lt();
+  int nfar = counters[CNT_FAR];
+  if (nfar > far_cap) nfar = far_cap;
+  for (int c = blockIdx.x * kRebinWarps + warp; c < nc; c += gridDim.x * kRebinWarps) {
+    int n_in = 0;
+    const int r1 = __ldg(ring_ptr + c + 1);
+    for (int r = __ldg(ring_ptr + c); r < r1; ++r) {
+      const int s = __ldg(ring_cell + r);
+      const int b = min(old_start[s], (int)cap), e = min(old_start[s + 1], (int)cap);
+      for (int base = b; base < e; base += 32) {
+        const int p = base + lane;
+        const bool pred = p < e && newcell[p] == c;
+        const unsigned m = __ballot_sync(PFEM2_FULL_MASK, pred);
+        const int pos = n_in + __popc(m & lt);
+        if (pred && pos < list_cap) list[pos] = p;
+        n_in += __popc(m);
+      }
+    }
+    if (nfar > 0) {
+      const int lo = far_lower_bound(far_keys, nfar, (unsigned long long)(unsigned)c << 32);
+      const int hi = far_lower_bound(far_keys, nfar, (unsigned long long)(unsigned)(c + 1) << 32);
+      __syncwarp();
+      if (hi > lo && lane == 0) {
+        int m = n_in < list_cap ? n_in : list_cap;
+        for (int k = lo; k < hi; ++k) {
+          const int p = (int)(far_keys[k] & 0xffffffffu);
+          if (p < 0 || p >= (int)cap) continue;
+          int j = m - 1;
+          while (j >= 0 && list[j] > p) {
+            if (j + 1 < list_cap) list[j + 1] = list[j];
+            --j;
+          }
+          if (j + 1 < list_cap) list[j + 1] = p;
+          if (m < list_cap) ++m;
+        }
+      }
+      n_in += hi - lo;
+      __syncwarp();
+    }
+    if (n_in > list_cap) {
+      if (lane == 0) atomicExch(counters + CNT_LIST_OVERFLOW, 1);
+      n_in = list_cap;
+    }
+    const DevInst& I = inst[__ldg(cell_inst + c)];
+    const int q0 = I.q[0], q1 = I.q[1], q2 = DIM == 3 ? I.q[2] : 1;
+    const int nb1 = q1 + 1, nb2 = q2 + 1;
+    const double h0 = 1.0 / q0, h1 = 1.0 / q1, h2 = 1.0 / q2;
+    int n_keep = n_in, n_new = 0;
+    if (CHECK) {
+      const int nb = (q0 + 1) * nb1 * nb2;
+      for (int k = lane; k < nb; k += 32) bcnt[k] = 0;
+      __syncwarp();
+      n_keep = 0;
+      for (int base = 0; base < n_in; base += 32) {
+        const int i = base + lane;
+        const bool active = i < n_in;
+        const int p = active ? list[i] : -1;
+        int bi = -1;
+        if (active) {
+          const int b0 = sub_bucket((double)oxi[p], h0, q0);
+          const int b1 = sub_bucket((double)oxi[cap + p], h1, q1);
+          const int b2 = DIM == 3 ? sub_bucket((double)oxi[2 * cap + p], h2, q2) : 0;
+          bi = (b0 * nb1 + b1) * nb2 + b2;
+        }
+        const unsigned peers = __match_any_sync(PFEM2_FULL_MASK, bi);
+        bool keep = false;
+        int prev = 0;
+        if (active) prev = bcnt[bi];
+        __syncwarp();
+        if (active) {
+          keep = prev + __popc(peers & lt) + 1 <= I.max_per_part;
+          if ((peers & lt) == 0) bcnt[bi] = prev + __popc(peers);
+        }
+        const unsigned km = __ballot_sync(PFEM2_FULL_MASK, keep);
+        const int kpos = n_keep + __popc(km & lt);
+        __syncwarp();
+        if (keep) list[kpos] = p;
+        n_keep += __popc(km);
+        __syncwarp();
+      }
+      // empty sub-cells -> new particles, (i,j,k) order
+      const int Q = q0 * q1 * q2;
+      for (int base = 0; base < Q; base += 32) {
+        const int t = base + lane;
+        bool e = false;
+        if (t < Q) {
+          const int i0 = t / (q1 * q2), i1 = (t / q2) % q1, i2 = t % q2;
+          e = bcnt[(i0 * nb1 + i1) * nb2 + i2] == 0;
+        }
+        const unsigned em = __ballot_sync(PFEM2_FULL_MASK, e);
+        const int pos = n_keep + n_new + __popc(em & lt);
+        if (e && pos < list_cap) list[pos] = -1 - t;
+        n_new += __popc(em);
+      }
+      if (n_keep + n_new > list_cap) {
+        if (lane == 0) atomicExch(counters + CNT_LIST_OVERFLOW, 1);
+        n_new = list_cap - n_keep;
+      }
+      __syncwarp();
+    }
+    const int ntot = n_keep + n_new;
+    if (PASS == 0) {
+      if (lane == 0) {
+        cell_count[c] = ntot;
+        if (CHECK) {
+          if (n_in - n_keep) atomicAdd(counters + CNT_REMOVED, n_in - n_keep);
+          if (n_new) atomicAdd(counters + CNT_RESEEDED, n_new);
+        }
+      }
+    } else {
+      const int out = new_start[c];
+      ProjAcc<DIM, R> acc;
+      if (PROJ) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+          for (int k = 0; k <= DIM; ++k) acc.a[v][k] = R(0);
+      }
+      for (int j = lane; j < ntot; j += 32) {
+        const int code = list[j];
+        R x[DIM], uu[DIM];
+        if (code >= 0) {
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            x[d] = oxi[d * cap + code];
+            uu[d] = ou[d * cap + code];
+          }
+        } else {
+          const int t = -1 - code;
+          const int id[3] = {t / (q1 * q2), (t / q2) % q1, t % q2};
+          const double hh[3] = {h0, h1, h2};
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) x[d] = R((id[d] + 1.0 / 2) * hh[d]);
+          R N[NV];
+          shape_values<DIM, R>(x, N);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) uu[d] = R(0);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            const int g = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) uu[d] = uu[d] + N[v] * Vr[(size_t)d * nv + g];
+          }
+        }
+        const size_t o = (size_t)out + j;
+        if (o < cap) {
+          ncell[o] = c;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            nxi[d * cap + o] = x[d];
+            nu[d * cap + o] = uu[d];
+          }
+        }
+        if (PROJ) proj_add<DIM, R>(acc, x, uu);
+      }
+      if (PROJ) proj_store<DIM, R>(acc, partial, c, lane);
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------------ scan
+// exclusive scan of cell_count[0..n) into out[0..n], out[n] = total.
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restrict__ in, int n, int* __restrict__ sums) {
+  __shared__ int ws[kScanThreads / 32];
+  const int base = blockIdx.x * kScanTile;
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    int i = base + threadIdx.x + k * kScanThreads;
+    if (i < n) s += in[i];
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = threadIdx.x < kScanThreads / 32 ? ws[threadIdx.x] : 0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) sums[blockIdx.x] = v;
+  }
+}
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+  __shared__ int ws[kScanThreads / 32 + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(PFEM2_FULL_MASK, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < kScanThreads / 32 ? ws[lane] : 0;
+    int z = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(PFEM2_FULL_MASK, z, o);
+      if (lane >= o) z += y;
+    }
+    if (lane < kScanThreads / 32) ws[lane] = z - w;
+    if (lane == kScanThreads / 32 - 1) ws[kScanThreads / 32] = z;
+  }
+  __syncthreads();
+  int res = ws[warp] + x - v;
+  *total = ws[kScanThreads / 32];
+  __syncthreads();
+  return res;
+}
+
+// scans the block sums in place (single block), writes the grand total
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int* sums, int nb, int* total_out0, int* total_out1,
+                                                            int* total_out2) {
+  int carry = 0;
+  for (int base = 0; base < nb; base += kScanThreads) {
+    int i = base + threadIdx.x;
+    int v = i < nb ? sums[i] : 0;
+    int tot;
+    int ex = block_exclusive_scan(v, &tot);
+    if (i < nb) sums[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) {
+    *total_out0 = carry;
+    if (total_out1) *total_out1 = carry;
+    if (total_out2) *total_out2 = carry;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restrict__ in, int n,
+                                                             const int* __restrict__ sums, int* __restrict__ out) {
+  const int base = blockIdx.x * kScanTile;
+  int vals[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    int i = base + threadIdx.x * kScanItems + k;
+    vals[k] = i < n ? in[i] : 0;
+    s += vals[k];
+  }
+  int tot;
+  int ex = block_exclusive_scan(s, &tot) + sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    int i = base + threadIdx.x * kScanItems + k;
+    if (i < n) out[i] = ex;
+    ex += vals[k];
+  }
+}
+
+static pfem2_status scan_counts(Ctx& c, const int* in, int n, int* out, int* np_out) {
+  int nb = (n + kScanTile - 1) / kScanTile;
+  k_scan_reduce<<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_tmp);
+  k_scan_sums<<<1, kScanThreads, 0, c.stream>>>(c.scan_tmp, nb, out + n, np_out, nullptr);
+  k_scan_final<<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_tmp, out);
+  c.launches += 3;
+  return PFEM2_OK;
+}
+
+template <int DIM, typename R, bool CHECK, bool PROJ>
+static void rebin_launch(Ctx& c, const int* newcell) {
+  const int o = c.cur, nb = 1 - c.cur;
+  const size_t smem = (size_t)kRebinWarps * (c.list_cap + kMaxBuckets) * sizeof(int);
+  const int grid = grid_for(c, (long long)c.nc * 32, kRebinWarps * 32, 8);
+  k_rebin<DIM, R, 0, CHECK, false><<<grid, kRebinWarps * 32, smem, c.stream>>>(
+      c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, nullptr, nullptr, nullptr,
+      nullptr, c.cell_count, c.nc, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_inst, c.cell_inst, c.cv,
+      (const R*)c.Vr, c.nv, nullptr, c.list_cap, c.d_counters);
+  scan_counts(c, c.cell_count, c.nc, c.cell_start[nb], c.d_np + nb);
+  k_rebin<DIM, R, 1, CHECK, PROJ><<<grid, kRebinWarps * 32, smem, c.stream>>>(
+      c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, c.pcell[nb], (R*)c.pxi[nb],
+      (R*)c.pu[nb], c.cell_start[nb], nullptr, c.nc, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_inst,
+      c.cell_inst, c.cv, (const R*)c.Vr, c.nv, (R*)c.partial, c.list_cap, c.d_counters);
+  c.launches += 2;
+  c.cur = nb;
+}
+
+template <int DIM, typename R>
+static pfem2_status rebin_impl(Ctx& c, bool check, bool proj, bool from_advect) {
+  const int* nc_arr = from_advect ? c.newcell : c.pcell[c.cur];
+  const size_t smem = (size_t)kRebinWarps * (c.list_cap + kMaxBuckets) * sizeof(int);
+  static bool attr_set[2][2][2] = {};
+  (void)attr_set;
+  auto set_attr = [&](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); };
+  if (check && proj) {
+    set_attr((const void*)k_rebin<DIM, R, 0, true, false>);
+    set_attr((const void*)k_rebin<DIM, R, 1, true, true>);
+    rebin_launch<DIM, R, true, true>(c, nc_arr);
+  } else if (check) {
+    set_attr((const void*)k_rebin<DIM, R, 0, true, false>);
+    set_attr((const void*)k_rebin<DIM, R, 1, true, false>);
+    rebin_launch<DIM, R, true, false>(c, nc_arr);
+  } else if (proj) {
+    set_attr((const void*)k_rebin<DIM, R, 0, false, false>);
+    set_attr((const void*)k_rebin<DIM, R, 1, false, true>);
+    rebin_launch<DIM, R, false, true>(c, nc_arr);
+  } else {
+    set_attr((const void*)k_rebin<DIM, R, 0, false, false>);
+    set_attr((const void*)k_rebin<DIM, R, 1, false, false>);
+    rebin_launch<DIM, R, false, false>(c, nc_arr);
+  }
+  return PFEM2_OK;
+}
+
+pfem2_status launch_rebin(Ctx& c, bool check, bool proj, bool from_advect) {
+  if (!from_advect) {
+    // no movers: make sure the far list is empty
+    PFEM2_CUDA(cudaMemsetAsync(c.d_counters + CNT_FAR, 0, sizeof(int), c.stream));
+  }
+  if (c.dim == 2) return c.mixed ? rebin_impl<2, float>(c, check, proj, from_advect) : rebin_impl<2, double>(c, check, proj, from_advect);
+  return c.mixed ? rebin_impl<3, float>(c, check, proj, from_advect) : rebin_impl<3, double>(c, check, proj, from_advect);
+}
+
+// --------------------------------------------------------------- project
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_project_cells(const int* __restrict__ cell_start, const R* __restrict__ xi,
+                                                       const R* __restrict__ u, size_t cap, int nc,
+                                                       R* __restrict__ partial) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int c = blockIdx.x * wpb + warp; c < nc; c += gridDim.x * wpb) {
+    const int b = min(cell_start[c], (int)cap), n = min(cell_start[c + 1], (int)cap) - b;
+    ProjAcc<DIM, R> acc;
+#pragma unroll
+    for (int v = 0; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+      for (int k = 0; k <= DIM; ++k) acc.a[v][k] = R(0);
+    for (int j = lane; j < n; j += 32) {
+      R x[DIM], uu[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        x[d] = xi[d * cap + b + j];
+        uu[d] = u[d * cap + b + j];
+      }
+      proj_add<DIM, R>(acc, x, uu);
+    }
+    proj_store<DIM, R>(acc, partial, c, lane);
+  }
+}
+
+// node gather: u_n = sum_k N u / sum_k N over the cells around node n, in
+// ascending cell order (deterministic, no float atomics)
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_project_nodes(int nv, const int* __restrict__ v2c_ptr,
+                                                       const int* __restrict__ v2c_cell,
+                                                       const unsigned char* __restrict__ v2c_loc,
+                                                       const R* __restrict__ partial,
+                                                       const unsigned char* __restrict__ zero_flag,
+                                                       double* __restrict__ V0, double* __restrict__ V1,
+                                                       double* __restrict__ V2, double* __restrict__ W,
+                                                       R* __restrict__ Vr, int* __restrict__ counters) {
+  constexpr int K = Dims<DIM>::NV * (DIM + 1);
+  double* V[3] = {V0, V1, V2};
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    R s[DIM + 1];
+#pragma unroll
+    for (int k = 0; k <= DIM; ++k) s[k] = R(0);
+    const int k1 = v2c_ptr[v + 1];
+    for (int k = v2c_ptr[v]; k < k1; ++k) {
+      const R* pp = partial + (size_t)v2c_cell[k] * K + v2c_loc[k] * (DIM + 1);
+#pragma unroll
+      for (int q = 0; q <= DIM; ++q) s[q] += pp[q];
+    }
+    const R w = s[DIM];
+    const bool z = zero_flag[v] != 0;
+    if (w == R(0) && k1 > v2c_ptr[v]) atomicAdd(counters + CNT_ZERO_WEIGHT, 1);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      R val = (w != R(0)) ? s[d] / w : R(0);
+      if (z) val = R(0);
+      V[d][v] = (double)val;
+      Vr[(size_t)d * nv + v] = val;
+    }
+    W[v] = (double)w;
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status project_impl(Ctx& c, bool partials_ready) {
+  const int b = c.cur;
+  if (!partials_ready) {
+    k_project_cells<DIM, R><<<grid_for(c, (long long)c.nc * 32, 256, 8), 256, 0, c.stream>>>(
+        c.cell_start[b], (const R*)c.pxi[b], (const R*)c.pu[b], (size_t)c.pcap, c.nc, (R*)c.partial);
+    c.launches++;
+  }
+  k_project_nodes<DIM, R><<<grid_for(c, c.nv, 256, 8), 256, 0, c.stream>>>(
+      c.nv, c.v2c_ptr, c.v2c_cell, c.v2c_loc, (const R*)c.partial, c.zero_flag, c.F[PFEM2_FIELD_VX],
+      c.F[PFEM2_FIELD_VY], c.dim == 3 ? c.F[PFEM2_FIELD_VZ] : c.F[PFEM2_FIELD_VZ], c.F[PFEM2_FIELD_NODE_WEIGHT],
+      (R*)c.Vr, c.d_counters);
+  c.launches++;
+  return PFEM2_OK;
+}
+
+pfem2_status launch_project(Ctx& c, bool partials_ready) {
+  if (c.dim == 2) return c.mixed ? project_impl<2, float>(c, partials_ready) : project_impl<2, double>(c, partials_ready);
+  return c.mixed ? project_impl<3, float>(c, partials_ready) : project_impl<3, double>(c, partials_ready);
+}
+
+// -------------------------------------------------- particle state access
+template <int DIM, typename R>
+__global__ void k_pack_out(const int* __restrict__ cell, const R* __restrict__ xi, const R* __restrict__ u,
+                           size_t cap, int p0, int n, int c_off, int* __restrict__ ocell, double* __restrict__ oxi,
+                           double* __restrict__ ou) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const size_t p = (size_t)p0 + j;
+    ocell[j] = cell[p] - c_off;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      oxi[(size_t)j * DIM + d] = (double)xi[d * cap + p];
+      ou[(size_t)j * DIM + d] = (double)u[d * cap + p];
+    }
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status read_impl(Ctx& c, int instance, int* cell, double* xi, double* u, int* n_out) {
+  const int b = c.cur;
+  const HostInst& in = c.inst[instance];
+  int se[2];
+  PFEM2_CUDA(cudaMemcpyAsync(&se[0], c.cell_start[b] + in.c_off, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(&se[1], c.cell_start[b] + in.c_off + in.nc, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  const int n = se[1] - se[0];
+  *n_out = n;
+  if (!cell) return PFEM2_OK;
+  if (n == 0) return PFEM2_OK;
+  int* dc;
+  double *dx, *du;
+  PFEM2_CUDA(cudaMallocAsync(&dc, sizeof(int) * n, c.stream));
+  PFEM2_CUDA(cudaMallocAsync(&dx, sizeof(double) * n * DIM, c.stream));
+  PFEM2_CUDA(cudaMallocAsync(&du, sizeof(double) * n * DIM, c.stream));
+  k_pack_out<DIM, R><<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.pcell[b], (const R*)c.pxi[b], (const R*)c.pu[b],
+                                                               (size_t)c.pcap, se[0], n, in.c_off, dc, dx, du);
+  c.launches++;
+  PFEM2_CUDA(cudaMemcpyAsync(cell, dc, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(xi, dx, sizeof(double) * n * DIM, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(u, du, sizeof(double) * n * DIM, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaFreeAsync(dc, c.stream));
+  PFEM2_CUDA(cudaFreeAsync(dx, c.stream));
+  PFEM2_CUDA(cudaFreeAsync(du, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  return PFEM2_OK;
+}
+
+pfem2_status read_particles(Ctx& c, int instance, int* cell, double* xi, double* u, int* n) {
+  if (c.dim == 2) return c.mixed ? read_impl<2, float>(c, instance, cell, xi, u, n) : read_impl<2, double>(c, instance, cell, xi, u, n);
+  return c.mixed ? read_impl<3, float>(c, instance, cell, xi, u, n) : read_impl<3, double>(c, instance, cell, xi, u, n);
+}
+
+// unsorted particles in, stable sort by cell through the rebin machinery:
+// the particles are first placed one per "virtual old segment" (all in the
+// segment of their own cell, in input order) and then rebinned without check.
+template <int DIM, typename R>
+__global__ void k_unpack_in(int n, const int* __restrict__ pos, const int* __restrict__ icell,
+                            const double* __restrict__ ixi, const double* __restrict__ iu, int* __restrict__ cell,
+                            R* __restrict__ xi, R* __restrict__ u, size_t cap) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const size_t p = pos[j];
+    cell[p] = icell[j];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      xi[d * cap + p] = R(ixi[(size_t)j * DIM + d]);
+      u[d * cap + p] = R(iu[(size_t)j * DIM + d]);
+    }
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status set_impl(Ctx& c, const int* counts, const int* cell, const double* xi, const double* u) {
+  // host-side stable placement by cell (a state-loading utility, not the step)
+  size_t n = 0;
+  for (size_t i = 0; i < c.inst.size(); ++i) n += counts[i];
+  if (n > (size_t)c.pcap) {
+    set_error("set_particles: capacity exceeded");
+    return PFEM2_PARTICLE_OVERFLOW;
+  }
+  std::vector<int> gcell(n), cnt(c.nc + 1, 0), pos(n);
+  size_t k = 0;
+  for (size_t i = 0; i < c.inst.size(); ++i)
+    for (int j = 0; j < counts[i]; ++j, ++k) {
+      int lc = cell[k];
+      if (lc < 0 || lc >= c.inst[i].nc) {
+        set_error("set_particles: cell out of range");
+        return PFEM2_INVALID_ARG;
+      }
+      gcell[k] = lc + c.inst[i].c_off;
+      cnt[gcell[k] + 1]++;
+    }
+  for (int i = 0; i < c.nc; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int> start(cnt.begin(), cnt.end());
+  for (size_t j = 0; j < n; ++j) pos[j] = cnt[gcell[j]]++;
+  const int b = c.cur;
+  int *dpos, *dcell;
+  double *dxi, *du;
+  size_t nn = n ? n : 1;
+  PFEM2_CUDA(cudaMalloc(&dpos, sizeof(int) * nn));
+  PFEM2_CUDA(cudaMalloc(&dcell, sizeof(int) * nn));
+  PFEM2_CUDA(cudaMalloc(&dxi, sizeof(double) * nn * DIM));
+  PFEM2_CUDA(cudaMalloc(&du, sizeof(double) * nn * DIM));
+  PFEM2_CUDA(cudaMemcpy(dpos, pos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  PFEM2_CUDA(cudaMemcpy(dcell, gcell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  PFEM2_CUDA(cudaMemcpy(dxi, xi, sizeof(double) * n * DIM, cudaMemcpyHostToDevice));
+  PFEM2_CUDA(cudaMemcpy(du, u, sizeof(double) * n * DIM, cudaMemcpyHostToDevice));
+  if (n) {
+    k_unpack_in<DIM, R><<<grid_for(c, n, 256), 256, 0, c.stream>>>((int)n, dpos, dcell, dxi, du, c.pcell[b],
+                                                                 (R*)c.pxi[b], (R*)c.pu[b], (size_t)c.pcap);
+    c.launches++;
+  }
+  PFEM2_CUDA(cudaMemcpyAsync(c.cell_start[b], start.data(), sizeof(int) * (c.nc + 1), cudaMemcpyHostToDevice, c.stream));
+  int nint = (int)n;
+  PFEM2_CUDA(cudaMemcpyAsync(c.d_np + b, &nint, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  cudaFree(dpos); cudaFree(dcell); cudaFree(dxi); cudaFree(du);
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
+}
+
+pfem2_status launch_set_particles(Ctx& c, const int* counts, const int* cell, const double* xi, const double* u) {
+  if (c.dim == 2) return c.mixed ? set_impl<2, float>(c, counts, cell, xi, u) : set_impl<2, double>(c, counts, cell, xi, u);
+  return c.mixed ? set_impl<3, float>(c, counts, cell, xi, u) : set_impl<3, double>(c, counts, cell, xi, u);
+}
+
+}  // namespace pfem2

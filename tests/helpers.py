@@ -1,0 +1,52 @@
+"""Shared helpers of the parity tests (oracle vs CUDA library)."""
+import numpy as np
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    n = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def near_face(xi, eps):
+    xi = np.asarray(xi)
+    return np.any(np.minimum(xi, 1.0 - xi) < eps, axis=-1)
+
+
+def compare_particles(o, g, eps_face, xi_tol, u_tol):
+    """o, g: (cell, xi, u) in storage order (sorted by cell, stable).
+
+    Cells whose particle counts agree are compared element-wise. Particles of
+    cells whose counts differ must all lie within eps_face (reference units)
+    of a face of their cell: membership may flip only there.
+    Returns a dict of statistics; raises AssertionError on a violation.
+    """
+    oc, ox, ou = o
+    gc, gx, gu = g
+    ncell = int(max(oc.max(initial=-1), gc.max(initial=-1))) + 1
+    co = np.bincount(oc, minlength=ncell)
+    cg = np.bincount(gc, minlength=ncell)
+    so = np.concatenate([[0], np.cumsum(co)])
+    sg = np.concatenate([[0], np.cumsum(cg)])
+    same = co == cg
+    idx_o = np.concatenate([np.arange(so[c], so[c + 1]) for c in np.nonzero(same)[0]]) if same.any() else np.zeros(0, int)
+    idx_g = np.concatenate([np.arange(sg[c], sg[c + 1]) for c in np.nonzero(same)[0]]) if same.any() else np.zeros(0, int)
+    dxi = np.abs(ox[idx_o] - gx[idx_g]).max(initial=0.0)
+    du = np.abs(ou[idx_o] - gu[idx_g]).max(initial=0.0)
+    bad_cells = np.nonzero(~same)[0]
+    flips = 0
+    for c in bad_cells:
+        a = ox[so[c]:so[c + 1]]
+        b = gx[sg[c]:sg[c + 1]]
+        # every particle not matched by a near-identical partner must be near a face
+        for arr, other in ((a, b), (b, a)):
+            for p in arr:
+                if other.size and np.abs(other - p).max(axis=1).min() < 10 * xi_tol:
+                    continue
+                assert near_face(p[None, :], eps_face)[0], f"membership differs away from faces in cell {c}: {p}"
+                flips += 1
+    assert dxi <= xi_tol, f"max |xi diff| {dxi} > {xi_tol}"
+    assert du <= u_tol, f"max |u diff| {du} > {u_tol}"
+    return {"dxi": dxi, "du": du, "flip_cells": len(bad_cells), "flips": flips,
+            "n_o": len(oc), "n_g": len(gc)}

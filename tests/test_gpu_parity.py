@@ -1,0 +1,240 @@
+"""Parity of the CUDA library (through the C ABI) against the FP64 oracle.
+
+Membership must match exactly except for particles within 1e-6 (FP64 path)
+or 2e-5 (mixed path, FP32 reference coordinates) of a cell face; floating
+point results are compared with the tolerances written in each test.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from pfem2_b200 import _abi as A
+from pfem2_b200 import cases
+from pfem2_b200.solver import Solver
+from tests.helpers import compare_particles, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PRECS = [A.PREC_FP64, A.PREC_MIXED]
+FACE_EPS = {A.PREC_FP64: 1e-6, A.PREC_MIXED: 2e-5}
+XI_TOL = {A.PREC_FP64: 1e-11, A.PREC_MIXED: 2e-5}
+
+
+def smooth_field(X, scale=1.0):
+    x, y = X[:, 0], X[:, 1]
+    ux = scale * (1.0 + 0.4 * np.sin(2.9 * y + 0.3) * np.cos(1.7 * x))
+    uy = scale * (0.35 * np.cos(2.3 * x - 0.2) * np.sin(1.1 * y + 0.5))
+    if X.shape[1] == 3:
+        z = X[:, 2]
+        uz = scale * 0.3 * np.sin(1.9 * x + 2.1 * z)
+        return [ux, uy, uz]
+    return [ux, uy]
+
+
+def spec_2d(dt=0.03, **kw):
+    sp = cases.poiseuille_2d(nx=32, ny=12, **kw)
+    sp.case.dt = dt
+    sp.case.vel_tol = 1e-11
+    sp.case.p_tol = 1e-11
+    return sp
+
+
+def spec_3d(dt=0.02, **kw):
+    sp = cases.pipe_3d(ny=6, nz=6, nx=12, **kw)
+    sp.case.dt = dt
+    sp.case.vel_tol = 1e-11
+    sp.case.p_tol = 1e-11
+    return sp
+
+
+def make_pair(sp, prec, **kw):
+    g = Solver(sp, precision=prec, **kw)
+    o = O.Oracle(sp.mesh, sp.case, movement_steps=kw.get("movement_steps", sp.movement_steps),
+                 max_per_part=kw.get("max_per_part", sp.max_per_part))
+    return g, o
+
+
+def set_vel(g, o, sp, fields, old=None):
+    dim = sp.mesh.dim
+    for d in range(dim):
+        g.set_field(A.FIELD_VX + d, fields[d])
+        o.set_field(A.FIELD_VX + d, fields[d])
+        ov = old[d] if old is not None else np.zeros_like(fields[d])
+        g.set_field(A.FIELD_OLD_VX + d, ov)
+        o.set_field(A.FIELD_OLD_VX + d, ov)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("dim", [2, 3])
+def test_seed(prec, dim):
+    sp = spec_2d() if dim == 2 else spec_3d()
+    g, o = make_pair(sp, prec)
+    f = smooth_field(sp.mesh.vertices)
+    set_vel(g, o, sp, f)
+    q = (4, 4) if dim == 2 else (3, 3, 3)
+    g.seed_particles(q, seed=7, jitter=0.1)
+    o.seed_particles(q, seed=7, jitter=0.1)
+    gc, gx, gu = g.particles()
+    oc, ox, ou = o.particles()
+    assert np.array_equal(gc, oc)
+    tol = 1e-14 if prec == A.PREC_FP64 else 1e-6
+    assert np.abs(gx - ox).max() <= tol
+    assert np.abs(gu - ou).max() <= tol * 4
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("dim", [2, 3])
+def test_correct(prec, dim):
+    sp = spec_2d() if dim == 2 else spec_3d()
+    g, o = make_pair(sp, prec)
+    X = sp.mesh.vertices
+    f0 = smooth_field(X)
+    set_vel(g, o, sp, f0)
+    q = (4, 4) if dim == 2 else (3, 3, 3)
+    g.seed_particles(q, seed=3, jitter=0.1)
+    o.seed_particles(q, seed=3, jitter=0.1)
+    f1 = smooth_field(X[:, ::-1] if dim == 2 else X[:, [2, 0, 1]], 0.7)
+    set_vel(g, o, sp, f1, old=f0)
+    g.correct_particles_velocities()
+    o.correct_particles_velocities()
+    gc, gx, gu = g.particles()
+    oc, ox, ou = o.particles()
+    assert np.array_equal(gc, oc)
+    tol = 1e-13 if prec == A.PREC_FP64 else 2e-6
+    assert np.abs(gu - ou).max() <= tol
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("check", [False, True])
+def test_move(prec, dim, check):
+    """advection with point location (and check_cell_for_empty_parts)."""
+    sp = spec_2d(dt=0.03) if dim == 2 else spec_3d(dt=0.015)
+    g, o = make_pair(sp, prec)
+    X = sp.mesh.vertices
+    f = smooth_field(X)
+    set_vel(g, o, sp, f)
+    q = (4, 4) if dim == 2 else (3, 3, 3)
+    g.seed_particles(q, seed=11, jitter=0.1)
+    o.seed_particles(q, seed=11, jitter=0.1)
+    for _ in range(3):
+        if check:
+            g.move_particles()
+            o.move_particles()
+        else:
+            g.advect()
+            o.advect()
+    r = compare_particles(o.particles(), g.particles(), FACE_EPS[prec], XI_TOL[prec],
+                          1e-12 if prec == A.PREC_FP64 else 1e-5)
+    gs, os_ = g.stats(), o.stats()
+    if prec == A.PREC_FP64:
+        assert r["flips"] == 0
+        assert gs["deleted"] == os_["deleted"]
+        if check:
+            assert gs["removed"] == os_["removed"] and gs["reseeded"] == os_["reseeded"]
+    assert gs["far"] == 0
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("dim", [2, 3])
+def test_project(prec, dim):
+    sp = spec_2d() if dim == 2 else spec_3d()
+    g, o = make_pair(sp, prec)
+    X = sp.mesh.vertices
+    f = smooth_field(X)
+    set_vel(g, o, sp, f)
+    q = (4, 4) if dim == 2 else (3, 3, 3)
+    g.seed_particles(q, seed=5, jitter=0.1)
+    o.seed_particles(q, seed=5, jitter=0.1)
+    g.distribute_particle_velocities_to_grid()
+    o.distribute_particle_velocities_to_grid()
+    tol = 1e-13 if prec == A.PREC_FP64 else 3e-7
+    for d in range(dim):
+        assert rel_l2(g.field(A.FIELD_VX + d), o.field(A.FIELD_VX + d)) <= tol
+    assert rel_l2(g.field(A.FIELD_NODE_WEIGHT), o.field(A.FIELD_NODE_WEIGHT)) <= tol
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("dim", [2, 3])
+def test_fem_step(prec, dim):
+    """prediction, pressure Poisson and correction solves from the same state."""
+    sp = spec_2d(dt=0.005) if dim == 2 else spec_3d(dt=0.002)
+    g, o = make_pair(sp, prec)
+    X = sp.mesh.vertices
+    f = smooth_field(X, 0.5)
+    set_vel(g, o, sp, f)
+    g.fem_step()
+    o.fem_step(1)
+    # FP64: both solve to an absolute residual of 1e-11; mixed: FP32 assembly
+    tol = {A.PREC_FP64: 1e-8, A.PREC_MIXED: 2e-5}[prec]
+    for fld in [A.FIELD_PRED_VX + d for d in range(dim)] + [A.FIELD_P] + [A.FIELD_VX + d for d in range(dim)]:
+        e = rel_l2(g.field(fld), o.field(fld))
+        assert e <= tol, (fld, e)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_steps_2d(prec):
+    """three whole time steps (correct, move, project, FEM) from seeding."""
+    sp = spec_2d(dt=0.01)
+    g, o = make_pair(sp, prec)
+    g.seed_particles(sp.q, seed=0, jitter=0.1)
+    o.seed_particles(sp.q, seed=0, jitter=0.1)
+    for _ in range(3):
+        g.step()
+        o.step(1)
+    tol = {A.PREC_FP64: 1e-8, A.PREC_MIXED: 1e-4}[prec]
+    for fld in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P):
+        e = rel_l2(g.field(fld), o.field(fld))
+        assert e <= tol, (fld, e)
+
+
+def test_fused_step_equals_member_calls():
+    """pfem2_step (fused kernels, CUDA graph) == the separate member calls, bit for bit."""
+    sp = spec_2d(dt=0.01)
+    a = Solver(sp, precision=A.PREC_FP64, use_graph=True)
+    b = Solver(sp, precision=A.PREC_FP64, use_graph=False)
+    for s in (a, b):
+        s.seed_particles(sp.q, seed=0, jitter=0.1)
+    for _ in range(3):
+        a.step()
+        b.correct_particles_velocities()
+        b.move_particles()
+        b.distribute_particle_velocities_to_grid()
+        b.fem_step()
+    for fld in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P):
+        assert np.array_equal(a.field(fld), b.field(fld))
+    ca, xa, ua = a.particles()
+    cb, xb, ub = b.particles()
+    assert np.array_equal(ca, cb) and np.array_equal(xa, xb) and np.array_equal(ua, ub)
+
+
+def test_batched_equals_single():
+    """two instances in one batch give the same bits as each instance alone."""
+    s1 = spec_2d(dt=0.01)
+    s2 = cases.poiseuille_2d(nx=20, ny=8)
+    s2.case.dt = 0.008
+    s2.case.vel_tol = s2.case.p_tol = 1e-11
+    both = Solver([s1, s2], precision=A.PREC_MIXED)
+    one = Solver(s1, precision=A.PREC_MIXED)
+    two = Solver(s2, precision=A.PREC_MIXED)
+    for s in (both, one, two):
+        s.seed_particles((4, 4), seed=0, jitter=0.1)
+    for _ in range(2):
+        for s in (both, one, two):
+            s.step()
+    for fld in (A.FIELD_VX, A.FIELD_P):
+        assert np.array_equal(both.field(fld, 0), one.field(fld, 0))
+        assert np.array_equal(both.field(fld, 1), two.field(fld, 0))
+
+
+def test_deterministic():
+    sp = spec_2d(dt=0.01)
+    outs = []
+    for _ in range(2):
+        s = Solver(sp, precision=A.PREC_MIXED)
+        s.seed_particles(sp.q, seed=0, jitter=0.1)
+        for _ in range(3):
+            s.step()
+        outs.append([s.field(f) for f in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P)])
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
