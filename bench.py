@@ -1,0 +1,360 @@
+"""Benchmark of the PFEM2 time step on B200 (one JSON line on rank 0).
+
+Workload (default): the 2D channel with a disk obstacle, ~52k Q1 cells,
+25 particles per cell (~1.3M particles), Re=100, dt=0.002: one `step` is one
+whole PFEM2 time step (correct -> move/locate/reseed -> project -> fractional
+-step FEM with the three Krylov solves) of the mixed-precision path, inputs
+resident in HBM. The FP64 path runs the same steps for the mixed-vs-FP64
+comparison and its field error.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: a single mesh does not shard, so N ranks run N independent
+replicas of the instance (weak scaling, no data-path collective); value is
+the sum of the ranks' instance-timesteps/s over the max-over-ranks time.
+
+--impl reference times the FP64 CPU restatement of the reference algorithm
+(oracle/, OpenMP over the host cores) on a bounded sample of the same
+workload; deal.II (the reference's own dependency) is not installed here.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--h", type=float, default=0.0088, help="cell size of the channel mesh (~52k cells)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(args):
+    from pfem2_b200 import cases
+
+    sp = cases.channel_disk(h=args.h)
+    return sp
+
+
+WORKLOAD_DESC = {
+    "workload": "2D channel [0,4]x[0,1] with disk r=0.1 at (0.5,0.5), O-grid+blocks Q1 mesh, "
+                "parabolic inflow Umax=1.5, Re=100, dt=0.002, 5x5 particles/cell",
+}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names[1:], parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def pressure_solve_bytes(s, iters, outer):
+    """Algorithmic bytes of the pressure solves, per the model in DESIGN.md:
+    inner CG iteration (FP32 inner type for the mixed path):
+        SELL SpMV  nnz*(val+col) + n*(x + y)
+        vectors    p = z + beta p (3 n), e += alpha p (3 n), r -= alpha q (3 n), z = D^-1 r (3 n)
+    FP64 refinement sweep: nnz*(8+4) + n*(x64 + e + b + r64) bytes."""
+    info = s.sizes()
+    n, nnz, rb = info["rows"], info["nnz"], info["real_bytes"]
+    inner = nnz * (rb + 4) + n * 2 * rb + 12 * n * rb
+    outerb = nnz * 12 + n * (8 + rb + 8 + 8)
+    return iters * inner + outer * outerb
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from pfem2_b200 import _abi as A
+    from pfem2_b200.solver import STAGE_NAMES, Solver
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    sp = workload(args)
+    s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True)
+    s.seed_particles(sp.q, sp.seed, sp.jitter)
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        s.step()
+    s.synchronize()
+    s.enable_stage_timing(True)
+    s.stage_times(reset=True)
+    it_p = 0
+    outer_p = 0
+    np_sum = 0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    l0 = s.launch_count()
+    clocks = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # > L2: every step starts cold (outside the timed events)
+        ev[k][0].record(stream)
+        s.step()
+        ev[k][1].record(stream)
+        st = s.stats()
+        it_p += st["iters"][3]
+        outer_p += st["refinements_p"]
+        np_sum += st["n_particles"]
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = s.launch_count() - l0
+    ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    stages = s.stage_times()
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_per_s = args.steps / (ms / 1e3)
+    value = steps_per_s * world
+    pupd = np_sum / (ms / 1e3) * world
+
+    # roofline: the pressure solve (dominant kernel), bytes from the live iteration counts
+    hbm, peak_kind = peaks()
+    ps_ms = stages[STAGE_NAMES.index("pressure_solve")]
+    ps_bytes = pressure_solve_bytes(s, it_p, outer_p)
+    achieved = ps_bytes / (ps_ms / 1e3) / 1e9 if ps_ms > 0 else None
+    s.enable_stage_timing(False)
+
+    # e2e: the same steps through the C ABI with a host read of the loads and
+    # of the Vx, Vy, P fields every step (pfem2_step_and_read)
+    fields = (A.FIELD_VX, A.FIELD_VY, A.FIELD_P)
+    loads = np.zeros(5)
+    out = np.zeros(sp.mesh.n_vertices * len(fields))
+    s.step_and_read(fields, loads, out)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.step_and_read(fields, loads, out)
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": args.steps / e2e_s * world, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
+           "d2h_bytes_per_step": int(out.nbytes + loads.nbytes)}
+
+    # FP64 leg on the same workload: its speed and the mixed-vs-FP64 field error
+    fp64 = None
+    if not args.no_fp64:
+        s64 = Solver(sp, precision=A.PREC_FP64, device=local, use_graph=True)
+        m2 = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True)
+        s64.seed_particles(sp.q, sp.seed, sp.jitter)
+        m2.seed_particles(sp.q, sp.seed, sp.jitter)
+        nst = args.warmup + args.steps
+        for _ in range(args.warmup):
+            s64.step()
+            m2.step()
+        st64 = torch.cuda.ExternalStream(s64.stream(), device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms64 = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(st64):
+                flush.zero_()
+            e0.record(st64)
+            s64.step()
+            e1.record(st64)
+            e1.synchronize()
+            ms64 += e0.elapsed_time(e1)
+            m2.step()
+        errs = {}
+        for name, f in (("vx", A.FIELD_VX), ("vy", A.FIELD_VY), ("p", A.FIELD_P)):
+            a, b = m2.field(f), s64.field(f)
+            errs[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        fp64 = {"timesteps_per_s": args.steps / (ms64 / 1e3), "steps_compared": nst,
+                "mixed_vs_fp64_rel_l2": errs}
+        s64.close()
+        m2.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sp, threads=1, budget_s=20.0)
+
+    res = {
+        "metric": "timesteps/s (mixed-precision PFEM2 step; particle updates/s and FP64 leg alongside)",
+        "value": value,
+        "unit": "timesteps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 particles/assembly/inner Krylov + f64 refinement",
+        "data": "synthetic (programmatic mesh, seeded particles)",
+        "config": dict(WORKLOAD_DESC, cells=sp.mesh.n_cells, vertices=sp.mesh.n_vertices,
+                       particles=int(np_sum / args.steps), l2="flushed between timed steps (256 MB write)",
+                       parallelism=f"replicas x{world}" if world > 1 else "single instance"),
+        "particle_updates_per_s": pupd,
+        "stage_ms_per_step": {n: stages[i] / args.steps for i, n in enumerate(STAGE_NAMES)},
+        "pressure_cg_iters_per_step": it_p / args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_krylov<float> (pressure solve)",
+                     "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None,
+                     "traffic": None, "algorithmic_bytes_per_step": ps_bytes / args.steps},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "fp64": fp64,
+        "cpu_baseline": cpu,
+    }
+    s.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+def cpu_baseline(sp, threads, budget_s):
+    """FP64 CPU restatement of the reference (oracle/) on the same workload:
+    time whole steps until the budget is used (>= 1 step)."""
+    import oracle as O
+
+    o = O.Oracle(sp.mesh, sp.case, movement_steps=sp.movement_steps, max_per_part=sp.max_per_part,
+                 threads=threads)
+    o.seed_particles(sp.q, sp.seed, sp.jitter)
+    o.step(1)  # warm-up step (first-touch, assembly)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or n >= 50:
+            break
+    return {"value": n / el, "unit": "timesteps/s", "cores": threads, "kind": "port",
+            "sample": f"{n} whole time steps of the same workload after 1 warm-up step, FP64, "
+                      f"{threads} thread(s)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sp = workload(args)
+    threads = os.cpu_count() or 1
+    import oracle as O
+
+    o = O.Oracle(sp.mesh, sp.case, movement_steps=sp.movement_steps, max_per_part=sp.max_per_part,
+                 threads=threads)
+    o.seed_particles(sp.q, sp.seed, sp.jitter)
+    for _ in range(max(1, min(args.warmup, 2))):
+        o.step(1)
+    budget = 120.0
+    n = 0
+    t0 = time.perf_counter()
+    while n < args.steps:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    v = n / el
+    res = {
+        "impl": "reference",
+        "metric": "timesteps/s (mixed-precision PFEM2 step; particle updates/s and FP64 leg alongside)",
+        "value": v, "unit": "timesteps/s", "n_gpus": world, "steps": n, "warmup": args.warmup,
+        "ms_per_step": el / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (programmatic mesh, seeded particles)",
+        "config": dict(WORKLOAD_DESC, cells=sp.mesh.n_cells, parallelism="host cores"),
+        "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} whole time steps (of {args.steps} requested, 120 s cap) after "
+                                   f"{max(1, min(args.warmup, 2))} warm-up steps; deal.II, which the "
+                                   f"reference needs, is not installed, so its FP64 CPU restatement runs"},
+        "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(res), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_info()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -221,10 +221,14 @@ pfem2_status pfem2_get_time(pfem2_ctx* ctx, double* time, int32_t* timestep_numb
 pfem2_status pfem2_synchronize(pfem2_ctx* ctx);
 /* Device kernel launches issued by this context so far (for accounting). */
 pfem2_status pfem2_launch_count(pfem2_ctx* ctx, int64_t* n);
-/* Device time (ms) of named stages accumulated since the last reset: stage
- * 0 correct+move, 1 rebin/check, 2 project, 3 assembly, 4 solves, 5 loads. */
-pfem2_status pfem2_stage_times(pfem2_ctx* ctx, double* ms6, int32_t reset);
-/* Enable per-stage CUDA-event timing (off by default; costs a few events/step). */
+/* Device time (ms) of the stages of pfem2_step accumulated since the last
+ * reset (PFEM2_N_STAGES values): 0 correct+advect+locate, 1 rebin (re-sort,
+ * check_cell_for_empty_parts, projection partials), 2 projection node gather,
+ * 3 prediction rhs + solves, 4 pressure rhs, 5 pressure solve, 6 correction
+ * rhs + solves + update. Needs pfem2_enable_stage_timing; synchronizes. */
+#define PFEM2_N_STAGES 7
+pfem2_status pfem2_stage_times(pfem2_ctx* ctx, double* ms, int32_t reset);
+/* Enable per-stage CUDA-event timing of pfem2_step (off by default). */
 pfem2_status pfem2_enable_stage_timing(pfem2_ctx* ctx, int32_t on);
 /* The CUDA stream (cudaStream_t) all work of the context is issued on. */
 pfem2_status pfem2_get_stream(pfem2_ctx* ctx, void** stream);

@@ -330,6 +330,7 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(krylov_setup(c));
   PFEM2_TRY(assemble_matrices(c));
   PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  PFEM2_TRY(krylov_setup_precond(c));
   PFEM2_CUDA(cudaGetLastError());
   c.setup_done = true;
   return PFEM2_OK;
@@ -384,6 +385,12 @@ static pfem2_status check_counters(Ctx& c, bool sync) {
 }
 
 // ------------------------------------------------------------ FEM step
+// stage boundary event; external so that it becomes a timing node when the
+// step is being captured into a CUDA graph
+static void mark(Ctx& c, int k) {
+  if (c.timing) cudaEventRecordWithFlags(c.ev[k], c.stream, cudaEventRecordExternal);
+}
+
 static pfem2_status fem_step_launch(Ctx& c) {
   for (int d = 0; d < c.dim; ++d)
     PFEM2_CUDA(cudaMemcpyAsync(c.F[PFEM2_FIELD_OLD_VX + d], c.F[PFEM2_FIELD_VX + d], sizeof(double) * c.nv,
@@ -395,20 +402,41 @@ static pfem2_status fem_step_launch(Ctx& c) {
   for (int oc = 0; oc < nouter; ++oc) {
     PFEM2_TRY(launch_rhs_prediction(c));
     PFEM2_TRY(krylov_solve(c, 0));
+    if (oc == nouter - 1) mark(c, 4);
     PFEM2_TRY(launch_rhs_pressure(c));
+    if (oc == nouter - 1) mark(c, 5);
     PFEM2_TRY(krylov_solve(c, 1));
+    if (oc == nouter - 1) mark(c, 6);
     PFEM2_TRY(launch_rhs_correction(c));
     PFEM2_TRY(krylov_solve(c, 2));
     PFEM2_TRY(launch_finish_fem(c));
   }
+  mark(c, 7);
   return PFEM2_OK;
 }
 
 static pfem2_status step_launch(Ctx& c) {
+  mark(c, 0);
   PFEM2_TRY(launch_advect(c, true));
+  mark(c, 1);
   PFEM2_TRY(launch_rebin(c, true, true, true));
+  mark(c, 2);
   PFEM2_TRY(launch_project(c, true));
+  mark(c, 3);
   PFEM2_TRY(fem_step_launch(c));
+  return PFEM2_OK;
+}
+
+// folds the events of the last timed step into stage_ms
+static pfem2_status collect_stage_times(Ctx& c) {
+  if (!c.ev_pending) return PFEM2_OK;
+  PFEM2_CUDA(cudaEventSynchronize(c.ev[7]));
+  for (int k = 0; k < PFEM2_N_STAGES; ++k) {
+    float ms = 0.f;
+    PFEM2_CUDA(cudaEventElapsedTime(&ms, c.ev[k], c.ev[k + 1]));
+    c.stage_ms[k] += ms;
+  }
+  c.ev_pending = false;
   return PFEM2_OK;
 }
 
@@ -664,7 +692,9 @@ static pfem2_status run_step(pfem2_ctx* x) {
 pfem2_status pfem2_step(pfem2_ctx* x) {
   SEED_CHECK(x);
   Ctx& c = x->c;
+  if (c.timing) PFEM2_TRY(collect_stage_times(c));
   PFEM2_TRY(run_step(x));
+  c.ev_pending = c.timing;
   c.time += c.inst[0].cs.dt;
   c.timestep += 1;
   PFEM2_CUDA(cudaGetLastError());
@@ -837,15 +867,22 @@ pfem2_status pfem2_launch_count(pfem2_ctx* x, int64_t* n) {
   return PFEM2_OK;
 }
 
-pfem2_status pfem2_stage_times(pfem2_ctx* x, double* ms6, int32_t reset) {
+pfem2_status pfem2_stage_times(pfem2_ctx* x, double* ms, int32_t reset) {
   CTX_CHECK(x);
-  if (ms6) std::memcpy(ms6, x->c.stage_ms, sizeof(double) * 6);
+  PFEM2_TRY(collect_stage_times(x->c));
+  if (ms) std::memcpy(ms, x->c.stage_ms, sizeof(double) * PFEM2_N_STAGES);
   if (reset) std::memset(x->c.stage_ms, 0, sizeof(x->c.stage_ms));
   return PFEM2_OK;
 }
 
 pfem2_status pfem2_enable_stage_timing(pfem2_ctx* x, int32_t on) {
   CTX_CHECK(x);
+  PFEM2_TRY(collect_stage_times(x->c));
+  if ((on != 0) != x->c.timing) {
+    // the captured graphs contain (or lack) the event records: recapture
+    for (int k = 0; k < 2; ++k)
+      if (x->graph[k]) { cudaGraphExecDestroy(x->graph[k]); x->graph[k] = nullptr; }
+  }
   x->c.timing = on != 0;
   return PFEM2_OK;
 }

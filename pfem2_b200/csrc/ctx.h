@@ -127,7 +127,7 @@ struct Ctx {
   size_t kws_bytes = 0;
   Tile* d_tiles[2] = {};      // [0] 1 component phase, [1] dim component phase
   int ntiles[2] = {};
-  int tile_slices = 8;
+  int tile_slices = 0;         // Krylov tile size in slices (0 = automatic)
   double* sys_scalars = nullptr;
   double* tile_part = nullptr;
   int* d_sysinfo = nullptr;
@@ -135,13 +135,17 @@ struct Ctx {
   int* d_err = nullptr;
   int coop_blocks = 0;
   int solve_threads = 256;
+  int solve_blocks_per_sm = 1;  // persistent Krylov grid: blocks per SM
+  bool two_level = true;        // pressure: block-Jacobi(32) + coarse correction
+  double refine_eta = 1e-3;     // mixed: inner residual reduction per FP64 refinement
 
   // graph
   cudaGraphExec_t graph = nullptr;
   bool graph_valid = false;
   bool timing = false;
   cudaEvent_t ev[8] = {};
-  double stage_ms[6] = {};
+  double stage_ms[PFEM2_N_STAGES] = {};
+  bool ev_pending = false;
 
   pfem2_stats stats{};
 };
@@ -195,6 +199,7 @@ pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev);
 
 // krylov.cu
 pfem2_status krylov_setup(Ctx& c);
+pfem2_status krylov_setup_precond(Ctx& c);
 // which: 0 prediction (dim systems per instance), 1 pressure, 2 correction
 pfem2_status krylov_solve(Ctx& c, int which);
 pfem2_status krylov_read_stats(Ctx& c);

@@ -1,26 +1,40 @@
-// krylov.cu -- batched, persistent preconditioned CG with FP64 iterative
-// refinement on the SELL-32 pattern (sm_100a).
+// krylov.cu -- batched, persistent preconditioned CG with FP64 reliable
+// updates on the SELL-32 pattern (sm_100a).
 //
-// One cooperative launch solves every system of a phase (components x
+// One cooperative launch solves every system of a solve phase (components x
 // instances) to the reference's stopping rule: the absolute 2-norm of the
-// unpreconditioned residual b - A x <= tol, at most max_iter iterations
-// (deal.II SolverControl, cylinder2D/cylinder2D.cc:736-779). The reference
-// runs BiCGStab + Jacobi/SSOR; the velocity, mass and pressure matrices
-// here are symmetric positive definite after symmetric Dirichlet
-// elimination, so CG reaches the same fixed point with one SpMV per step.
+// unpreconditioned residual b - A x <= tol within max_iter iterations
+// (deal.II SolverControl(max_iter, tol), cylinder2D/cylinder2D.cc:736-779).
+// The reference runs BiCGStab with Jacobi (velocity) / SSOR (pressure); the
+// prediction, mass and Poisson matrices here are symmetric positive definite
+// after the symmetric Dirichlet elimination, so CG reaches the same solution.
 //
-// Per system a small state machine runs:
-//   OUTER  r64 = b - A64 (x + e) in FP64, res = ||r64||; x += e, e = 0;
-//          done when res <= tol, otherwise start an inner solve
-//   INNER  Jacobi-PCG on A_in e = r in the inner type R (FP32 for the mixed
-//          path, FP64 for the plain path), FP64 dot products; back to OUTER
-//          once ||r_inner|| <= max(eta * res, tol / 2)
-// Each iteration is two phases separated by a bounded grid barrier:
-//   A  p' = z + beta p ; q = A (z + beta p)   (p double-buffered)   | pq
-//   B  e += alpha p' ; r -= alpha q ; z = D^-1 r                    | rz, rr
-// Tile partials are reduced by the last block to finish a system's tiles
-// (threadfence + counter), in a fixed order, so results are deterministic.
+// Each CG iteration is two phases separated by a bounded grid barrier:
+//   A  p' = z + beta p ; q = A (z + beta p)     (p double buffered)  | (p', q)
+//   B  e += alpha p' ; r -= alpha q ; z = M^-1 r                    | (r, z), (r, r), sum r
+// Every block that owns tiles of a system computes that system's scalars
+// itself, from the per-tile partial sums of the previous phase, in a fixed
+// order: no block publishes scalars and no phase waits for a finalizer.
+//
+// Preconditioners: Jacobi for the prediction and mass systems; for the
+// pressure Poisson system an additive two-level preconditioner
+//   M^-1 = B^-1 + Z E^-1 Z^T,
+// B = the 32x32 diagonal blocks of A (one SELL slice = one warp, inverted at
+// setup, applied with warp shuffles), Z = indicator vectors of the tiles of
+// the system (contiguous runs of slices), E = Z^T A Z (inverted at setup,
+// FP32 copy in shared memory). The coarse part needs the tile sums of r,
+// which are partials of phase B anyway, so it is applied on the fly in
+// phase A (z_i = (B^-1 r)_i + y_tile(i), y = E^-1 Z^T r) and costs no
+// extra barrier.
+//
+// The iterate is split x + e: e accumulates in the inner type R (FP32 for
+// the mixed path, FP64 for the plain path); once the recurrence residual
+// has dropped below max(eta * res, tol / 2) a reliable update runs in FP64
+// (phase A: r64 = b - A64 (x + e); phase B: x += e, e = 0, r = r64) and CG
+// restarts from the true residual. A system is done when the FP64 residual
+// is <= tol.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <vector>
 
@@ -29,162 +43,137 @@
 
 namespace pfem2 {
 
-constexpr int kSolveThreads = 256;  // 8 warps, one SELL slice each per tile
+constexpr int kSolveThreads = 256;  // 8 warps
+constexpr int kWarps = kSolveThreads / 32;
+constexpr int kMaxLocalSys = 16;
 
-enum { ST_INNER = 0, ST_OUTER = 1, ST_DONE = 2 };
-enum { SD_RHO = 0, SD_ALPHA, SD_BETA, SD_RES, SD_INTOL, SD_RR, SD_TOL, SD_N };
-enum { SI_STATE = 0, SI_IT, SI_PAR, SI_DONEFLAG, SI_OUTER, SI_MAXIT, SI_N };
+// system states (A states act in even iterations, B states in odd ones)
+enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4 };
+// actions
+enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5 };
 
 template <typename R> struct SolveArgs {
   int ncomp, ninst, nsys, ntiles, nv;
   const Tile* tiles;
-  const int* sys_t0;  // [nsys+1] first tile of each system
+  const int* sys_t0;     // [nsys+1] first tile of each system
+  const int* blk_t0;     // [grid+1] first tile of each block
   const int* sl_ptr;
   const int* sl_len;
   const int* sl_col;
   const double* A64[3];
   const R* Ain[3];
   const R* dinv[3];
+  // two-level data (pressure phase)
+  const R* Binv;         // [nslices][32 cols][32 rows]
+  const float* Einv;     // per system D_s x D_s (symmetric), at sys_eoff[s]
+  const int* sys_eoff;
+  const int* sys_D;      // coarse size = tiles of the system
+  const int* sys_sl0;    // first slice of the system
+  const int* sys_sps;    // slices per tile (= per coarse subdomain)
+  int dmax;              // max D over systems (smem stride)
   double* x[3];
   const double* b[3];
   const unsigned char* isd[3];
-  const double* g[3];   // Dirichlet values to preset in x (nullptr -> 0)
-  // workspace per component slot: nv entries each
+  const double* g[3];    // Dirichlet values preset in x (nullptr -> 0)
+  const double* tol_i;   // per instance
+  const int* maxit_i;    // per instance
+  // workspace per component slot, nv entries each
+  R *e, *r, *z, *p, *q;  // p: 2 buffers; z = B^-1 r (two-level) or D^-1 r
   double* r64;
-  R* e;
-  R* r;
-  R* z;
-  R* p;   // 2*ncomp*nv
-  R* q;
-  double* part;  // [ntiles][2]
-  int* cnt;      // [nsys] finished-tile counters
-  double* sd;    // [nsys][SD_N]
-  int* si;       // [nsys][SI_N]
-  int* active;   // number of unfinished systems
+  double* part;          // [2][ntiles][3], by iteration parity
+  int* active;
+  int* out_it;           // [nsys] iterations
+  double* out_res;       // [nsys] final residual norm
+  int* out_outer;        // [nsys] FP64 residual evaluations
   double eta;
-  int iter_cap;  // hard bound on the global iteration count
+  int iter_cap;
   GridBarrier gb;
 };
 
-// deterministic block reduction of up to 2 doubles (fixed order)
-template <int NK>
-__device__ __forceinline__ void block_reduce_store(double (&v)[NK], double* out) {
-  __shared__ double red[kSolveThreads / 32][2];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int k = 0; k < NK; ++k) v[k] = warp_sum(v[k]);
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < NK; ++k) red[warp][k] = v[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NK; ++k) {
-      double s = 0.0;
-      for (int w = 0; w < kSolveThreads / 32; ++w) s += red[w][k];
-      out[k] = s;
-    }
-  }
-  __syncthreads();
-}
-
-// sum of the partials of system s (whole block, fixed order)
-__device__ __forceinline__ void system_sum(const double* part, int t0, int t1, int nk, double* res) {
-  __shared__ double red[kSolveThreads][2];
-  double a0 = 0.0, a1 = 0.0;
-  for (int t = t0 + threadIdx.x; t < t1; t += kSolveThreads) {
-    a0 += __ldcg(part + (size_t)t * 2);
-    if (nk > 1) a1 += __ldcg(part + (size_t)t * 2 + 1);
-  }
-  red[threadIdx.x][0] = a0;
-  red[threadIdx.x][1] = a1;
-  __syncthreads();
-  for (int s = kSolveThreads / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      red[threadIdx.x][0] += red[threadIdx.x + s][0];
-      red[threadIdx.x][1] += red[threadIdx.x + s][1];
-    }
-    __syncthreads();
-  }
-  res[0] = red[0][0];
-  res[1] = red[0][1];
-  __syncthreads();
-}
-
-// called by all threads of the block after it finished its tiles of system s
-// in the current phase (ntouched of them); the last contributor finalizes.
-template <typename R, int PHASE>
-__device__ void contribute(const SolveArgs<R>& a, int s, int ntouched) {
-  __shared__ int s_last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const int t0 = a.sys_t0[s], t1 = a.sys_t0[s + 1];
-    int old = atomicAdd(a.cnt + s, ntouched);
-    s_last = (old + ntouched == t1 - t0);
-    if (s_last) {
-      a.cnt[s] = 0;
-      __threadfence();
-    }
-  }
-  __syncthreads();
-  if (!s_last) return;
+struct LocalSys {
+  int sys, state, it, outer, par, first, owner, maxit, act;
+  int D, sl0, sps;
+  double tol, intol, res, rz_prev, alpha, beta, rzc;
   double sum[2];
-  system_sum(a.part, a.sys_t0[s], a.sys_t0[s + 1], PHASE == 0 ? 1 : 2, sum);
-  if (threadIdx.x == 0) {
-    volatile double* sd = a.sd + (size_t)s * SD_N;
-    volatile int* si = a.si + (size_t)s * SI_N;
-    const int st = si[SI_STATE];
-    if (PHASE == 0) {
-      if (st == ST_OUTER) {
-        const double res = sqrt(sum[0]);
-        sd[SD_RES] = res;
-        const bool conv = res <= sd[SD_TOL];
-        const bool out_of_its = si[SI_IT] >= si[SI_MAXIT];
-        si[SI_DONEFLAG] = (conv || out_of_its) ? 1 : 0;
-        sd[SD_INTOL] = fmax(a.eta * res, 0.5 * sd[SD_TOL]);
-        si[SI_OUTER] += 1;
-      } else if (st == ST_INNER) {
-        sd[SD_ALPHA] = sum[0] != 0.0 ? sd[SD_RHO] / sum[0] : 0.0;
-      }
-    } else {
-      if (st == ST_OUTER) {
-        if (si[SI_DONEFLAG]) {
-          si[SI_STATE] = ST_DONE;
-          atomicSub(a.active, 1);
-        } else {
-          sd[SD_RHO] = sum[0];
-          sd[SD_RR] = sqrt(sum[1]);
-          sd[SD_BETA] = 0.0;
-          si[SI_STATE] = ST_INNER;
-        }
-      } else if (st == ST_INNER) {
-        si[SI_IT] += 1;
-        const double rr = sqrt(sum[1]);
-        sd[SD_RR] = rr;
-        if (rr <= sd[SD_INTOL] || si[SI_IT] >= si[SI_MAXIT] || !(rr == rr)) {
-          si[SI_STATE] = ST_OUTER;
-        } else {
-          sd[SD_BETA] = sd[SD_RHO] != 0.0 ? sum[0] / sd[SD_RHO] : 0.0;
-          sd[SD_RHO] = sum[0];
-          si[SI_PAR] ^= 1;
-        }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
+};
+
+// z = B^-1 r on one SELL slice: lane i holds r_i, returns z_i
+template <typename R>
+__device__ __forceinline__ R block_jacobi32(const R* __restrict__ Binv, int slice, R ri, int lane) {
+  const R* B = Binv + (size_t)slice * 1024;
+  R acc = R(0);
+#pragma unroll 8
+  for (int j = 0; j < 32; ++j) acc += B[j * 32 + lane] * __shfl_sync(PFEM2_FULL_MASK, ri, j);
+  return acc;
 }
 
-template <typename R>
+template <typename R, bool TWO>
 __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
+  extern __shared__ unsigned char dyn_smem[];
+  __shared__ LocalSys ls[kMaxLocalSys];
+  __shared__ double red[kWarps][2];
+  __shared__ int s_nls, s_sys0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t nv = (size_t)a.nv;
-  // ---- init: preset Dirichlet values, e = 0, p = 0
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+  const int t_lo = a.blk_t0[blockIdx.x], t_hi = a.blk_t0[blockIdx.x + 1];
+  // two-level shared memory: per local system E^-1 (dmax^2 floats), y and Z^T r (dmax doubles each)
+  float* sE = reinterpret_cast<float*>(dyn_smem);
+  const int nE = a.dmax * a.dmax;
+
+  // ---- local systems of this block
+  if (threadIdx.x == 0) {
+    int n = 0, s0 = -1;
+    if (t_hi > t_lo) {
+      s0 = a.tiles[t_lo].sys;
+      n = a.tiles[t_hi - 1].sys - s0 + 1;
+    }
+    if (n > kMaxLocalSys) n = kMaxLocalSys;  // the host guarantees n <= kMaxLocalSys
+    s_nls = n;
+    s_sys0 = s0;
+    for (int k = 0; k < n; ++k) {
+      LocalSys& L = ls[k];
+      const int s = s0 + k, inst = s % a.ninst;
+      L.sys = s;
+      L.state = S_OUT_A;
+      L.it = L.outer = L.par = 0;
+      L.first = 1;
+      L.owner = a.sys_t0[s] >= t_lo && a.sys_t0[s] < t_hi;
+      L.maxit = a.maxit_i[inst];
+      L.tol = a.tol_i[inst];
+      L.intol = 0.5 * L.tol;
+      L.res = L.rz_prev = L.alpha = L.beta = L.rzc = 0.0;
+      L.act = ACT_NONE;
+      if (TWO) {
+        L.D = a.sys_D[s];
+        L.sl0 = a.sys_sl0[s];
+        L.sps = a.sys_sps[s];
+      } else {
+        L.D = 0; L.sl0 = 0; L.sps = 1;
+      }
+    }
+  }
+  __syncthreads();
+  const int nls = s_nls, sys0 = s_sys0;
+  float* sEk[kMaxLocalSys];
+  double* sYk[kMaxLocalSys];
+  double* sSk[kMaxLocalSys];
+  if (TWO) {
+    double* ybase = reinterpret_cast<double*>(sE + (size_t)nls * nE + ((nls * nE) & 1));
+    for (int k = 0; k < nls; ++k) {
+      sEk[k] = sE + (size_t)k * nE;
+      sYk[k] = ybase + (size_t)k * 2 * a.dmax;
+      sSk[k] = sYk[k] + a.dmax;
+      const float* src = a.Einv + a.sys_eoff[ls[k].sys];
+      const int n2 = ls[k].D * ls[k].D;
+      for (int i = threadIdx.x; i < n2; i += kSolveThreads) sEk[k][i] = src[i];
+    }
+  }
+
+  // ---- init: Dirichlet values preset in x, e = 0, p = 0
+  for (int t = t_lo; t < t_hi; ++t) {
     const Tile T = a.tiles[t];
     const int k = T.comp;
-    for (int sl = T.s0 + warp; sl < T.s1; sl += kSolveThreads / 32) {
+    for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
       const int row = sl * 32 + lane;
       if (a.isd[k][row]) a.x[k][row] = a.g[k] ? a.g[k][row] : 0.0;
       a.e[k * nv + row] = R(0);
@@ -193,236 +182,502 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
     }
   }
   if (!grid_sync(a.gb)) return;
+
   for (int iter = 0;; ++iter) {
     if (*(volatile int*)a.active <= 0) break;
     if (iter >= a.iter_cap) {
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.gb.err, 2);
       break;
     }
-    // ------------------------------------------------------------ phase A
-    {
-      int cur_s = -1, touched = 0;
-      for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const Tile T = a.tiles[t];
-        if (T.sys != cur_s) {
-          if (cur_s >= 0) contribute<R, 0>(a, cur_s, touched);
-          cur_s = T.sys;
-          touched = 0;
+    const bool phaseA = (iter & 1) == 0;
+    const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 3;
+    // ---- sums of the previous phase's partials (warp 0, fixed order)
+    if (warp == 0) {
+      for (int k = 0; k < nls; ++k) {
+        const int st = ls[k].state;
+        if (st == S_DONE || st == S_OUT_A) continue;
+        const int t0 = a.sys_t0[ls[k].sys], t1 = a.sys_t0[ls[k].sys + 1];
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
+        for (int t = t0 + lane; t < t1; t += 32) {
+          s0 += __ldcg(prev + (size_t)t * 3);
+          s1 += __ldcg(prev + (size_t)t * 3 + 1);
         }
-        ++touched;
-        const int k = T.comp;
-        const int st = __ldcg(a.si + (size_t)T.sys * SI_N + SI_STATE);
-        double v[1] = {0.0};
-        if (st == ST_OUTER) {
-          const double* A = a.A64[k];
-          const double* xk = a.x[k];
-          const R* ek = a.e + k * nv;
-          for (int sl = T.s0 + warp; sl < T.s1; sl += kSolveThreads / 32) {
-            const int row = sl * 32 + lane;
-            const int base = a.sl_ptr[sl], len = a.sl_len[sl];
-            double s = 0.0;
-            for (int j = 0; j < len; ++j) {
-              const int ei = base + j * 32 + lane;
-              const int col = __ldg(a.sl_col + ei);
-              s += A[ei] * (__ldcg(xk + col) + (double)__ldcg(ek + col));
-            }
-            const double rr = a.b[k][row] - s;
-            a.r64[k * nv + row] = rr;
-            v[0] += rr * rr;
-          }
-        } else if (st == ST_INNER) {
-          const double* sd = a.sd + (size_t)T.sys * SD_N;
-          const R beta = R(__ldcg(sd + SD_BETA));
-          const int par = __ldcg(a.si + (size_t)T.sys * SI_N + SI_PAR);
-          const R* pold = a.p + (2 * k + (par ^ 1)) * nv;
-          R* pnew = a.p + (2 * k + par) * nv;
-          const R* zk = a.z + k * nv;
-          const R* A = a.Ain[k];
-          for (int sl = T.s0 + warp; sl < T.s1; sl += kSolveThreads / 32) {
-            const int row = sl * 32 + lane;
-            const int base = a.sl_ptr[sl], len = a.sl_len[sl];
-            R s = R(0);
-            if (beta != R(0)) {
-              for (int j = 0; j < len; ++j) {
-                const int ei = base + j * 32 + lane;
-                const int col = __ldg(a.sl_col + ei);
-                s += A[ei] * (__ldcg(zk + col) + beta * __ldcg(pold + col));
-              }
-            } else {
-              for (int j = 0; j < len; ++j) {
-                const int ei = base + j * 32 + lane;
-                s += A[ei] * __ldcg(zk + __ldg(a.sl_col + ei));
-              }
-            }
-            const R pn = beta != R(0) ? zk[row] + beta * pold[row] : zk[row];
-            pnew[row] = pn;
-            a.q[k * nv + row] = s;
-            v[0] += (double)pn * (double)s;
-          }
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        if (lane == 0) {
+          ls[k].sum[0] = s0;
+          ls[k].sum[1] = s1;
         }
-        double outv[1];
-        block_reduce_store<1>(v, outv);
-        if (threadIdx.x == 0) a.part[(size_t)t * 2] = outv[0];
       }
-      if (cur_s >= 0) contribute<R, 0>(a, cur_s, touched);
     }
-    if (!grid_sync(a.gb)) return;
-    // ------------------------------------------------------------ phase B
-    {
-      int cur_s = -1, touched = 0;
-      for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const Tile T = a.tiles[t];
-        if (T.sys != cur_s) {
-          if (cur_s >= 0) contribute<R, 1>(a, cur_s, touched);
-          cur_s = T.sys;
-          touched = 0;
+    // ---- coarse correction y = E^-1 Z^T r for systems about to run phase A
+    if (TWO && phaseA) {
+      for (int k = 0; k < nls; ++k) {
+        if (ls[k].state != S_A) continue;
+        const int D = ls[k].D, t0 = a.sys_t0[ls[k].sys];
+        for (int d = threadIdx.x; d < D; d += kSolveThreads) sSk[k][d] = __ldcg(prev + (size_t)(t0 + d) * 3 + 2);
+        __syncthreads();
+        for (int j = threadIdx.x; j < D; j += kSolveThreads) {
+          double acc = 0.0;
+          const float* Ej = sEk[k];
+          for (int d = 0; d < D; ++d) acc += (double)Ej[d * D + j] * sSk[k][d];  // E^-1 symmetric
+          sYk[k][j] = acc;
         }
-        ++touched;
-        const int k = T.comp;
-        const int* si = a.si + (size_t)T.sys * SI_N;
-        const double* sd = a.sd + (size_t)T.sys * SD_N;
-        const int st = __ldcg(si + SI_STATE);
-        double v[2] = {0.0, 0.0};
-        if (st == ST_OUTER) {
-          const bool done = __ldcg(si + SI_DONEFLAG) != 0;
-          for (int sl = T.s0 + warp; sl < T.s1; sl += kSolveThreads / 32) {
-            const int row = sl * 32 + lane;
-            a.x[k][row] += (double)a.e[k * nv + row];
-            a.e[k * nv + row] = R(0);
-            if (!done) {
-              const R rr = R(a.r64[k * nv + row]);
-              const R zz = rr * a.dinv[k][row];
-              a.r[k * nv + row] = rr;
-              a.z[k * nv + row] = zz;
-              v[0] += (double)rr * (double)zz;
-              v[1] += (double)rr * (double)rr;
-            }
-          }
-        } else if (st == ST_INNER) {
-          const R alpha = R(__ldcg(sd + SD_ALPHA));
-          const int par = __ldcg(si + SI_PAR);
-          const R* pnew = a.p + (2 * k + par) * nv;
-          for (int sl = T.s0 + warp; sl < T.s1; sl += kSolveThreads / 32) {
-            const int row = sl * 32 + lane;
-            const size_t o = k * nv + row;
-            a.e[o] += alpha * pnew[row];
-            const R rr = a.r[o] - alpha * a.q[o];
-            const R zz = rr * a.dinv[k][row];
-            a.r[o] = rr;
-            a.z[o] = zz;
-            v[0] += (double)rr * (double)zz;
-            v[1] += (double)rr * (double)rr;
-          }
-        }
-        double outv[2];
-        block_reduce_store<2>(v, outv);
-        if (threadIdx.x == 0) {
-          a.part[(size_t)t * 2] = outv[0];
-          a.part[(size_t)t * 2 + 1] = outv[1];
+        __syncthreads();
+        if (warp == 0) {
+          double c = 0.0;
+          for (int d = lane; d < D; d += 32) c += sSk[k][d] * sYk[k][d];
+          c = warp_sum(c);
+          if (lane == 0) ls[k].rzc = c;
         }
       }
-      if (cur_s >= 0) contribute<R, 1>(a, cur_s, touched);
+    }
+    __syncthreads();
+    // ---- decisions (thread 0; identical in every block owning the system)
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < nls; ++k) {
+        LocalSys& L = ls[k];
+        int act = ACT_NONE;
+        if (phaseA) {
+          if (L.state == S_OUT_A) {
+            act = ACT_OUT_A;
+            L.state = S_OUT_B;
+          } else if (L.state == S_A) {
+            const double rz = L.sum[0] + (TWO ? L.rzc : 0.0), rr = sqrt(L.sum[1]);
+            if (rr <= L.intol || L.it >= L.maxit || !(rr == rr)) {
+              act = ACT_OUT_A;  // reliable update in FP64
+              L.state = S_OUT_B;
+            } else {
+              L.beta = L.first ? 0.0 : (L.rz_prev != 0.0 ? rz / L.rz_prev : 0.0);
+              L.rz_prev = rz;
+              L.first = 0;
+              act = ACT_A;
+              L.state = S_B;
+            }
+          }
+        } else {
+          if (L.state == S_OUT_B) {
+            L.res = sqrt(L.sum[0]);
+            L.outer += 1;
+            if (L.res <= L.tol || L.it >= L.maxit || !(L.res == L.res)) {
+              act = ACT_OUT_DONE;
+              L.state = S_DONE;
+            } else {
+              L.intol = fmax(a.eta * L.res, 0.5 * L.tol);
+              L.first = 1;  // CG restarts from the true residual
+              act = ACT_OUT_B;
+              L.state = S_A;
+            }
+          } else if (L.state == S_B) {
+            L.alpha = L.sum[0] != 0.0 ? L.rz_prev / L.sum[0] : 0.0;
+            L.it += 1;
+            act = ACT_B;
+            L.state = S_A;
+          }
+        }
+        L.act = act;
+      }
+    }
+    __syncthreads();
+    // ---- work on the own tiles
+    for (int t = t_lo; t < t_hi; ++t) {
+      const Tile T = a.tiles[t];
+      const int k = T.comp;
+      const int lk = T.sys - sys0;
+      const LocalSys& L = ls[lk];
+      const int act = L.act;
+      if (act == ACT_NONE) continue;
+      double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+      const R* dinv = a.dinv[k];
+      R* e = a.e + k * nv;
+      R* r = a.r + k * nv;
+      R* z = a.z + k * nv;
+      R* q = a.q + k * nv;
+      double* r64 = a.r64 + k * nv;
+      if (act == ACT_OUT_A) {
+        const double* A = a.A64[k];
+        const double* xk = a.x[k];
+        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+          const int row = sl * 32 + lane;
+          const int base = a.sl_ptr[sl], len = a.sl_len[sl];
+          double acc = 0.0;
+          for (int j = 0; j < len; ++j) {
+            const int ei = base + j * 32 + lane;
+            const int col = __ldg(a.sl_col + ei);
+            acc += A[ei] * (__ldcg(xk + col) + (double)__ldcg(e + col));
+          }
+          const double rr = a.b[k][row] - acc;
+          r64[row] = rr;
+          v0 += rr * rr;
+        }
+      } else if (act == ACT_OUT_B || act == ACT_OUT_DONE) {
+        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+          const int row = sl * 32 + lane;
+          a.x[k][row] += (double)e[row];
+          e[row] = R(0);
+          if (act == ACT_OUT_B) {
+            const R rr = R(r64[row]);
+            const R zz = TWO ? block_jacobi32<R>(a.Binv, sl, rr, lane) : rr * dinv[row];
+            r[row] = rr;
+            z[row] = zz;
+            v0 += (double)rr * (double)zz;
+            v1 += (double)rr * (double)rr;
+            v2 += (double)rr;
+          }
+        }
+      } else if (act == ACT_A) {
+        const R beta = R(L.beta);
+        R* pn = a.p + (2 * k + L.par) * nv;
+        const R* po = a.p + (2 * k + (L.par ^ 1)) * nv;
+        const R* A = a.Ain[k];
+        const double* y = TWO ? sYk[lk] : nullptr;
+        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+          const int row = sl * 32 + lane;
+          const int base = a.sl_ptr[sl], len = a.sl_len[sl];
+          R acc = R(0);
+          for (int j = 0; j < len; ++j) {
+            const int ei = base + j * 32 + lane;
+            const int col = __ldg(a.sl_col + ei);
+            R zc = __ldcg(z + col);
+            if (TWO) zc += R(y[((col >> 5) - L.sl0) / L.sps]);
+            acc += A[ei] * (zc + beta * __ldcg(po + col));
+          }
+          R zr = z[row];
+          if (TWO) zr += R(y[(sl - L.sl0) / L.sps]);
+          const R pp = zr + beta * po[row];
+          pn[row] = pp;
+          q[row] = acc;
+          v0 += (double)pp * (double)acc;
+        }
+      } else if (act == ACT_B) {
+        const R alpha = R(L.alpha);
+        const R* pn = a.p + (2 * k + L.par) * nv;
+        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+          const int row = sl * 32 + lane;
+          e[row] += alpha * pn[row];
+          const R rr = r[row] - alpha * q[row];
+          const R zz = TWO ? block_jacobi32<R>(a.Binv, sl, rr, lane) : rr * dinv[row];
+          r[row] = rr;
+          z[row] = zz;
+          v0 += (double)rr * (double)zz;
+          v1 += (double)rr * (double)rr;
+          v2 += (double)rr;
+        }
+      }
+      // deterministic block reduction into this iteration's parity buffer
+      v0 = warp_sum(v0);
+      v1 = warp_sum(v1);
+      v2 = warp_sum(v2);
+      if (lane == 0) {
+        red[warp][0] = v0;
+        red[warp][1] = v1;
+      }
+      __shared__ double red2[kWarps];
+      if (lane == 0) red2[warp] = v2;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int wv = 0; wv < kWarps; ++wv) {
+          s0 += red[wv][0];
+          s1 += red[wv][1];
+          s2 += red2[wv];
+        }
+        double* dst = a.part + ((size_t)(iter & 1) * a.ntiles + t) * 3;
+        dst[0] = s0;
+        dst[1] = s1;
+        dst[2] = s2;
+      }
+      __syncthreads();
+    }
+    // ---- bookkeeping
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < nls; ++k) {
+        LocalSys& L = ls[k];
+        if (L.act == ACT_B) L.par ^= 1;
+        if (L.act == ACT_OUT_DONE && L.owner) {
+          a.out_it[L.sys] = L.it;
+          a.out_res[L.sys] = L.res;
+          a.out_outer[L.sys] = L.outer;
+          atomicSub(a.active, 1);
+        }
+        L.act = ACT_NONE;
+      }
     }
     if (!grid_sync(a.gb)) return;
   }
 }
 
 // ------------------------------------------------------------------ host
-static std::vector<Tile> build_tiles(const Ctx& c, int ncomp, std::vector<int>& sys_t0) {
-  std::vector<Tile> tiles;
-  const int ni = (int)c.inst.size();
-  sys_t0.assign(ncomp * ni + 1, 0);
-  for (int k = 0; k < ncomp; ++k)
-    for (int i = 0; i < ni; ++i) {
-      const int s = k * ni + i;
-      sys_t0[s] = (int)tiles.size();
-      const int sl0 = c.inst[i].v_off / kSlice, sl1 = (c.inst[i].v_off + c.inst[i].nv_pad) / kSlice;
-      for (int a = sl0; a < sl1; a += c.tile_slices) tiles.push_back(Tile{s, k, a, std::min(sl1, a + c.tile_slices)});
-    }
-  sys_t0[ncomp * ni] = (int)tiles.size();
-  return tiles;
-}
-
 struct KrylovWs {
   Tile* tiles[2];
   int* sys_t0[2];
-  int ntiles[2];
-  int nsys[2];
-  double* r64;
-  void* e;
-  void* r;
-  void* z;
-  void* p;
-  void* q;
-  double* part;
-  int* cnt;
-  double* sd[3];  // per solve kind (prediction, pressure, correction)
-  int* si[3];
-  int* active;
-  int coop_blocks[2];  // per inner type: 0 float, 1 double
+  int* blk_t0[2];
+  int ntiles[2], nsys[2], grid[2];
+  std::vector<Tile> h_tiles0;
+  std::vector<int> h_sys_t0_0;
+  // two-level data of the pressure phase (phase 0)
+  bool two_level = false;
+  int dmax = 0, nls_max = 1;
+  size_t smem_two = 0;
+  void* Binv = nullptr;
+  float* Einv = nullptr;
+  int *sys_eoff = nullptr, *sys_D = nullptr, *sys_sl0 = nullptr, *sys_sps = nullptr;
+  void *e = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p = nullptr;
+  double* r64 = nullptr;
+  double* part = nullptr;
+  int* active = nullptr;
+  int* out_it[3];
+  double* out_res[3];
+  int* out_outer[3];
 };
+
+static int max_local_systems(const std::vector<Tile>& tiles, const std::vector<int>& bt0) {
+  int worst = 0;
+  for (size_t b = 0; b + 1 < bt0.size(); ++b)
+    if (bt0[b + 1] > bt0[b]) worst = std::max(worst, tiles[bt0[b + 1] - 1].sys - tiles[bt0[b]].sys + 1);
+  return worst;
+}
+
+template <typename R, bool TWO>
+static int occupancy(size_t smem) {
+  int occ = 0;
+  // one process-wide upper bound, so contexts with different coarse sizes coexist
+  if (TWO) cudaFuncSetAttribute((const void*)k_krylov<R, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_krylov<R, TWO>, kSolveThreads, smem) != cudaSuccess) return 0;
+  return occ;
+}
 
 pfem2_status krylov_setup(Ctx& c) {
   KrylovWs* w = new KrylovWs();
-  const int dim = c.dim;
+  c.kws = w;
+  const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
   const size_t rs = c.mixed ? sizeof(float) : sizeof(double);
+  const int bps = std::max(1, c.solve_blocks_per_sm);
   int maxtiles = 0, maxsys = 0;
   for (int ph = 0; ph < 2; ++ph) {
-    std::vector<int> st0;
-    auto tiles = build_tiles(c, ph == 0 ? 1 : dim, st0);
-    w->ntiles[ph] = (int)tiles.size();
+    const int ncomp = ph == 0 ? 1 : dim;
+    std::vector<Tile> tiles;
+    std::vector<int> st0(ncomp * ni + 1, 0);
+    if (ph == 0) {
+      // pressure: tiles = coarse subdomains, at most dmax per system
+      const int dcap = ni == 1 ? 208 : 96;
+      w->dmax = 1;
+      for (int i = 0; i < ni; ++i) {
+        st0[i] = (int)tiles.size();
+        const int sl0 = c.inst[i].v_off / kSlice, nsl = c.inst[i].nv_pad / kSlice;
+        int D = std::min((nsl + 7) / 8, dcap);
+        const int sps = (nsl + D - 1) / D;
+        D = (nsl + sps - 1) / sps;
+        for (int a = 0; a < nsl; a += sps) tiles.push_back(Tile{i, 0, sl0 + a, sl0 + std::min(nsl, a + sps)});
+        w->dmax = std::max(w->dmax, D);
+      }
+      st0[ni] = (int)tiles.size();
+    } else {
+      const long long slices = (long long)c.nslices * ncomp;
+      const long long target = 2LL * bps * c.num_sms;
+      int ts = (int)std::max<long long>(8, (slices + target - 1) / target);
+      if (c.tile_slices > 0) ts = c.tile_slices;
+      for (int k = 0; k < ncomp; ++k)
+        for (int i = 0; i < ni; ++i) {
+          const int sidx = k * ni + i;
+          st0[sidx] = (int)tiles.size();
+          const int sl0 = c.inst[i].v_off / kSlice, sl1 = (c.inst[i].v_off + c.inst[i].nv_pad) / kSlice;
+          for (int a = sl0; a < sl1; a += ts) tiles.push_back(Tile{sidx, k, a, std::min(sl1, a + ts)});
+        }
+      st0[ncomp * ni] = (int)tiles.size();
+    }
+    const int T = (int)tiles.size();
+    int occ;
+    size_t smem = 0;
+    if (ph == 0) {
+      // shared memory for the coarse inverses: sized after the chunking below,
+      // first with one local system to bound the grid
+      w->nls_max = 1;
+      smem = (size_t)w->dmax * w->dmax * 4 + 8 + 2 * (size_t)w->dmax * 8;
+      occ = c.mixed ? occupancy<float, true>(smem) : occupancy<double, true>(smem);
+    } else {
+      occ = c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0);
+    }
+    if (occ < 1) {
+      set_error("krylov: the solver kernel cannot be resident");
+      return PFEM2_CUDA_ERROR;
+    }
+    const int G = std::min(T, std::min(occ, bps) * c.num_sms);
+    std::vector<int> bt0(G + 1);
+    for (int b = 0; b <= G; ++b) bt0[b] = (int)((long long)T * b / G);
+    const int nls = max_local_systems(tiles, bt0);
+    if (nls > kMaxLocalSys) {
+      set_error("krylov: more than 16 systems would share one block (instances too small for the batch)");
+      return PFEM2_INVALID_ARG;
+    }
+    if (ph == 0) {
+      w->nls_max = nls;
+      w->smem_two = (size_t)nls * w->dmax * w->dmax * 4 + 8 + 2 * (size_t)nls * w->dmax * 8;
+      if (w->smem_two > 220 * 1024) {
+        set_error("krylov: coarse inverses of the pressure systems exceed shared memory");
+        return PFEM2_INVALID_ARG;
+      }
+      const int occ2 = c.mixed ? occupancy<float, true>(w->smem_two) : occupancy<double, true>(w->smem_two);
+      if (occ2 * c.num_sms < G) {
+        set_error("krylov: the two-level solver grid cannot be resident");
+        return PFEM2_CUDA_ERROR;
+      }
+      w->h_tiles0 = tiles;
+      w->h_sys_t0_0 = st0;
+    }
+    w->ntiles[ph] = T;
     w->nsys[ph] = (int)st0.size() - 1;
-    PFEM2_CUDA(cudaMalloc(&w->tiles[ph], sizeof(Tile) * tiles.size()));
-    PFEM2_CUDA(cudaMemcpy(w->tiles[ph], tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+    w->grid[ph] = G;
+    PFEM2_CUDA(cudaMalloc(&w->tiles[ph], sizeof(Tile) * T));
+    PFEM2_CUDA(cudaMemcpy(w->tiles[ph], tiles.data(), sizeof(Tile) * T, cudaMemcpyHostToDevice));
     PFEM2_CUDA(cudaMalloc(&w->sys_t0[ph], sizeof(int) * st0.size()));
     PFEM2_CUDA(cudaMemcpy(w->sys_t0[ph], st0.data(), sizeof(int) * st0.size(), cudaMemcpyHostToDevice));
-    maxtiles = std::max(maxtiles, (int)tiles.size());
+    PFEM2_CUDA(cudaMalloc(&w->blk_t0[ph], sizeof(int) * bt0.size()));
+    PFEM2_CUDA(cudaMemcpy(w->blk_t0[ph], bt0.data(), sizeof(int) * bt0.size(), cudaMemcpyHostToDevice));
+    maxtiles = std::max(maxtiles, T);
     maxsys = std::max(maxsys, w->nsys[ph]);
   }
-  PFEM2_CUDA(cudaMalloc(&w->r64, sizeof(double) * nv * dim));
-  PFEM2_CUDA(cudaMalloc(&w->e, rs * nv * dim));
-  PFEM2_CUDA(cudaMalloc(&w->r, rs * nv * dim));
-  PFEM2_CUDA(cudaMalloc(&w->z, rs * nv * dim));
-  PFEM2_CUDA(cudaMalloc(&w->p, rs * nv * dim * 2));
-  PFEM2_CUDA(cudaMalloc(&w->q, rs * nv * dim));
-  PFEM2_CUDA(cudaMemset(w->p, 0, rs * nv * dim * 2));
-  PFEM2_CUDA(cudaMemset(w->z, 0, rs * nv * dim));
-  PFEM2_CUDA(cudaMemset(w->e, 0, rs * nv * dim));
-  PFEM2_CUDA(cudaMalloc(&w->part, sizeof(double) * 2 * maxtiles));
-  PFEM2_CUDA(cudaMalloc(&w->cnt, sizeof(int) * maxsys));
-  PFEM2_CUDA(cudaMemset(w->cnt, 0, sizeof(int) * maxsys));
-  for (int k = 0; k < 3; ++k) {
-    PFEM2_CUDA(cudaMalloc(&w->sd[k], sizeof(double) * SD_N * maxsys));
-    PFEM2_CUDA(cudaMalloc(&w->si[k], sizeof(int) * SI_N * maxsys));
-    PFEM2_CUDA(cudaMemset(w->sd[k], 0, sizeof(double) * SD_N * maxsys));
-    PFEM2_CUDA(cudaMemset(w->si[k], 0, sizeof(int) * SI_N * maxsys));
+  void** vecs[] = {&w->e, &w->r, &w->z, &w->q};
+  for (void** v : vecs) {
+    PFEM2_CUDA(cudaMalloc(v, rs * nv * dim));
+    PFEM2_CUDA(cudaMemset(*v, 0, rs * nv * dim));
   }
+  PFEM2_CUDA(cudaMalloc(&w->p, rs * nv * dim * 2));
+  PFEM2_CUDA(cudaMemset(w->p, 0, rs * nv * dim * 2));
+  PFEM2_CUDA(cudaMalloc(&w->r64, sizeof(double) * nv * dim));
+  PFEM2_CUDA(cudaMemset(w->r64, 0, sizeof(double) * nv * dim));
+  PFEM2_CUDA(cudaMalloc(&w->part, sizeof(double) * 6 * maxtiles));
+  PFEM2_CUDA(cudaMemset(w->part, 0, sizeof(double) * 6 * maxtiles));
   PFEM2_CUDA(cudaMalloc(&w->active, sizeof(int)));
-  int nb = 0;
-  PFEM2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_krylov<float>, kSolveThreads, 0));
-  w->coop_blocks[0] = std::max(1, nb) * c.num_sms;
-  PFEM2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_krylov<double>, kSolveThreads, 0));
-  w->coop_blocks[1] = std::max(1, nb) * c.num_sms;
-  c.kws = w;
+  for (int k = 0; k < 3; ++k) {
+    PFEM2_CUDA(cudaMalloc(&w->out_it[k], sizeof(int) * maxsys));
+    PFEM2_CUDA(cudaMalloc(&w->out_res[k], sizeof(double) * maxsys));
+    PFEM2_CUDA(cudaMalloc(&w->out_outer[k], sizeof(int) * maxsys));
+    PFEM2_CUDA(cudaMemset(w->out_it[k], 0, sizeof(int) * maxsys));
+    PFEM2_CUDA(cudaMemset(w->out_res[k], 0, sizeof(double) * maxsys));
+    PFEM2_CUDA(cudaMemset(w->out_outer[k], 0, sizeof(int) * maxsys));
+  }
   return PFEM2_OK;
 }
 
-// per-system initial scalars, uploaded before each phase (graph-capturable:
-// a small kernel writes them from the instance table)
-__global__ void k_init_sys(int nsys, int ninst, const double* __restrict__ tol_i,
-                           const int* __restrict__ maxit_i, double* __restrict__ sd, int* __restrict__ si,
-                           int* __restrict__ cnt, int* __restrict__ active, unsigned* __restrict__ barrier,
-                           int* __restrict__ err) {
-  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
-    cnt[s] = 0;
-    const int i = s % ninst;
-    double* d = sd + (size_t)s * SD_N;
-    int* q = si + (size_t)s * SI_N;
-    d[SD_RHO] = 0.0; d[SD_ALPHA] = 0.0; d[SD_BETA] = 0.0; d[SD_RES] = 0.0;
-    d[SD_INTOL] = 0.0; d[SD_RR] = 0.0; d[SD_TOL] = tol_i[i];
-    q[SI_STATE] = ST_OUTER; q[SI_IT] = 0; q[SI_PAR] = 0; q[SI_DONEFLAG] = 0; q[SI_OUTER] = 0; q[SI_MAXIT] = maxit_i[i];
+// in-place inverse of an SPD matrix (Cholesky, then L^-T L^-1); false if not SPD
+static bool spd_inverse(std::vector<double>& M, int n) {
+  std::vector<double> L((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double d = M[(size_t)j * n + j];
+    for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+    if (!(d > 0.0)) return false;
+    d = std::sqrt(d);
+    L[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double s = M[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+      L[(size_t)i * n + j] = s / d;
+    }
   }
+  // Linv (lower)
+  std::vector<double> Li((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
+    for (int i = j + 1; i < n; ++i) {
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
+      Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = 0.0;
+      for (int k = i; k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
+      M[(size_t)i * n + j] = s;
+      M[(size_t)j * n + i] = s;
+    }
+  return true;
+}
+
+// block-Jacobi inverses of the 32x32 slice blocks and the coarse inverses
+// E^-1 = (Z^T A Z)^-1 of the pressure matrix (after Dirichlet elimination).
+pfem2_status krylov_setup_precond(Ctx& c) {
+  KrylovWs* w = (KrylovWs*)c.kws;
+  const int ni = (int)c.inst.size();
+  std::vector<double> A(c.nell);
+  std::vector<int> col(c.nell), len(c.nslices);
+  PFEM2_CUDA(cudaMemcpy(A.data(), c.A64[3], sizeof(double) * c.nell, cudaMemcpyDeviceToHost));
+  PFEM2_CUDA(cudaMemcpy(col.data(), c.sl_col, sizeof(int) * c.nell, cudaMemcpyDeviceToHost));
+  PFEM2_CUDA(cudaMemcpy(len.data(), c.sl_len, sizeof(int) * c.nslices, cudaMemcpyDeviceToHost));
+  const std::vector<int>& sp = c.h_sl_ptr;
+  // block Jacobi
+  std::vector<double> B(1024);
+  std::vector<double> bj64;
+  std::vector<float> bj32;
+  if (c.mixed) bj32.resize((size_t)c.nslices * 1024);
+  else bj64.resize((size_t)c.nslices * 1024);
+  for (int s = 0; s < c.nslices; ++s) {
+    std::fill(B.begin(), B.end(), 0.0);
+    for (int l = 0; l < 32; ++l)
+      for (int j = 0; j < len[s]; ++j) {
+        const int e = sp[s] + j * 32 + l;
+        const int cc = col[e];
+        if (cc / 32 == s) B[(size_t)l * 32 + (cc % 32)] += A[e];
+      }
+    if (!spd_inverse(B, 32)) {
+      set_error("krylov: a diagonal block of the pressure matrix is not SPD");
+      return PFEM2_MESH_ERROR;
+    }
+    for (int jj = 0; jj < 32; ++jj)
+      for (int i = 0; i < 32; ++i) {
+        const double v = B[(size_t)i * 32 + jj];
+        if (c.mixed) bj32[(size_t)s * 1024 + jj * 32 + i] = (float)v;
+        else bj64[(size_t)s * 1024 + jj * 32 + i] = v;
+      }
+  }
+  const size_t bbytes = (size_t)c.nslices * 1024 * (c.mixed ? 4 : 8);
+  PFEM2_CUDA(cudaMalloc(&w->Binv, bbytes));
+  PFEM2_CUDA(cudaMemcpy(w->Binv, c.mixed ? (void*)bj32.data() : (void*)bj64.data(), bbytes, cudaMemcpyHostToDevice));
+  // coarse inverses per system (tile = subdomain)
+  const std::vector<Tile>& tiles = w->h_tiles0;
+  const std::vector<int>& st0 = w->h_sys_t0_0;
+  std::vector<int> eoff(ni), Dv(ni), sl0v(ni), spsv(ni);
+  std::vector<float> Einv;
+  std::vector<int> sub_of_slice(c.nslices, -1);
+  for (int i = 0; i < ni; ++i) {
+    const int t0 = st0[i], t1 = st0[i + 1], D = t1 - t0;
+    Dv[i] = D;
+    sl0v[i] = tiles[t0].s0;
+    spsv[i] = tiles[t0].s1 - tiles[t0].s0;
+    for (int t = t0; t < t1; ++t)
+      for (int s = tiles[t].s0; s < tiles[t].s1; ++s) sub_of_slice[s] = t - t0;
+    std::vector<double> E((size_t)D * D, 0.0);
+    for (int t = t0; t < t1; ++t)
+      for (int s = tiles[t].s0; s < tiles[t].s1; ++s)
+        for (int l = 0; l < 32; ++l)
+          for (int j = 0; j < len[s]; ++j) {
+            const int e = sp[s] + j * 32 + l;
+            E[(size_t)(t - t0) * D + sub_of_slice[col[e] / 32]] += A[e];
+          }
+    if (!spd_inverse(E, D)) {
+      set_error("krylov: the coarse pressure matrix is not SPD");
+      return PFEM2_MESH_ERROR;
+    }
+    eoff[i] = (int)Einv.size();
+    for (double v : E) Einv.push_back((float)v);
+  }
+  PFEM2_CUDA(cudaMalloc(&w->Einv, sizeof(float) * Einv.size()));
+  PFEM2_CUDA(cudaMemcpy(w->Einv, Einv.data(), sizeof(float) * Einv.size(), cudaMemcpyHostToDevice));
+  int** dst[] = {&w->sys_eoff, &w->sys_D, &w->sys_sl0, &w->sys_sps};
+  std::vector<int>* src[] = {&eoff, &Dv, &sl0v, &spsv};
+  for (int k = 0; k < 4; ++k) {
+    PFEM2_CUDA(cudaMalloc(dst[k], sizeof(int) * ni));
+    PFEM2_CUDA(cudaMemcpy(*dst[k], src[k]->data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
+  }
+  w->two_level = true;
+  return PFEM2_OK;
+}
+
+__global__ void k_init_solve(int nsys, int* __restrict__ active, unsigned* __restrict__ barrier,
+                             int* __restrict__ err) {
   if (threadIdx.x == 0) {
     *active = nsys;
     barrier[0] = 0;
@@ -431,13 +686,13 @@ __global__ void k_init_sys(int nsys, int ninst, const double* __restrict__ tol_i
   }
 }
 
-
 template <typename R>
 static pfem2_status solve_impl(Ctx& c, int which) {
   KrylovWs* w = (KrylovWs*)c.kws;
   const int ph = which == 1 ? 0 : 1;
   const int ncomp = which == 1 ? 1 : c.dim;
   const int ni = (int)c.inst.size();
+  const bool two = which == 1 && w->two_level && c.two_level;
   SolveArgs<R> a{};
   a.ncomp = ncomp;
   a.ninst = ni;
@@ -446,18 +701,23 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.nv = c.nv;
   a.tiles = w->tiles[ph];
   a.sys_t0 = w->sys_t0[ph];
+  a.blk_t0 = w->blk_t0[ph];
   a.sl_ptr = c.sl_ptr;
   a.sl_len = c.sl_len;
   a.sl_col = c.sl_col;
+  a.Binv = (const R*)w->Binv;
+  a.Einv = w->Einv;
+  a.sys_eoff = w->sys_eoff;
+  a.sys_D = w->sys_D;
+  a.sys_sl0 = w->sys_sl0;
+  a.sys_sps = w->sys_sps;
+  a.dmax = w->dmax;
   for (int k = 0; k < 3; ++k) {
     const int kk = k < ncomp ? k : 0;
-    int m;
-    if (which == 0) m = kk;
-    else if (which == 1) m = 3;
-    else m = 4 + kk;
-    a.A64[k] = c.A64[m];
-    a.Ain[k] = c.mixed ? (const R*)c.A32[m] : (const R*)c.A64[m];
-    a.dinv[k] = c.mixed ? (const R*)c.dinv32[m] : (const R*)c.dinv64[m];
+    const int mtx = which == 0 ? kk : (which == 1 ? 3 : 4 + kk);
+    a.A64[k] = c.A64[mtx];
+    a.Ain[k] = c.mixed ? (const R*)c.A32[mtx] : (const R*)c.A64[mtx];
+    a.dinv[k] = c.mixed ? (const R*)c.dinv32[mtx] : (const R*)c.dinv64[mtx];
     if (which == 0) {
       a.x[k] = c.F[PFEM2_FIELD_PRED_VX + kk];
       a.b[k] = c.rhs[kk];
@@ -475,32 +735,31 @@ static pfem2_status solve_impl(Ctx& c, int which) {
       a.g[k] = nullptr;
     }
   }
+  a.tol_i = (const double*)c.sys_scalars + (which == 1 ? ni : 0);
+  a.maxit_i = c.d_sysinfo;
+  a.e = (R*)w->e; a.r = (R*)w->r; a.z = (R*)w->z; a.q = (R*)w->q; a.p = (R*)w->p;
   a.r64 = w->r64;
-  a.e = (R*)w->e;
-  a.r = (R*)w->r;
-  a.z = (R*)w->z;
-  a.p = (R*)w->p;
-  a.q = (R*)w->q;
   a.part = w->part;
-  a.cnt = w->cnt;
-  a.sd = w->sd[which];
-  a.si = w->si[which];
   a.active = w->active;
-  a.eta = c.mixed ? 1e-4 : 0.0;
+  a.out_it = w->out_it[which];
+  a.out_res = w->out_res[which];
+  a.out_outer = w->out_outer[which];
+  a.eta = c.mixed ? c.refine_eta : 0.0;
   int mx = 0;
   for (auto& in : c.inst) mx = std::max(mx, in.cs.max_iter > 0 ? in.cs.max_iter : 10000);
   a.iter_cap = 2 * mx + 64;
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
-  // tolerances / max_iter per instance
-  double* tol = (double*)c.sys_scalars + (which == 1 ? ni : 0);
-  int* maxit = c.d_sysinfo;
-  k_init_sys<<<1, 256, 0, c.stream>>>(a.nsys, ni, tol, maxit, a.sd, a.si, w->cnt, w->active, c.barrier, c.d_err);
+  k_init_solve<<<1, 32, 0, c.stream>>>(a.nsys, w->active, c.barrier, c.d_err);
   c.launches++;
-  const int blocks = std::min(a.ntiles, w->coop_blocks[sizeof(R) == 8 ? 1 : 0]);
   void* args[] = {&a};
-  PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R>, dim3(blocks), dim3(kSolveThreads), args, 0, c.stream));
+  if (two)
+    PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, true>, dim3(w->grid[ph]), dim3(kSolveThreads),
+                                           args, w->smem_two, c.stream));
+  else
+    PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, false>, dim3(w->grid[ph]), dim3(kSolveThreads),
+                                           args, 0, c.stream));
   c.launches++;
   return PFEM2_OK;
 }
@@ -509,41 +768,44 @@ pfem2_status krylov_solve(Ctx& c, int which) {
   return c.mixed ? solve_impl<float>(c, which) : solve_impl<double>(c, which);
 }
 
-// copies per-system iteration counts / residuals into c.stats (max over
-// instances); NOT_CONVERGED if any system ended above its tolerance
+// per-system iteration counts / residuals into c.stats (max over
+// instances); NOT_CONVERGED if a system ended above its tolerance
 static pfem2_status read_stats_phase(Ctx& c, int which) {
   KrylovWs* w = (KrylovWs*)c.kws;
   const int ph = which == 1 ? 0 : 1;
   const int ns = w->nsys[ph];
-  std::vector<double> sd((size_t)ns * SD_N);
-  std::vector<int> si((size_t)ns * SI_N);
-  PFEM2_CUDA(cudaMemcpyAsync(sd.data(), w->sd[which], sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, c.stream));
-  PFEM2_CUDA(cudaMemcpyAsync(si.data(), w->si[which], sizeof(int) * si.size(), cudaMemcpyDeviceToHost, c.stream));
+  std::vector<int> it(ns), outer(ns);
+  std::vector<double> res(ns);
+  PFEM2_CUDA(cudaMemcpyAsync(it.data(), w->out_it[which], sizeof(int) * ns, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(res.data(), w->out_res[which], sizeof(double) * ns, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(outer.data(), w->out_outer[which], sizeof(int) * ns, cudaMemcpyDeviceToHost, c.stream));
   PFEM2_CUDA(cudaStreamSynchronize(c.stream));
   const int ni = (int)c.inst.size();
   const int ncomp = which == 1 ? 1 : c.dim;
   bool notconv = false;
   for (int k = 0; k < ncomp; ++k) {
-    int slot = which == 0 ? k : (which == 1 ? 3 : 4 + k);
-    int it = 0;
-    double res = 0.0;
+    const int slot = which == 0 ? k : (which == 1 ? 3 : 4 + k);
+    int mit = 0, mo = 0;
+    double mres = 0.0;
     for (int i = 0; i < ni; ++i) {
       const int s = k * ni + i;
-      it = std::max(it, si[(size_t)s * SI_N + SI_IT]);
-      res = std::max(res, sd[(size_t)s * SD_N + SD_RES]);
-      if (sd[(size_t)s * SD_N + SD_RES] > sd[(size_t)s * SD_N + SD_TOL]) notconv = true;
+      mit = std::max(mit, it[s]);
+      mo = std::max(mo, outer[s]);
+      mres = std::max(mres, res[s]);
+      const double tol = which == 1 ? c.inst[i].cs.p_tol : c.inst[i].cs.vel_tol;
+      if (res[s] > tol) notconv = true;
     }
-    c.stats.iters[slot] = it;
-    c.stats.residual[slot] = res;
-    if (which == 1) c.stats.refinements_p = si[SI_OUTER];
+    c.stats.iters[slot] = mit;
+    c.stats.residual[slot] = mres;
+    if (which == 1) c.stats.refinements_p = mo;
   }
   return notconv ? PFEM2_NOT_CONVERGED : PFEM2_OK;
 }
 
 pfem2_status krylov_read_stats(Ctx& c) {
   pfem2_status worst = PFEM2_OK;
-  for (int w = 0; w < 3; ++w) {
-    pfem2_status s = read_stats_phase(c, w);
+  for (int wch = 0; wch < 3; ++wch) {
+    pfem2_status s = read_stats_phase(c, wch);
     if (s != PFEM2_OK && worst == PFEM2_OK) worst = s;
   }
   int err = 0;

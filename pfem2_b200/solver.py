@@ -26,6 +26,8 @@ class Pfem2Error(RuntimeError):
 
 
 _LIB = None
+N_STAGES = 7
+STAGE_NAMES = ["advect", "rebin", "project_nodes", "prediction", "pressure_rhs", "pressure_solve", "correction"]
 
 # every entry point declared in include/pfem2.h
 EXPORTS = [
@@ -217,13 +219,18 @@ class Solver:
         u = np.ascontiguousarray(np.concatenate([p[2] for p in per_instance]), np.float64)
         self._check(self.L.pfem2_set_particles(self.h, _iptr(counts), _iptr(cell), _dptr(xi), _dptr(u)))
 
-    def stats(self):
+    def stats(self, check=True):
+        """Counters of the last particle pass and the last Krylov solves. With
+        check=False a failing status (e.g. NOT_CONVERGED) is returned in the
+        dict under 'status' instead of raised."""
         s = A.Stats()
-        self._check(self.L.pfem2_get_stats(self.h, C.byref(s)))
+        st = self.L.pfem2_get_stats(self.h, C.byref(s))
+        if check:
+            self._check(st)
         return {"n_particles": s.n_particles, "deleted": s.n_deleted_last_move,
                 "removed": s.n_removed_last_check, "reseeded": s.n_reseeded_last_check,
                 "far": s.n_far_movers_last_move, "iters": list(s.iters), "residual": list(s.residual),
-                "refinements_p": s.refinements_p}
+                "refinements_p": s.refinements_p, "status": st}
 
     def synchronize(self):
         self._check(self.L.pfem2_synchronize(self.h))
@@ -232,6 +239,26 @@ class Solver:
         n = C.c_int64()
         self._check(self.L.pfem2_launch_count(self.h, C.byref(n)))
         return n.value
+
+    def sizes(self):
+        """Rows (vertices), CSR nonzeros and arithmetic-type bytes of the batch."""
+        rows = nnz = 0
+        for sp in self.specs:
+            cv = sp.mesh.cells.astype(np.int64)
+            nvc = cv.shape[1]
+            a = np.repeat(cv, nvc, axis=1).reshape(-1)
+            b = np.tile(cv, (1, nvc)).reshape(-1)
+            nnz += len(np.unique(a * sp.mesh.n_vertices + b))
+            rows += sp.mesh.n_vertices
+        return {"rows": rows, "nnz": nnz, "real_bytes": 4 if self.cfg.precision == A.PREC_MIXED else 8}
+
+    def enable_stage_timing(self, on=True):
+        self._check(self.L.pfem2_enable_stage_timing(self.h, 1 if on else 0))
+
+    def stage_times(self, reset=False):
+        ms = np.zeros(N_STAGES)
+        self._check(self.L.pfem2_stage_times(self.h, _dptr(ms), 1 if reset else 0))
+        return ms
 
     def stream(self):
         s = C.c_void_p()

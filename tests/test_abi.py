@@ -1,0 +1,99 @@
+"""CPU checks of the C ABI: the ctypes mirror matches include/pfem2.h field
+for field, and libpfem2b.so loads and exports every declared entry point
+(no compute calls: this runs without a GPU)."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from pfem2_b200 import _abi as A
+from pfem2_b200 import solver
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pfem2.h")
+
+STRUCTS = {
+    "pfem2_dirichlet": (A.Dirichlet, ["boundary_id", "kind", "axis", "value", "a", "b"]),
+    "pfem2_case": (A.Case, ["mu", "rho", "dt", "n_dirichlet", "dirichlet", "open_boundary_mask",
+                            "open_boundary_pressure_flux", "zero_after_projection_mask", "load_patch_id",
+                            "probe_a", "probe_b", "outer_corrections", "load_diam", "load_umean", "vel_tol",
+                            "p_tol", "max_iter", "vel_solver", "p_solver", "reassemble_every_step"]),
+    "pfem2_mesh_view": (A.MeshView, ["n_vertices", "n_cells", "vertices", "cells", "face_boundary_id"]),
+    "pfem2_config": (A.Config, ["dim", "precision", "device", "movement_steps", "max_particles_per_cell_part",
+                                "particles_per_cell_max", "particle_capacity_factor", "far_mover_capacity",
+                                "use_graph"]),
+    "pfem2_stats": (A.Stats, ["n_particles", "n_deleted_last_move", "n_removed_last_check",
+                              "n_reseeded_last_check", "n_far_movers_last_move", "iters", "residual",
+                              "refinements_p"]),
+}
+
+
+def test_struct_layout_matches_header():
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    for cname, (_, fields) in STRUCTS.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "probe.c")
+        exe = os.path.join(d, "probe")
+        open(src, "w").write("\n".join(lines))
+        subprocess.check_call(["/usr/bin/gcc", "-std=c11", "-o", exe, src])
+        out = subprocess.check_output([exe]).decode().split("\n")
+    got = {}
+    for ln in out:
+        if ln.strip():
+            n, f, v = ln.split()
+            got[(n, f)] = int(v)
+    for cname, (cls, fields) in STRUCTS.items():
+        assert got[(cname, "sizeof")] == C.sizeof(cls), cname
+        for f in fields:
+            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)
+
+
+def declared_entry_points():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(pfem2_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_exports_cover_header():
+    names = declared_entry_points()
+    assert set(names) == set(solver.EXPORTS)
+    from pfem2_b200 import build as B
+    B.build()
+    lib = C.CDLL(solver.LIB_PATH)
+    for n in names:
+        assert hasattr(lib, n), n
+    lib.pfem2_abi_version.restype = C.c_int32
+    assert lib.pfem2_abi_version() == 1
+
+
+def test_status_codes_match_header():
+    txt = open(HEADER).read()
+    for name, val in (("PFEM2_OK", A.OK), ("PFEM2_INVALID_ARG", A.INVALID_ARG), ("PFEM2_CUDA_ERROR", A.CUDA_ERROR),
+                      ("PFEM2_NOT_CONVERGED", A.NOT_CONVERGED), ("PFEM2_TIMEOUT", A.TIMEOUT),
+                      ("PFEM2_PARTICLE_OVERFLOW", A.PARTICLE_OVERFLOW), ("PFEM2_NO_DEVICE", A.NO_DEVICE),
+                      ("PFEM2_BAD_STATE", A.BAD_STATE), ("PFEM2_MESH_ERROR", A.MESH_ERROR),
+                      ("PFEM2_FIELD_NODE_WEIGHT", A.FIELD_NODE_WEIGHT), ("PFEM2_FIELD_P", A.FIELD_P)):
+        m = re.search(rf"\b{name}\s*=\s*(\d+)", txt)
+        assert m and int(m.group(1)) == val, name
+
+
+def test_create_without_device_fails_loudly():
+    """On a machine without a CUDA device the library refuses to run (no CPU fallback)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    from pfem2_b200 import cases
+    sp = cases.poiseuille_2d(nx=4, ny=2)
+    with pytest.raises(solver.Pfem2Error) as e:
+        solver.Solver(sp)
+    assert e.value.status in (A.NO_DEVICE, A.CUDA_ERROR)
