@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -515,6 +516,17 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   Ctx& c = x->c;
   cudaSetDevice(c.device);
   cudaStreamSynchronize(c.stream);
+  if (const char* path = getenv("PFEM2_SOLVER_PROFILE")) {
+    // solver sub-phase times of block 0, appended as one line per context
+    unsigned long long pr[18] = {};
+    krylov_profile(c, pr);
+    if (FILE* f = fopen(path, "a")) {
+      fprintf(f, "prec=%s", c.mixed ? "mixed" : "fp64");
+      for (int k = 0; k < 18; ++k) fprintf(f, " %llu", pr[k]);
+      fprintf(f, "\n");
+      fclose(f);
+    }
+  }
   for (int k = 0; k < 2; ++k)
     if (x->graph[k]) cudaGraphExecDestroy(x->graph[k]);
   // device memory is released with the context's allocations; free the big ones

@@ -187,22 +187,30 @@ struct GridBarrier {
 
 #define PFEM2_BARRIER_SPIN_LIMIT (1u << 26)
 
-__device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
+// `gl` is thread 0's copy of the generation counter (0 after the reset that
+// precedes every launch), so arriving costs one atomic and no extra read.
+// With `stop` non-null the last block to arrive also reads *stop_src and
+// publishes (*stop_src <= 0) in bit 31 of the release word, so every block
+// learns a global termination condition without another memory round trip.
+__device__ __forceinline__ bool grid_sync(const GridBarrier& gb, unsigned& gl, const int* stop_src = nullptr,
+                                          bool* stop = nullptr) {
   __syncthreads();
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_stop;
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = gb.gen;
-    unsigned g = *vgen;
+    const unsigned g = gl;
     __threadfence();
     unsigned arrived = atomicAdd(gb.count, 1u);
     int ok = 1;
+    unsigned word = g + 1;
     if (arrived == gridDim.x - 1) {
       *gb.count = 0;
       __threadfence();
-      atomicAdd(gb.gen, 1u);
+      if (stop_src && *(volatile const int*)stop_src <= 0) word |= 0x80000000u;
+      atomicExch(gb.gen, word);
     } else {
       unsigned spins = 0;
-      while (*vgen == g) {
+      while ((word = *vgen) == g) {
         if (++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)gb.err) {
           atomicExch(gb.err, 1);
           ok = 0;
@@ -212,9 +220,12 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
       }
     }
     __threadfence();
+    gl = word;
+    s_stop = (word >> 31) & 1u;
     s_ok = ok && (*(volatile int*)gb.err == 0);
   }
   __syncthreads();
+  if (stop) *stop = s_stop != 0;
   return s_ok != 0;
 }
 

@@ -203,5 +203,6 @@ pfem2_status krylov_setup_precond(Ctx& c);
 // which: 0 prediction (dim systems per instance), 1 pressure, 2 correction
 pfem2_status krylov_solve(Ctx& c, int which);
 pfem2_status krylov_read_stats(Ctx& c);
+void krylov_profile(Ctx& c, unsigned long long* out18);
 
 }  // namespace pfem2

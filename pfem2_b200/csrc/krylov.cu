@@ -35,6 +35,7 @@
 // is <= tol.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <vector>
 
@@ -43,7 +44,7 @@
 
 namespace pfem2 {
 
-constexpr int kSolveThreads = 256;  // 8 warps
+constexpr int kSolveThreads = 384;  // 12 warps
 constexpr int kWarps = kSolveThreads / 32;
 constexpr int kMaxLocalSys = 16;
 
@@ -71,6 +72,7 @@ template <typename R> struct SolveArgs {
   const int* sys_sl0;    // first slice of the system
   const int* sys_sps;    // slices per tile (= per coarse subdomain)
   int dmax;              // max D over systems (smem stride)
+  int binv_smem;         // 1: this block's B^-1 slices are staged in shared memory
   double* x[3];
   const double* b[3];
   const unsigned char* isd[3];
@@ -88,7 +90,14 @@ template <typename R> struct SolveArgs {
   double eta;
   int iter_cap;
   GridBarrier gb;
+  unsigned long long* prof;  // optional: ns spent per sub-phase by block 0 (PFEM2_SOLVER_PROFILE)
 };
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 struct LocalSys {
   int sys, state, it, outer, par, first, owner, maxit, act;
@@ -116,6 +125,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t nv = (size_t)a.nv;
   const int t_lo = a.blk_t0[blockIdx.x], t_hi = a.blk_t0[blockIdx.x + 1];
+  unsigned bar_gen = 0;
   // two-level shared memory: per local system E^-1 (dmax^2 floats), y and Z^T r (dmax doubles each)
   float* sE = reinterpret_cast<float*>(dyn_smem);
   const int nE = a.dmax * a.dmax;
@@ -157,15 +167,25 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
   float* sEk[kMaxLocalSys];
   double* sYk[kMaxLocalSys];
   double* sSk[kMaxLocalSys];
+  const R* Bsrc = a.Binv;  // B^-1 of slice s at Bsrc + (s - bsl0) * 1024
+  int bsl0 = 0;
   if (TWO) {
     double* ybase = reinterpret_cast<double*>(sE + (size_t)nls * nE + ((nls * nE) & 1));
     for (int k = 0; k < nls; ++k) {
       sEk[k] = sE + (size_t)k * nE;
-      sYk[k] = ybase + (size_t)k * 2 * a.dmax;
-      sSk[k] = sYk[k] + a.dmax;
+      sYk[k] = ybase + (size_t)k * 3 * a.dmax;
+      sSk[k] = sYk[k] + 2 * a.dmax;
       const float* src = a.Einv + a.sys_eoff[ls[k].sys];
       const int n2 = ls[k].D * ls[k].D;
       for (int i = threadIdx.x; i < n2; i += kSolveThreads) sEk[k][i] = src[i];
+    }
+    if (a.binv_smem && t_hi > t_lo) {
+      R* sB = reinterpret_cast<R*>(ybase + (size_t)nls * 3 * a.dmax);
+      bsl0 = a.tiles[t_lo].s0;
+      const int nsl = a.tiles[t_hi - 1].s1 - bsl0;
+      const R* g = a.Binv + (size_t)bsl0 * 1024;
+      for (int i = threadIdx.x; i < nsl * 1024; i += kSolveThreads) sB[i] = g[i];
+      Bsrc = sB;
     }
   }
 
@@ -181,16 +201,40 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       a.p[(2 * k + 1) * nv + row] = R(0);
     }
   }
-  if (!grid_sync(a.gb)) return;
+  bool stop = false;
+  if (!grid_sync(a.gb, bar_gen)) return;
 
+  const bool prof = a.prof != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+  unsigned long long tp[6] = {0, 0, 0, 0, 0, 0}, tlast = prof ? gtimer() : 0;
+#define PFEM2_PROF(k)                       \
+  if (prof) {                               \
+    const unsigned long long tn = gtimer(); \
+    tp[k] += tn - tlast;                    \
+    tlast = tn;                             \
+  }
   for (int iter = 0;; ++iter) {
-    if (*(volatile int*)a.active <= 0) break;
+    if (stop) break;  // published by the last barrier: every system is done
     if (iter >= a.iter_cap) {
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.gb.err, 2);
       break;
     }
     const bool phaseA = (iter & 1) == 0;
     const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 3;
+    PFEM2_PROF(5);
+    // ---- Z^T r of the systems about to run phase A (warps 1..), loaded while
+    // warp 0 sums the scalar partials
+    if (TWO && phaseA && warp > 0) {
+      for (int k = 0; k < nls; ++k) {
+        if (ls[k].state != S_A) continue;
+        const int D = ls[k].D, t0 = a.sys_t0[ls[k].sys];
+        float* sf = reinterpret_cast<float*>(sYk[k] + a.dmax);
+        for (int d = threadIdx.x - 32; d < D; d += kSolveThreads - 32) {
+          const double v = __ldcg(prev + (size_t)(t0 + d) * 3 + 2);
+          sSk[k][d] = v;
+          sf[d] = (float)v;
+        }
+      }
+    }
     // ---- sums of the previous phase's partials (warp 0, fixed order)
     if (warp == 0) {
       for (int k = 0; k < nls; ++k) {
@@ -211,18 +255,28 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         }
       }
     }
+    __syncthreads();
+    PFEM2_PROF(0);
     // ---- coarse correction y = E^-1 Z^T r for systems about to run phase A
     if (TWO && phaseA) {
       for (int k = 0; k < nls; ++k) {
         if (ls[k].state != S_A) continue;
         const int D = ls[k].D, t0 = a.sys_t0[ls[k].sys];
-        for (int d = threadIdx.x; d < D; d += kSolveThreads) sSk[k][d] = __ldcg(prev + (size_t)(t0 + d) * 3 + 2);
-        __syncthreads();
+        const float* sf = reinterpret_cast<const float*>(sYk[k] + a.dmax);  // FP32 copy of Z^T r
+        (void)t0;
         for (int j = threadIdx.x; j < D; j += kSolveThreads) {
-          double acc = 0.0;
-          const float* Ej = sEk[k];
-          for (int d = 0; d < D; ++d) acc += (double)Ej[d * D + j] * sSk[k][d];  // E^-1 symmetric
-          sYk[k][j] = acc;
+          // y_j = sum_d E^-1[d][j] s_d (E^-1 symmetric: column reads are conflict free)
+          const float* Ej = sEk[k] + j;
+          float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+          int d = 0;
+          for (; d + 3 < D; d += 4) {
+            a0 = fmaf(Ej[(d + 0) * D], sf[d + 0], a0);
+            a1 = fmaf(Ej[(d + 1) * D], sf[d + 1], a1);
+            a2 = fmaf(Ej[(d + 2) * D], sf[d + 2], a2);
+            a3 = fmaf(Ej[(d + 3) * D], sf[d + 3], a3);
+          }
+          for (; d < D; ++d) a0 = fmaf(Ej[d * D], sf[d], a0);
+          sYk[k][j] = (double)((a0 + a1) + (a2 + a3));
         }
         __syncthreads();
         if (warp == 0) {
@@ -234,6 +288,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       }
     }
     __syncthreads();
+    PFEM2_PROF(1);
     // ---- decisions (thread 0; identical in every block owning the system)
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
@@ -280,6 +335,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       }
     }
     __syncthreads();
+    PFEM2_PROF(2);
     // ---- work on the own tiles
     for (int t = t_lo; t < t_hi; ++t) {
       const Tile T = a.tiles[t];
@@ -318,7 +374,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
           e[row] = R(0);
           if (act == ACT_OUT_B) {
             const R rr = R(r64[row]);
-            const R zz = TWO ? block_jacobi32<R>(a.Binv, sl, rr, lane) : rr * dinv[row];
+            const R zz = TWO ? block_jacobi32<R>(Bsrc, sl - bsl0, rr, lane) : rr * dinv[row];
             r[row] = rr;
             z[row] = zz;
             v0 += (double)rr * (double)zz;
@@ -357,7 +413,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
           const int row = sl * 32 + lane;
           e[row] += alpha * pn[row];
           const R rr = r[row] - alpha * q[row];
-          const R zz = TWO ? block_jacobi32<R>(a.Binv, sl, rr, lane) : rr * dinv[row];
+          const R zz = TWO ? block_jacobi32<R>(Bsrc, sl - bsl0, rr, lane) : rr * dinv[row];
           r[row] = rr;
           z[row] = zz;
           v0 += (double)rr * (double)zz;
@@ -390,6 +446,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       }
       __syncthreads();
     }
+    PFEM2_PROF(3);
     // ---- bookkeeping
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
@@ -404,8 +461,13 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         L.act = ACT_NONE;
       }
     }
-    if (!grid_sync(a.gb)) return;
+    PFEM2_PROF(3);
+    if (!grid_sync(a.gb, bar_gen, a.active, &stop)) return;
+    PFEM2_PROF(4);
   }
+  if (prof)
+    for (int k = 0; k < 6; ++k) atomicAdd(a.prof + k, tp[k]);
+#undef PFEM2_PROF
 }
 
 // ------------------------------------------------------------------ host
@@ -420,6 +482,7 @@ struct KrylovWs {
   bool two_level = false;
   int dmax = 0, nls_max = 1;
   size_t smem_two = 0;
+  int binv_smem = 0;
   void* Binv = nullptr;
   float* Einv = nullptr;
   int *sys_eoff = nullptr, *sys_D = nullptr, *sys_sl0 = nullptr, *sys_sps = nullptr;
@@ -430,6 +493,7 @@ struct KrylovWs {
   int* out_it[3];
   double* out_res[3];
   int* out_outer[3];
+  unsigned long long* prof = nullptr;  // [3 solve kinds][6]
 };
 
 static int max_local_systems(const std::vector<Tile>& tiles, const std::vector<int>& bt0) {
@@ -461,13 +525,18 @@ pfem2_status krylov_setup(Ctx& c) {
     std::vector<Tile> tiles;
     std::vector<int> st0(ncomp * ni + 1, 0);
     if (ph == 0) {
-      // pressure: tiles = coarse subdomains, at most dmax per system
-      const int dcap = ni == 1 ? 208 : 96;
+      // pressure: tiles = coarse subdomains; about one per block of the
+      // persistent grid (balanced work), at most dcap per system
+      const int dcap = ni == 1 ? 160 : 96;
+      const int nb = bps * c.num_sms;
+      long long tot_sl = 0;
+      for (int i = 0; i < ni; ++i) tot_sl += c.inst[i].nv_pad / kSlice;
       w->dmax = 1;
       for (int i = 0; i < ni; ++i) {
         st0[i] = (int)tiles.size();
         const int sl0 = c.inst[i].v_off / kSlice, nsl = c.inst[i].nv_pad / kSlice;
-        int D = std::min((nsl + 7) / 8, dcap);
+        const long long share = std::max<long long>(1, (long long)nb * nsl / tot_sl);
+        int D = (int)std::min<long long>(std::min<long long>(share, dcap), nsl);
         const int sps = (nsl + D - 1) / D;
         D = (nsl + sps - 1) / sps;
         for (int a = 0; a < nsl; a += sps) tiles.push_back(Tile{i, 0, sl0 + a, sl0 + std::min(nsl, a + sps)});
@@ -495,7 +564,7 @@ pfem2_status krylov_setup(Ctx& c) {
       // shared memory for the coarse inverses: sized after the chunking below,
       // first with one local system to bound the grid
       w->nls_max = 1;
-      smem = (size_t)w->dmax * w->dmax * 4 + 8 + 2 * (size_t)w->dmax * 8;
+      smem = (size_t)w->dmax * w->dmax * 4 + 8 + 3 * (size_t)w->dmax * 8;
       occ = c.mixed ? occupancy<float, true>(smem) : occupancy<double, true>(smem);
     } else {
       occ = c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0);
@@ -514,7 +583,15 @@ pfem2_status krylov_setup(Ctx& c) {
     }
     if (ph == 0) {
       w->nls_max = nls;
-      w->smem_two = (size_t)nls * w->dmax * w->dmax * 4 + 8 + 2 * (size_t)nls * w->dmax * 8;
+      w->smem_two = (size_t)nls * w->dmax * w->dmax * 4 + 8 + 3 * (size_t)nls * w->dmax * 8;
+      int maxsl = 0;
+      for (int b = 0; b < G; ++b)
+        if (bt0[b + 1] > bt0[b]) maxsl = std::max(maxsl, tiles[bt0[b + 1] - 1].s1 - tiles[bt0[b]].s0);
+      const size_t bj = (size_t)maxsl * 1024 * rs;
+      if (w->smem_two + bj <= 220 * 1024) {
+        w->smem_two += bj;
+        w->binv_smem = 1;
+      }
       if (w->smem_two > 220 * 1024) {
         set_error("krylov: coarse inverses of the pressure systems exceed shared memory");
         return PFEM2_INVALID_ARG;
@@ -551,6 +628,10 @@ pfem2_status krylov_setup(Ctx& c) {
   PFEM2_CUDA(cudaMalloc(&w->part, sizeof(double) * 6 * maxtiles));
   PFEM2_CUDA(cudaMemset(w->part, 0, sizeof(double) * 6 * maxtiles));
   PFEM2_CUDA(cudaMalloc(&w->active, sizeof(int)));
+  if (getenv("PFEM2_SOLVER_PROFILE")) {
+    PFEM2_CUDA(cudaMalloc(&w->prof, sizeof(unsigned long long) * 18));
+    PFEM2_CUDA(cudaMemset(w->prof, 0, sizeof(unsigned long long) * 18));
+  }
   for (int k = 0; k < 3; ++k) {
     PFEM2_CUDA(cudaMalloc(&w->out_it[k], sizeof(int) * maxsys));
     PFEM2_CUDA(cudaMalloc(&w->out_res[k], sizeof(double) * maxsys));
@@ -712,6 +793,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.sys_sl0 = w->sys_sl0;
   a.sys_sps = w->sys_sps;
   a.dmax = w->dmax;
+  a.binv_smem = w->binv_smem;
   for (int k = 0; k < 3; ++k) {
     const int kk = k < ncomp ? k : 0;
     const int mtx = which == 0 ? kk : (which == 1 ? 3 : 4 + kk);
@@ -751,6 +833,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
+  a.prof = w->prof ? w->prof + 6 * which : nullptr;
   k_init_solve<<<1, 32, 0, c.stream>>>(a.nsys, w->active, c.barrier, c.d_err);
   c.launches++;
   void* args[] = {&a};
@@ -800,6 +883,13 @@ static pfem2_status read_stats_phase(Ctx& c, int which) {
     if (which == 1) c.stats.refinements_p = mo;
   }
   return notconv ? PFEM2_NOT_CONVERGED : PFEM2_OK;
+}
+
+// sub-phase times of block 0 (ns): sums, coarse, decisions, work, barrier, loop
+void krylov_profile(Ctx& c, unsigned long long* out18) {
+  KrylovWs* w = (KrylovWs*)c.kws;
+  if (!w || !w->prof) return;
+  cudaMemcpy(out18, w->prof, sizeof(unsigned long long) * 18, cudaMemcpyDeviceToHost);
 }
 
 pfem2_status krylov_read_stats(Ctx& c) {
