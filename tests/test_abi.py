@@ -97,3 +97,25 @@ def test_create_without_device_fails_loudly():
     with pytest.raises(solver.Pfem2Error) as e:
         solver.Solver(sp)
     assert e.value.status in (A.NO_DEVICE, A.CUDA_ERROR)
+
+
+def test_cpp_shim_compiles_and_links():
+    """the header-only pfem2Solver shim compiles against pfem2.h and links to libpfem2b.so"""
+    from pfem2_b200 import build as B
+    B.build()
+    src = (
+        '#include "pfem2_solver.hpp"\n'
+        "int main(int argc, char**) {\n"
+        "  if (argc > 5) { pfem2_config c{}; pfem2_mesh_view m{}; pfem2_case k{};\n"
+        "    pfem2b::Solver s(c, m, k); s.seed_particles({4, 4}); s.correct_particles_velocities();\n"
+        "    s.move_particles(); s.distribute_particle_velocities_to_grid(); s.fem_step();\n"
+        "    std::ofstream f(\"forces.csv\"); s.calculate_loads(3, &f); s.step(); }\n"
+        "  return pfem2_abi_version() == 1 ? 0 : 1; }\n")
+    with tempfile.TemporaryDirectory() as d:
+        cpp = os.path.join(d, "drv.cpp")
+        exe = os.path.join(d, "drv")
+        open(cpp, "w").write(src)
+        libdir = os.path.dirname(solver.LIB_PATH)
+        subprocess.check_call(["g++", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), cpp, "-o", exe,
+                               "-L", libdir, "-lpfem2b", f"-Wl,-rpath,{libdir}"])
+        assert subprocess.call([exe]) == 0
