@@ -235,6 +235,28 @@ pfem2_status pfem2_get_stream(pfem2_ctx* ctx, void** stream);
 const char* pfem2_last_error(void);
 int32_t pfem2_abi_version(void);
 
+/* ---- projection without allocation ----
+ * No counterpart in the reference. For callers that cannot let the library
+ * call cudaMalloc (a host code that owns all device memory through its own
+ * pool, or work being recorded into a CUDA graph): the particle -> grid
+ * projection of distribute_particle_velocities_to_grid on caller-owned
+ * device buffers, FP64, allocating nothing. Its per-cell scratch is a fixed
+ * device array of PFEM2_NOALLOC_MAX_CELLS cells held by every GPU that loads
+ * the library; larger meshes are rejected with PFEM2_INVALID_ARG. The first
+ * call on a device looks the array up (make it before any stream capture);
+ * calls that overlap on the GPU race on the shared array.
+ *   vertex_cell_ptr [n_vertices+1], vertex_cell / vertex_cell_local: cells
+ *   around each vertex (ascending) and the vertex's local index there;
+ *   cell_start [n_cells+1]: particle offsets, particles sorted by cell;
+ *   xi, u [n_particles][dim]; out node_u [n_vertices][dim], node_w [n_vertices]
+ *   (node_u = 0 where node_w = 0); stream: a cudaStream_t or NULL. */
+#define PFEM2_NOALLOC_MAX_CELLS 65536
+pfem2_status pfem2_project_noalloc(int32_t dim, int32_t n_cells, int32_t n_vertices,
+                                   const int32_t* vertex_cell_ptr, const int32_t* vertex_cell,
+                                   const int32_t* vertex_cell_local, const int32_t* cell_start,
+                                   const double* xi, const double* u, double* node_u, double* node_w,
+                                   void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

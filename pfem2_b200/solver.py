@@ -36,7 +36,7 @@ EXPORTS = [
     "pfem2_step", "pfem2_step_and_read", "pfem2_get_field", "pfem2_set_field", "pfem2_particle_count",
     "pfem2_get_particles", "pfem2_set_particles", "pfem2_get_stats", "pfem2_get_time", "pfem2_synchronize",
     "pfem2_launch_count", "pfem2_stage_times", "pfem2_enable_stage_timing", "pfem2_get_stream",
-    "pfem2_last_error", "pfem2_abi_version",
+    "pfem2_last_error", "pfem2_abi_version", "pfem2_project_noalloc",
 ]
 
 
@@ -75,6 +75,7 @@ def load_library(path=LIB_PATH):
         "pfem2_enable_stage_timing": [vp, C.c_int32],
         "pfem2_get_stream": [vp, C.POINTER(vp)],
     }
+    sig["pfem2_project_noalloc"] = [C.c_int32, C.c_int32, C.c_int32] + [vp] * 8 + [vp]
     for name, args in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
