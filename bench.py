@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--h", type=float, default=0.0088, help="cell size of the channel mesh (~52k cells)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stress-n", type=int, default=2048, help="particle-stress mesh: n x n cells (0 = skip)")
+    ap.add_argument("--ensemble-n", type=int, default=64, help="instances of the batched leg (0 = skip)")
+    ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of the stress and ensemble legs")
     return ap.parse_args()
 
 
@@ -246,6 +249,11 @@ def run_ours(args, rank, world, local):
         s64.close()
         m2.close()
 
+    stress = stress_leg(args, local, flush) if args.stress_n > 0 else None
+    ensemble = None
+    if args.ensemble_n > 0:
+        ensemble = ensemble_leg(args, local, flush, fp64["timesteps_per_s"] if fp64 else None)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sp, threads=1, budget_s=20.0)
@@ -277,6 +285,8 @@ def run_ours(args, rank, world, local):
         "gpu_launches": int(launches),
         "clocks": clk,
         "fp64": fp64,
+        "particle_stress": stress,
+        "ensemble": ensemble,
         "cpu_baseline": cpu,
     }
     s.close()
@@ -285,6 +295,113 @@ def run_ours(args, rank, world, local):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(res), flush=True)
+
+
+def timed_steps(solver, stream, flush, steps):
+    """per-step CUDA events on the library stream, L2 flushed between steps"""
+    import torch
+
+    tot = 0.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0.record(stream)
+        solver.step()
+        e1.record(stream)
+        e1.synchronize()
+        tot += e0.elapsed_time(e1)
+    return tot
+
+
+def stress_leg(args, local, flush):
+    """particle kernels alone (advect + project + correct) on a frozen field:
+    unit square n x n, 4x4 particles per cell uniform in their sub-cells"""
+    import torch
+
+    from pfem2_b200 import _abi as A
+    from pfem2_b200 import cases
+    from pfem2_b200.solver import STAGE_NAMES, Solver
+
+    n = args.stress_n
+    sp = cases.stress_2d(n=n)
+    s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True, particles_only=True, capacity_factor=1.3)
+    ux, uy = sp.meta["ux"], sp.meta["uy"]
+    for f, v in ((A.FIELD_VX, ux), (A.FIELD_VY, uy), (A.FIELD_PRED_VX, ux), (A.FIELD_PRED_VY, uy)):
+        s.set_field(f, v)
+    s.seed_particles(sp.q, sp.seed, sp.jitter)
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+    for _ in range(2):
+        s.step()
+    s.synchronize()
+    s.enable_stage_timing(True)
+    s.stage_times(reset=True)
+    st0 = s.stats()
+    ms = timed_steps(s, stream, flush, args.extra_steps)
+    st = s.stats()
+    stages = s.stage_times()
+    k = args.extra_steps
+    npart = 0.5 * (st0["n_particles"] + st["n_particles"])
+    nc, nv = sp.mesh.n_cells, sp.mesh.n_vertices
+    hbm, kind = peaks()
+    # algorithmic bytes (FP32 SoA): advect reads cell+xi+u (20 B) and writes
+    # xi+u+newcell (20 B) per particle; the rebin passes read newcell (4 B),
+    # then newcell+xi+u (20 B) and write cell+xi+u (20 B) per particle plus
+    # 2 offsets and 48 B of projection partials per cell; the node gather
+    # reads the partials and writes 12 B per node.
+    b_adv = 40.0 * npart
+    b_reb = 44.0 * npart + (8 + 48) * nc
+    b_nod = 48.0 * nc + 28.0 * nv
+    adv_ms = stages[STAGE_NAMES.index("advect")] / k
+    reb_ms = stages[STAGE_NAMES.index("rebin")] / k
+    nod_ms = stages[STAGE_NAMES.index("project_nodes")] / k
+    gbs = lambda b, t: b / (t / 1e3) / 1e9 if t > 0 else None
+    out = {
+        "workload": f"unit square {n}x{n} Q1, 4x4 particles/cell uniform in sub-cells (seed 1), frozen "
+                    f"divergence-free field of 32 random stream-function modes, CFL 0.5; correct+advect+rebin+project",
+        "cells": nc, "particles": int(npart), "ms_per_step": ms / k,
+        "particle_updates_per_s": npart * k / (ms / 1e3),
+        "advect": {"ms": adv_ms, "GB/s": gbs(b_adv, adv_ms), "frac": gbs(b_adv, adv_ms) / hbm if adv_ms else None},
+        "rebin": {"ms": reb_ms, "GB/s": gbs(b_reb, reb_ms), "frac": gbs(b_reb, reb_ms) / hbm if reb_ms else None},
+        "project_nodes": {"ms": nod_ms, "GB/s": gbs(b_nod, nod_ms)},
+        "step_GB/s": gbs(b_adv + b_reb + b_nod, ms / k), "peak": hbm, "peak_kind": kind,
+        "deleted_per_step": st["deleted"], "far_movers": st["far"],
+    }
+    s.close()
+    return out
+
+
+def ensemble_leg(args, local, flush, fp64_single):
+    """many independent channel instances of uneven size in one batch:
+    every stage is one launch for all of them"""
+    import torch
+
+    from pfem2_b200 import _abi as A
+    from pfem2_b200 import cases
+    from pfem2_b200.solver import Solver
+
+    specs = cases.ensemble(n=args.ensemble_n)
+    s = Solver(specs, precision=A.PREC_MIXED, device=local, use_graph=True)
+    s.seed_particles(specs[0].q, 2, 0.0)
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+    for _ in range(3):
+        s.step()
+    s.synchronize()
+    ms = timed_steps(s, stream, flush, args.extra_steps)
+    st = s.stats()
+    cells = sum(sp.mesh.n_cells for sp in specs)
+    inst_steps = len(specs) * args.extra_steps / (ms / 1e3)
+    out = {
+        "workload": f"{len(specs)} channel-with-disk instances, cells log-uniform 5k-60k, Re log-uniform 20-200, "
+                    f"r uniform 0.05-0.15 (seed 2), 5x5 particles/cell, one batch",
+        "instances": len(specs), "cells": cells, "particles": st["n_particles"],
+        "ms_per_batch_step": ms / args.extra_steps, "instance_timesteps_per_s": inst_steps,
+        "cell_updates_per_s": cells * args.extra_steps / (ms / 1e3),
+        "max_pressure_cg_iters": st["iters"][3],
+        "vs_fp64_single_instance_timesteps_per_s": (inst_steps / fp64_single) if fp64_single else None,
+    }
+    s.close()
+    return out
 
 
 def cpu_baseline(sp, threads, budget_s):

@@ -141,6 +141,11 @@ typedef struct {
   double particle_capacity_factor; /* particle storage = factor * seeded count (0 = 2.0) */
   int32_t far_mover_capacity;      /* particles that leave the 1-ring of their cell in one step (0 = auto) */
   int32_t use_graph;               /* capture pfem2_step as a CUDA graph */
+  /* 1: no FEM (no matrices are set up; pfem2_fem_step is refused). pfem2_step
+   * then runs correct -> move -> project on a frozen velocity field held in
+   * PFEM2_FIELD_PRED_V*: after each step V is reset to the frozen field and
+   * V_old to the new projection (the particle-kernel stress workload). */
+  int32_t particles_only;
 } pfem2_config;
 
 typedef struct pfem2_ctx pfem2_ctx;

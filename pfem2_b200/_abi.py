@@ -63,6 +63,7 @@ class Config(C.Structure):
         ("particles_per_cell_max", C.c_int32),
         ("particle_capacity_factor", C.c_double),
         ("far_mover_capacity", C.c_int32), ("use_graph", C.c_int32),
+        ("particles_only", C.c_int32),
     ]
 
 

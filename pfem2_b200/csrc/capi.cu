@@ -160,9 +160,10 @@ static pfem2_status do_setup(Ctx& c) {
     c.ring_max = std::max(c.ring_max, (int)tmp.size());
   }
   // sparsity: per row diagonal first, then ascending columns; SELL-32
-  std::vector<std::vector<int>> rows(nv);
+  // (not needed without FEM)
+  std::vector<std::vector<int>> rows(c.cfg.particles_only ? 0 : nv);
   int maxlen = 1;
-  for (int i = 0; i < nv; ++i) {
+  for (int i = 0; i < (int)rows.size(); ++i) {
     tmp.clear();
     for (int k = v2c_ptr[i]; k < v2c_ptr[i + 1]; ++k)
       for (int b = 0; b < NV; ++b) tmp.push_back(cv[(size_t)v2c_cell[k] * NV + b]);
@@ -174,7 +175,7 @@ static pfem2_status do_setup(Ctx& c) {
       if (j != i) r.push_back(j);
     maxlen = std::max(maxlen, (int)r.size());
   }
-  c.nslices = nv / kSlice;
+  c.nslices = c.cfg.particles_only ? 0 : nv / kSlice;
   std::vector<int> sl_ptr(c.nslices + 1, 0), sl_len(c.nslices);
   for (int s = 0; s < c.nslices; ++s) {
     int L = 1;
@@ -194,8 +195,8 @@ static pfem2_status do_setup(Ctx& c) {
       c.nnz += (int)r.size();
       for (int j = 0; j < sl_len[s]; ++j) sl_col[sl_ptr[s] + j * kSlice + l] = j < (int)r.size() ? r[j] : row;
     }
-  std::vector<int> inc_slot((size_t)c.ninc * NV);
-  for (int i = 0; i < nv; ++i) {
+  std::vector<int> inc_slot(c.cfg.particles_only ? 0 : (size_t)c.ninc * NV);
+  for (int i = 0; i < (int)rows.size(); ++i) {
     auto& r = rows[i];
     int s = i / kSlice, l = i % kSlice;
     for (int k = v2c_ptr[i]; k < v2c_ptr[i + 1]; ++k)
@@ -293,7 +294,7 @@ static pfem2_status do_setup(Ctx& c) {
     c.sys_scalars = t;
     PFEM2_TRY(upload(&c.d_sysinfo, maxit));
   }
-  for (int k = 0; k < kNumSys; ++k) {
+  for (int k = 0; k < kNumSys && !c.cfg.particles_only; ++k) {
     PFEM2_TRY(dalloc(&c.A64[k], c.nell));
     PFEM2_TRY(dalloc(&c.A32[k], c.nell));
     PFEM2_TRY(dalloc(&c.dinv64[k], nv));
@@ -328,10 +329,12 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(dalloc(&c.barrier, 2));
   PFEM2_TRY(dalloc(&c.d_err, 1));
   c.list_cap = c.cfg.particles_per_cell_max > 0 ? c.cfg.particles_per_cell_max : (dim == 2 ? 512 : 1024);
-  PFEM2_TRY(krylov_setup(c));
-  PFEM2_TRY(assemble_matrices(c));
-  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
-  PFEM2_TRY(krylov_setup_precond(c));
+  if (!c.cfg.particles_only) {
+    PFEM2_TRY(krylov_setup(c));
+    PFEM2_TRY(assemble_matrices(c));
+    PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+    PFEM2_TRY(krylov_setup_precond(c));
+  }
   PFEM2_CUDA(cudaGetLastError());
   c.setup_done = true;
   return PFEM2_OK;
@@ -424,6 +427,11 @@ static pfem2_status step_launch(Ctx& c) {
   mark(c, 2);
   PFEM2_TRY(launch_project(c, true));
   mark(c, 3);
+  if (c.cfg.particles_only) {
+    PFEM2_TRY(launch_restore_frozen(c));
+    for (int k = 4; k < 8; ++k) mark(c, k);
+    return PFEM2_OK;
+  }
   PFEM2_TRY(fem_step_launch(c));
   return PFEM2_OK;
 }
@@ -657,6 +665,10 @@ pfem2_status pfem2_project(pfem2_ctx* x) {
 
 pfem2_status pfem2_fem_step(pfem2_ctx* x) {
   SETUP_CHECK(x);
+  if (x->c.cfg.particles_only) {
+    set_error("pfem2_fem_step: the context was created with particles_only");
+    return PFEM2_BAD_STATE;
+  }
   PFEM2_TRY(fem_step_launch(x->c));
   PFEM2_CUDA(cudaStreamSynchronize(x->c.stream));
   PFEM2_CUDA(cudaGetLastError());
@@ -855,7 +867,7 @@ pfem2_status pfem2_get_stats(pfem2_ctx* x, pfem2_stats* out) {
   SETUP_CHECK(x);
   if (!out) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
   pfem2_status s1 = x->c.seeded ? check_counters(x->c, true) : PFEM2_OK;
-  pfem2_status s2 = krylov_read_stats(x->c);
+  pfem2_status s2 = x->c.cfg.particles_only ? PFEM2_OK : krylov_read_stats(x->c);
   *out = x->c.stats;
   return s1 != PFEM2_OK ? s1 : s2;
 }

@@ -195,6 +195,7 @@ pfem2_status launch_rhs_prediction(Ctx& c);
 pfem2_status launch_rhs_pressure(Ctx& c);
 pfem2_status launch_rhs_correction(Ctx& c);
 pfem2_status launch_finish_fem(Ctx& c);
+pfem2_status launch_restore_frozen(Ctx& c);
 pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev);
 
 // krylov.cu

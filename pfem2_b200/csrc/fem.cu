@@ -537,6 +537,41 @@ pfem2_status launch_finish_fem(Ctx& c) {
   return PFEM2_OK;
 }
 
+// particles-only step: V_old = the new projection, V = the frozen field
+template <int DIM, typename R>
+__global__ void k_restore_frozen(int nv, double* __restrict__ V0, double* __restrict__ V1, double* __restrict__ V2,
+                                 double* __restrict__ O0, double* __restrict__ O1, double* __restrict__ O2,
+                                 const double* __restrict__ F0, const double* __restrict__ F1,
+                                 const double* __restrict__ F2, R* __restrict__ Vr, R* __restrict__ dVr) {
+  double* V[3] = {V0, V1, V2};
+  double* O[3] = {O0, O1, O2};
+  const double* Fz[3] = {F0, F1, F2};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double proj = V[d][i], fz = Fz[d][i];
+      O[d][i] = proj;
+      V[d][i] = fz;
+      Vr[(size_t)d * nv + i] = R(fz);
+      dVr[(size_t)d * nv + i] = R(fz - proj);
+    }
+  }
+}
+
+template <int DIM, typename R>
+static void restore_impl(Ctx& c) {
+  k_restore_frozen<DIM, R><<<grid_for(c, c.nv, 256, 8), 256, 0, c.stream>>>(
+      c.nv, c.F[PFEM2_FIELD_VX], c.F[PFEM2_FIELD_VY], c.F[PFEM2_FIELD_VZ], c.F[PFEM2_FIELD_OLD_VX],
+      c.F[PFEM2_FIELD_OLD_VY], c.F[PFEM2_FIELD_OLD_VZ], c.F[PFEM2_FIELD_PRED_VX], c.F[PFEM2_FIELD_PRED_VY],
+      c.F[PFEM2_FIELD_PRED_VZ], (R*)c.Vr, (R*)c.dVr);
+  c.launches++;
+}
+pfem2_status launch_restore_frozen(Ctx& c) {
+  if (c.dim == 2) { if (c.mixed) restore_impl<2, float>(c); else restore_impl<2, double>(c); }
+  else { if (c.mixed) restore_impl<3, float>(c); else restore_impl<3, double>(c); }
+  return PFEM2_OK;
+}
+
 // ---------------------------------------------------------------- loads
 // One block; FP64 face integrals over the instance's cells (fixed-order
 // block reduction, so the result is deterministic).

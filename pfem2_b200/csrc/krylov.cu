@@ -527,6 +527,8 @@ pfem2_status krylov_setup(Ctx& c) {
     if (ph == 0) {
       // pressure: tiles = coarse subdomains; about one per block of the
       // persistent grid (balanced work), at most dcap per system
+      // (a batch: subdomains of ~8 slices, at most dcap per system, so every
+      // instance gets a coarse space of its own size)
       const int dcap = ni == 1 ? 160 : 96;
       const int nb = bps * c.num_sms;
       long long tot_sl = 0;
@@ -535,7 +537,7 @@ pfem2_status krylov_setup(Ctx& c) {
       for (int i = 0; i < ni; ++i) {
         st0[i] = (int)tiles.size();
         const int sl0 = c.inst[i].v_off / kSlice, nsl = c.inst[i].nv_pad / kSlice;
-        const long long share = std::max<long long>(1, (long long)nb * nsl / tot_sl);
+        const long long share = ni == 1 ? std::max<long long>(1, (long long)nb * nsl / tot_sl) : (nsl + 7) / 8;
         int D = (int)std::min<long long>(std::min<long long>(share, dcap), nsl);
         const int sps = (nsl + D - 1) / D;
         D = (nsl + sps - 1) / sps;

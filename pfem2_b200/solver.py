@@ -99,7 +99,7 @@ class Solver:
     """pfem2Solver over a batch of instances (one instance = one case)."""
 
     def __init__(self, specs, precision=A.PREC_MIXED, device=0, movement_steps=None, max_per_part=None,
-                 use_graph=True, capacity_factor=2.0, per_cell_max=0):
+                 use_graph=True, capacity_factor=2.0, per_cell_max=0, particles_only=False):
         if not isinstance(specs, (list, tuple)):
             specs = [specs]
         self.L = load_library()
@@ -115,6 +115,7 @@ class Solver:
         cfg.particle_capacity_factor = capacity_factor
         cfg.far_mover_capacity = 0
         cfg.use_graph = 1 if use_graph else 0
+        cfg.particles_only = 1 if particles_only else 0
         self.cfg = cfg
         h = C.c_void_p()
         self._check(self.L.pfem2_create(C.byref(cfg), C.byref(h)))

@@ -24,7 +24,7 @@ STRUCTS = {
     "pfem2_mesh_view": (A.MeshView, ["n_vertices", "n_cells", "vertices", "cells", "face_boundary_id"]),
     "pfem2_config": (A.Config, ["dim", "precision", "device", "movement_steps", "max_particles_per_cell_part",
                                 "particles_per_cell_max", "particle_capacity_factor", "far_mover_capacity",
-                                "use_graph"]),
+                                "use_graph", "particles_only"]),
     "pfem2_stats": (A.Stats, ["n_particles", "n_deleted_last_move", "n_removed_last_check",
                               "n_reseeded_last_check", "n_far_movers_last_move", "iters", "residual",
                               "refinements_p"]),

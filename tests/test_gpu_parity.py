@@ -239,3 +239,51 @@ def test_deterministic():
         outs.append([s.field(f) for f in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P)])
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_particles_only_step(prec):
+    """the particle-kernel workload: correct -> move -> project on a frozen field"""
+    sp = cases.stress_2d(n=24)
+    g = Solver(sp, precision=prec, particles_only=True)
+    o = O.Oracle(sp.mesh, sp.case, movement_steps=sp.movement_steps, max_per_part=sp.max_per_part)
+    ux, uy = sp.meta["ux"], sp.meta["uy"]
+    for f, v in ((A.FIELD_VX, ux), (A.FIELD_VY, uy), (A.FIELD_PRED_VX, ux), (A.FIELD_PRED_VY, uy)):
+        g.set_field(f, v)
+    o.set_field(A.FIELD_VX, ux)
+    o.set_field(A.FIELD_VY, uy)
+    g.seed_particles(sp.q, sp.seed, sp.jitter)
+    o.seed_particles(sp.q, sp.seed, sp.jitter)
+    for _ in range(3):
+        g.step()
+        o.correct_particles_velocities()
+        o.move_particles()
+        o.distribute_particle_velocities_to_grid()
+        proj = [o.field(A.FIELD_VX), o.field(A.FIELD_VY)]
+        o.set_field(A.FIELD_OLD_VX, proj[0])
+        o.set_field(A.FIELD_OLD_VY, proj[1])
+        o.set_field(A.FIELD_VX, ux)
+        o.set_field(A.FIELD_VY, uy)
+        oproj = proj
+    gproj = [g.field(A.FIELD_OLD_VX), g.field(A.FIELD_OLD_VY)]
+    tol = {A.PREC_FP64: 1e-12, A.PREC_MIXED: 1e-4}[prec]
+    for d in range(2):
+        assert rel_l2(gproj[d], oproj[d]) <= tol
+    r = compare_particles(o.particles(), g.particles(), FACE_EPS[prec], XI_TOL[prec],
+                          1e-12 if prec == A.PREC_FP64 else 1e-4)
+    if prec == A.PREC_FP64:
+        assert r["flips"] == 0
+
+
+def test_ensemble_batch_runs():
+    """a small batch of uneven channel instances converges in every stage"""
+    specs = cases.ensemble(n=4, cells_lo=2000, cells_hi=6000)
+    s = Solver(specs, precision=A.PREC_MIXED)
+    s.seed_particles(specs[0].q, 2, 0.0)
+    for _ in range(2):
+        s.step()
+    st = s.stats()
+    assert st["status"] == A.OK
+    for i in range(len(specs)):
+        v = s.field(A.FIELD_VX, i)
+        assert np.all(np.isfinite(v)) and np.abs(v).max() < 10.0
