@@ -325,7 +325,7 @@ def stress_leg(args, local, flush):
 
     n = args.stress_n
     sp = cases.stress_2d(n=n)
-    s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True, particles_only=True, capacity_factor=1.3)
+    s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True, particles_only=True, capacity_factor=3.0)
     ux, uy = sp.meta["ux"], sp.meta["uy"]
     for f, v in ((A.FIELD_VX, ux), (A.FIELD_VY, uy), (A.FIELD_PRED_VX, ux), (A.FIELD_PRED_VY, uy)):
         s.set_field(f, v)

@@ -39,7 +39,7 @@ def build_solver(args):
         s.seed_particles(sp.q, sp.seed, sp.jitter)
     elif args.case == "stress":
         sp = cases.stress_2d(n=args.n or 2048)
-        s = Solver(sp, precision=prec, particles_only=True, capacity_factor=1.3)
+        s = Solver(sp, precision=prec, particles_only=True, capacity_factor=3.0)
         for f, v in ((A.FIELD_VX, sp.meta["ux"]), (A.FIELD_VY, sp.meta["uy"]), (A.FIELD_PRED_VX, sp.meta["ux"]),
                      (A.FIELD_PRED_VY, sp.meta["uy"])):
             s.set_field(f, v)

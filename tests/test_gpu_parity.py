@@ -210,7 +210,10 @@ def test_fused_step_equals_member_calls():
 
 
 def test_batched_equals_single():
-    """two instances in one batch give the same bits as each instance alone."""
+    """two instances in one batch give the instances' own results: bit for bit
+    in the particle kernels and the Jacobi solves; the pressure solve of a
+    batch uses per-instance coarse subdomains of its own size, so there the
+    fields agree to the solver tolerance."""
     s1 = spec_2d(dt=0.01)
     s2 = cases.poiseuille_2d(nx=20, ny=8)
     s2.case.dt = 0.008
@@ -224,8 +227,9 @@ def test_batched_equals_single():
         for s in (both, one, two):
             s.step()
     for fld in (A.FIELD_VX, A.FIELD_P):
-        assert np.array_equal(both.field(fld, 0), one.field(fld, 0))
-        assert np.array_equal(both.field(fld, 1), two.field(fld, 0))
+        assert rel_l2(both.field(fld, 0), one.field(fld, 0)) <= 1e-6
+        assert rel_l2(both.field(fld, 1), two.field(fld, 0)) <= 1e-6
+    assert both.n_particles(0) == one.n_particles(0) and both.n_particles(1) == two.n_particles(0)
 
 
 def test_deterministic():
