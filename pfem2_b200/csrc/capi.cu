@@ -49,6 +49,7 @@ static pfem2_status upload(T** p, const std::vector<T>& v) {
     if (s_ != PFEM2_OK) return s_;           \
   } while (0)
 
+
 // host pinned mirror of the step counters (deferred error reporting)
 struct StepMirror {
   int counters[CNT_N];
@@ -61,6 +62,67 @@ static double bc_value(const pfem2_dirichlet& d, const double* x) {
     return d.value * 4.0 * (s - d.a) * (d.b - s) / (L * L);
   }
   return d.value;
+}
+
+// per-cell geometry records of the particle kernels (FP64 math, stored in R)
+template <int DIM, typename R>
+static pfem2_status upload_cell_geo(Ctx& c, const std::vector<double>& X, const std::vector<int>& cv) {
+  constexpr int NV = 1 << DIM;
+  std::vector<CellGeo<DIM, R>> geo(c.nc);
+  for (int ce = 0; ce < c.nc; ++ce) {
+    CellGeo<DIM, R>& g = geo[ce];
+    double D[NV][DIM];
+    const int g0 = cv[(size_t)ce * NV];
+    for (int a = 0; a < DIM; ++a) g.x0[a] = X[(size_t)g0 * DIM + a];
+    double scale = 0.0;
+    for (int v = 0; v < NV; ++v)
+      for (int a = 0; a < DIM; ++a) {
+        D[v][a] = X[(size_t)cv[(size_t)ce * NV + v] * DIM + a] - g.x0[a];
+        scale = std::max(scale, std::fabs(D[v][a]));
+        if (v > 0) g.D[v - 1][a] = (R)D[v][a];
+      }
+    // Jacobian at the centre: dx_a/dxi_b = sum_v D_v,a dN_v/dxi_b (xi = 1/2)
+    double J[DIM * DIM] = {};
+    for (int v = 0; v < NV; ++v)
+      for (int b = 0; b < DIM; ++b) {
+        const double sgn = ((v >> b) & 1) ? 1.0 : -1.0;
+        const double w = sgn * std::pow(0.5, DIM - 1);
+        for (int a = 0; a < DIM; ++a) J[a * DIM + b] += D[v][a] * w;
+      }
+    double Ji[DIM * DIM];
+    double det;
+    if (DIM == 2) {
+      det = J[0] * J[3] - J[1] * J[2];
+      Ji[0] = J[3] / det; Ji[1] = -J[1] / det; Ji[2] = -J[2] / det; Ji[3] = J[0] / det;
+    } else {
+      const double a = J[0], b = J[1], cc = J[2], d = J[3], e = J[4], f = J[5], gg = J[6], h = J[7], i = J[8];
+      const double A = e * i - f * h, B = -(d * i - f * gg), Cc = d * h - e * gg;
+      det = a * A + b * B + cc * Cc;
+      Ji[0] = A / det; Ji[1] = -(b * i - cc * h) / det; Ji[2] = (b * f - cc * e) / det;
+      Ji[3] = B / det; Ji[4] = (a * i - cc * gg) / det; Ji[5] = -(a * f - cc * d) / det;
+      Ji[6] = Cc / det; Ji[7] = -(a * h - b * gg) / det; Ji[8] = (a * e - b * d) / det;
+    }
+    if (!(det > 0.0)) {
+      set_error("mesh: a cell has a non-positive Jacobian");
+      return PFEM2_MESH_ERROR;
+    }
+    for (int k = 0; k < DIM * DIM; ++k) g.Ji[k] = (R)Ji[k];
+    // affine: every vertex offset is the sum of the edge offsets of its bits
+    bool aff = true;
+    for (int v = 0; v < NV && aff; ++v)
+      for (int a = 0; a < DIM; ++a) {
+        double s = 0.0;
+        for (int b = 0; b < DIM; ++b)
+          if ((v >> b) & 1) s += D[1 << b][a];
+        if (std::fabs(D[v][a] - s) > 1e-13 * scale) { aff = false; break; }
+      }
+    g.affine = aff ? 1 : 0;
+  }
+  CellGeo<DIM, R>* dptr = nullptr;
+  const pfem2_status st = upload(&dptr, geo);
+  if (st != PFEM2_OK) return st;
+  c.cell_geo = dptr;
+  return PFEM2_OK;
 }
 
 // --------------------------------------------------------------- setup
@@ -253,6 +315,7 @@ static pfem2_status do_setup(Ctx& c) {
     d.open_mask = in.cs.open_boundary_mask;
     d.q[0] = d.q[1] = d.q[2] = 1;
     d.max_per_part = c.cfg.max_particles_per_cell_part;
+    d.dt_sub = in.cs.dt / c.cfg.movement_steps;
     d.v_off = in.v_off; d.nv_pad = in.nv_pad; d.c_off = in.c_off; d.nc = in.nc;
     tols[i] = in.cs.vel_tol;
     tols[c.inst.size() + i] = in.cs.p_tol;
@@ -275,6 +338,8 @@ static pfem2_status do_setup(Ctx& c) {
   } else {
     c.v2c_dir_r = c.v2c_dir;
   }
+  if (dim == 2) PFEM2_TRY((c.mixed ? upload_cell_geo<2, float>(c, X, cv) : upload_cell_geo<2, double>(c, X, cv)));
+  else PFEM2_TRY((c.mixed ? upload_cell_geo<3, float>(c, X, cv) : upload_cell_geo<3, double>(c, X, cv)));
   PFEM2_TRY(upload(&c.ring_ptr, ring_ptr));
   PFEM2_TRY(upload(&c.ring_cell, ring_cell));
   PFEM2_TRY(upload(&c.sl_ptr, sl_ptr));
@@ -538,7 +603,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   for (int k = 0; k < 2; ++k)
     if (x->graph[k]) cudaGraphExecDestroy(x->graph[k]);
   // device memory is released with the context's allocations; free the big ones
-  void* ptrs[] = {c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
+  void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.d_inst,
                   c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.cell_count, c.d_np, c.d_counters,
                   c.far_keys, c.scan_tmp, c.barrier, c.d_err, c.newcell};

@@ -110,6 +110,30 @@ __device__ __forceinline__ void local_jacobian(const LocalCell<DIM, R>& L, const
       for (int b = 0; b < DIM; ++b) J[a * DIM + b] += L.D[v][a] * dN[v * DIM + b];
 }
 
+// Per-cell geometry record of the particle kernels: origin X_0 (FP64),
+// vertex offsets D_v = X_v - X_0 (v >= 1) and the inverse Jacobian at the
+// cell centre in the arithmetic type, and whether the map is affine (then
+// xi = Ji (x - X_0) exactly and no Newton iteration is needed).
+template <int DIM, typename R> struct __align__(16) CellGeo {
+  double x0[DIM];
+  R D[Dims<DIM>::NV - 1][DIM];
+  R Ji[DIM * DIM];
+  int affine;
+};
+
+template <int DIM, typename R>
+__device__ __forceinline__ void geo_to_local(const CellGeo<DIM, R>& g, LocalCell<DIM, R>& L, double* x0) {
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    x0[a] = g.x0[a];
+    L.D[0][a] = R(0);
+  }
+#pragma unroll
+  for (int v = 1; v < Dims<DIM>::NV; ++v)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) L.D[v][a] = g.D[v - 1][a];
+}
+
 template <typename R> struct NewtonTol;
 template <> struct NewtonTol<double> {
   static constexpr double step = 1e-12;
@@ -127,6 +151,56 @@ template <int DIM, typename R>
 __device__ __forceinline__ bool local_inverse(const LocalCell<DIM, R>& L, const R* x, R* xi) {
 #pragma unroll
   for (int d = 0; d < DIM; ++d) xi[d] = R(0.5);
+  for (int it = 0; it < NewtonTol<R>::iters; ++it) {
+    R F[DIM], J[DIM * DIM], Ji[DIM * DIM];
+    local_map<DIM, R>(L, xi, F);
+    local_jacobian<DIM, R>(L, xi, J);
+    R det = det_inv<DIM, R>(J, Ji);
+    if (!(det > R(0))) return false;
+    R mx = R(0);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      R s = R(0);
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) s += Ji[a * DIM + b] * (F[b] - x[b]);
+      xi[a] -= s;
+      mx = fmax(mx, fabs(s));
+    }
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+      if (!(fabs(xi[a]) < R(1e6))) return false;
+    if (mx < NewtonTol<R>::step) return true;
+  }
+  return false;
+}
+
+// Inverse map with the cell record: direct for affine cells, otherwise
+// Newton started from the linearisation at the cell centre.
+template <int DIM, typename R>
+__device__ __forceinline__ bool geo_inverse(const CellGeo<DIM, R>& g, const LocalCell<DIM, R>& L, const R* x,
+                                            R* xi) {
+  if (g.affine) {
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      R s = R(0);
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) s += g.Ji[a * DIM + b] * x[b];
+      xi[a] = s;
+    }
+    return true;
+  }
+  R c[DIM];
+  R half[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) half[d] = R(0.5);
+  local_map<DIM, R>(L, half, c);
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    R s = R(0.5);
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) s += g.Ji[a * DIM + b] * (x[b] - c[b]);
+    xi[a] = s;
+  }
   for (int it = 0; it < NewtonTol<R>::iters; ++it) {
     R F[DIM], J[DIM * DIM], Ji[DIM * DIM];
     local_map<DIM, R>(L, xi, F);

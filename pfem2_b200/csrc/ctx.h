@@ -19,6 +19,7 @@ constexpr int kNumSys = 7;          // pred x,y,z, pressure, mass x,y,z
 // Per-instance parameters visible to kernels.
 struct DevInst {
   double mu, rho, dt, open_flux;
+  double dt_sub;  // dt / PARTICLES_MOVEMENT_STEPS
   unsigned open_mask;
   int q[3];
   int max_per_part;
@@ -69,6 +70,7 @@ struct Ctx {
   unsigned char* v2c_loc = nullptr;
   double* v2c_dir = nullptr;
   void* v2c_dir_r = nullptr;  // Real copy for the particle kernels
+  void* cell_geo = nullptr;   // [nc] CellGeo<dim, Real>: local frame, inverse Jacobian, affine flag
   int* ring_ptr = nullptr;
   int* ring_cell = nullptr;
   DevInst* d_inst = nullptr;

@@ -184,7 +184,7 @@ pfem2_status launch_correct(Ctx& c) {
 template <int DIM, typename R, bool FUSE>
 __global__ void __launch_bounds__(256) k_advect(
     const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
-    const int* __restrict__ d_np, const double* __restrict__ X, const int* __restrict__ cv,
+    const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
     const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
     const int* __restrict__ cell_inst, const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
     const R* __restrict__ v2c_dir, const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell,
@@ -209,10 +209,12 @@ __global__ void __launch_bounds__(256) k_advect(
         for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
       }
     }
-    const R dts = R(inst[__ldg(cell_inst + c0)].dt / S);
+    const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
+    CellGeo<DIM, R> G = geo[c];
     LocalCell<DIM, R> L;
     double x0[DIM];
-    load_local_cell<DIM, R>(X, cv, c, L, x0);
+    geo_to_local<DIM, R>(G, L, x0);
+    (void)S;
     bool alive = true;
     for (int s = 0; s < S && alive; ++s) {
       shape_values<DIM, R>(x, N);
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(256) k_advect(
       local_map<DIM, R>(L, x, xo);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) xn[d] = xo[d] + uf[d] * dts;
-      if (local_inverse<DIM, R>(L, xn, x2) && inside_unit<DIM, R>(x2)) {
+      if (geo_inverse<DIM, R>(G, L, xn, x2) && inside_unit<DIM, R>(x2)) {
 #pragma unroll
         for (int d = 0; d < DIM; ++d) x[d] = x2[d];
         continue;
@@ -287,15 +289,17 @@ __global__ void __launch_bounds__(256) k_advect(
       bool found = false;
       for (int i = 0; i < nk && !found; ++i) {
         const int cc = __ldg(v2c_cell + k0 + perm[i]);
+        const CellGeo<DIM, R> Gc = geo[cc];
         LocalCell<DIM, R> Lc;
         double xc[DIM];
-        load_local_cell<DIM, R>(X, cv, cc, Lc, xc);
+        geo_to_local<DIM, R>(Gc, Lc, xc);
         R t[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) t[d] = xn[d] + R(x0[d] - xc[d]);
-        if (local_inverse<DIM, R>(Lc, t, x2) && inside_unit<DIM, R>(x2)) {
+        if (geo_inverse<DIM, R>(Gc, Lc, t, x2) && inside_unit<DIM, R>(x2)) {
           found = true;
           c = cc;
+          G = Gc;
           L = Lc;
 #pragma unroll
           for (int d = 0; d < DIM; ++d) {
@@ -361,12 +365,14 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
   int S = c.cfg.movement_steps;
   if (fuse)
     k_advect<DIM, R, true><<<grid, 256, 0, c.stream>>>(
-        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b, c.X, c.cv, (const R*)c.Vr,
+        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
+        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr,
         (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
         c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
   else
     k_advect<DIM, R, false><<<grid, 256, 0, c.stream>>>(
-        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b, c.X, c.cv, (const R*)c.Vr,
+        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
+        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr,
         (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
         c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
   c.launches++;
@@ -423,10 +429,13 @@ __device__ __forceinline__ void proj_store(ProjAcc<DIM, R>& acc, R* __restrict__
   }
 }
 
-// sub-cell index of check_cell_for_empty_parts: unsigned(xi / h), which is q
-// for xi == 1 (a bucket of its own, as in the reference); clamped to [0, q]
+// sub-cell index of check_cell_for_empty_parts: unsigned(xi / h) with
+// h = 1.0 / q, which is q for xi == 1 (a bucket of its own, as in the
+// reference); clamped to [0, q]. xi * q has the same integer part unless it
+// lies within rounding of an integer, and only there the quotient is formed.
 __device__ __forceinline__ int sub_bucket(double xi, double h, int q) {
-  double t = xi / h;
+  double t = xi * (double)q;
+  if (fabs(t - rint(t)) <= 1e-12 * fmax(1.0, fabs(t))) t = xi / h;
   if (!(t >= 0.0)) t = 0.0;
   if (t > (double)q) t = (double)q;
   return (int)(unsigned)t;
@@ -458,18 +467,48 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
   int nfar = counters[CNT_FAR];
   if (nfar > far_cap) nfar = far_cap;
   for (int c = blockIdx.x * kRebinWarps + warp; c < nc; c += gridDim.x * kRebinWarps) {
+    // gather the incoming particles of c in (ring cell, segment) order: the
+    // ring's segment bounds are loaded across lanes, then the first 32
+    // new-cell ids of 8 segments at a time, so the loads overlap
     int n_in = 0;
-    const int r1 = __ldg(ring_ptr + c + 1);
-    for (int r = __ldg(ring_ptr + c); r < r1; ++r) {
-      const int s = __ldg(ring_cell + r);
-      const int b = min(old_start[s], (int)cap), e = min(old_start[s + 1], (int)cap);
-      for (int base = b; base < e; base += 32) {
-        const int p = base + lane;
-        const bool pred = p < e && newcell[p] == c;
-        const unsigned m = __ballot_sync(PFEM2_FULL_MASK, pred);
-        const int pos = n_in + __popc(m & lt);
-        if (pred && pos < list_cap) list[pos] = p;
-        n_in += __popc(m);
+    const int r0 = __ldg(ring_ptr + c), nr = __ldg(ring_ptr + c + 1) - r0;
+    for (int kb = 0; kb < nr; kb += 32) {
+      int sb = 0, se = 0;
+      if (kb + lane < nr) {
+        const int s = __ldg(ring_cell + r0 + kb + lane);
+        sb = min(old_start[s], (int)cap);
+        se = min(old_start[s + 1], (int)cap);
+      }
+      const int ng = min(32, nr - kb);
+      for (int k0 = 0; k0 < ng; k0 += 8) {
+        int v[8], bs[8], es[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          bs[j] = __shfl_sync(PFEM2_FULL_MASK, sb, (k0 + j) & 31);
+          es[j] = __shfl_sync(PFEM2_FULL_MASK, se, (k0 + j) & 31);
+          const int p = bs[j] + lane;
+          v[j] = (k0 + j < ng && p < es[j]) ? newcell[p] : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (k0 + j >= ng) break;
+          {
+            const int p = bs[j] + lane;
+            const bool pred = v[j] == c;
+            const unsigned m = __ballot_sync(PFEM2_FULL_MASK, pred);
+            const int pos = n_in + __popc(m & lt);
+            if (pred && pos < list_cap) list[pos] = p;
+            n_in += __popc(m);
+          }
+          for (int base = bs[j] + 32; base < es[j]; base += 32) {  // segments longer than a warp
+            const int p = base + lane;
+            const bool pred = p < es[j] && newcell[p] == c;
+            const unsigned m = __ballot_sync(PFEM2_FULL_MASK, pred);
+            const int pos = n_in + __popc(m & lt);
+            if (pred && pos < list_cap) list[pos] = p;
+            n_in += __popc(m);
+          }
+        }
       }
     }
     if (nfar > 0) {
