@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpfem2b.so")
-SOURCES = ["capi.cu", "particles.cu", "fem.cu", "krylov.cu", "project_noalloc.cu"]
+SOURCES = ["capi.cu", "particles.cu", "fem.cu", "krylov.cu", "amg.cu", "project_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

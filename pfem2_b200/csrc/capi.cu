@@ -43,11 +43,6 @@ static pfem2_status upload(T** p, const std::vector<T>& v) {
   return PFEM2_OK;
 }
 
-#define PFEM2_TRY(x)                         \
-  do {                                       \
-    pfem2_status s_ = (x);                   \
-    if (s_ != PFEM2_OK) return s_;           \
-  } while (0)
 
 
 // host pinned mirror of the step counters (deferred error reporting)
@@ -602,6 +597,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   }
   for (int k = 0; k < 2; ++k)
     if (x->graph[k]) cudaGraphExecDestroy(x->graph[k]);
+  krylov_free(c);
   // device memory is released with the context's allocations; free the big ones
   void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.d_inst,

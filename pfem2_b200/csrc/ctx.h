@@ -138,7 +138,7 @@ struct Ctx {
   int coop_blocks = 0;
   int solve_threads = 256;
   int solve_blocks_per_sm = 1;  // persistent Krylov grid: blocks per SM
-  bool two_level = true;        // pressure: block-Jacobi(32) + coarse correction
+  bool two_level = true;        // pressure: multigrid preconditioner (else Jacobi)
   double refine_eta = 1e-3;     // mixed: inner residual reduction per FP64 refinement
 
   // graph
@@ -173,6 +173,12 @@ pfem2_status cuda_status(cudaError_t e, const char* where);
     if (e_ != cudaSuccess) return ::pfem2::cuda_status(e_, #call);    \
   } while (0)
 
+#define PFEM2_TRY(x)                         \
+  do {                                       \
+    pfem2_status s_ = (x);                   \
+    if (s_ != PFEM2_OK) return s_;           \
+  } while (0)
+
 inline int grid_for(const Ctx& c, long long n, int threads, int per_sm = 8) {
   long long b = (n + threads - 1) / threads;
   long long cap = (long long)c.num_sms * per_sm;
@@ -203,6 +209,7 @@ pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev);
 // krylov.cu
 pfem2_status krylov_setup(Ctx& c);
 pfem2_status krylov_setup_precond(Ctx& c);
+void krylov_free(Ctx& c);
 // which: 0 prediction (dim systems per instance), 1 pressure, 2 correction
 pfem2_status krylov_solve(Ctx& c, int which);
 pfem2_status krylov_read_stats(Ctx& c);

@@ -5,40 +5,43 @@
 // instances) to the reference's stopping rule: the absolute 2-norm of the
 // unpreconditioned residual b - A x <= tol within max_iter iterations
 // (deal.II SolverControl(max_iter, tol), cylinder2D/cylinder2D.cc:736-779).
-// The reference runs BiCGStab with Jacobi (velocity) / SSOR (pressure); the
-// prediction, mass and Poisson matrices here are symmetric positive definite
-// after the symmetric Dirichlet elimination, so CG reaches the same solution.
+// The reference runs BiCGStab with Jacobi (velocity) / SSOR or AMG
+// (pressure); the prediction, mass and Poisson matrices here are symmetric
+// positive definite after the symmetric Dirichlet elimination, so CG reaches
+// the same solution.
 //
-// Each CG iteration is two phases separated by a bounded grid barrier:
-//   A  p' = z + beta p ; q = A (z + beta p)     (p double buffered)  | (p', q)
-//   B  e += alpha p' ; r -= alpha q ; z = M^-1 r                    | (r, z), (r, r), sum r
-// Every block that owns tiles of a system computes that system's scalars
-// itself, from the per-tile partial sums of the previous phase, in a fixed
-// order: no block publishes scalars and no phase waits for a finalizer.
+// The work between two bounded grid barriers is a "phase". Every block that
+// owns tiles of a system computes that system's scalars itself, from the
+// per-tile partial sums of the previous phase, in a fixed order: no block
+// publishes scalars and no phase waits for a finalizer.
 //
-// Preconditioners: Jacobi for the prediction and mass systems; for the
-// pressure Poisson system an additive two-level preconditioner
-//   M^-1 = B^-1 + Z E^-1 Z^T,
-// B = the 32x32 diagonal blocks of A (one SELL slice = one warp, inverted at
-// setup, applied with warp shuffles), Z = indicator vectors of the tiles of
-// the system (contiguous runs of slices), E = Z^T A Z (inverted at setup,
-// FP32 copy in shared memory). The coarse part needs the tile sums of r,
-// which are partials of phase B anyway, so it is applied on the fly in
-// phase A (z_i = (B^-1 r)_i + y_tile(i), y = E^-1 Z^T r) and costs no
-// extra barrier.
+// Jacobi-preconditioned systems (prediction, mass) take two phases per
+// iteration:
+//   A  p' = z + beta p ; q = A p'                 (p double buffered) | (p', q)
+//   B  e += alpha p' ; r -= alpha q ; z = D^-1 r                     | (r, z), (r, r)
+// The pressure systems are preconditioned with one multigrid V(1,1) cycle
+// in additive form (amg.h) and take four:
+//   B   e += alpha p' ; r' = r - alpha q (r double buffered) ;
+//       b1 = R01 r' (level-1 rows of the block, r' formed on the fly)  | (r', r')
+//   D   b2 = R12 b1 ; b3 = R13 b1
+//   UZ  x3 = E^-1 b3, x2 = J2 b2 + Pt2 x3, x1 = J1 b1 + Pt1 x2 on the
+//       block's own and halo coarse dofs (shared memory, redundant across
+//       blocks), z = J0 r + Pt0 x1 on the own rows                  | (r, z)
+//   A   p' = z + beta p ; q = A p'                                  | (p', q)
+// so the coarse levels never need a barrier of their own.
 //
 // The iterate is split x + e: e accumulates in the inner type R (FP32 for
 // the mixed path, FP64 for the plain path); once the recurrence residual
 // has dropped below max(eta * res, tol / 2) a reliable update runs in FP64
-// (phase A: r64 = b - A64 (x + e); phase B: x += e, e = 0, r = r64) and CG
-// restarts from the true residual. A system is done when the FP64 residual
-// is <= tol.
+// (r64 = b - A64 (x + e), then x += e, e = 0, r = r64) and CG restarts from
+// the true residual. A system is done when the FP64 residual is <= tol.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
 #include <vector>
 
+#include "amg.h"
 #include "common.cuh"
 #include "ctx.h"
 
@@ -48,10 +51,8 @@ constexpr int kSolveThreads = 384;  // 12 warps
 constexpr int kWarps = kSolveThreads / 32;
 constexpr int kMaxLocalSys = 16;
 
-// system states (A states act in even iterations, B states in odd ones)
-enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4 };
-// actions
-enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5 };
+enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_D = 5, S_UZ = 6 };
+enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_D = 6, ACT_UZ = 7 };
 
 template <typename R> struct SolveArgs {
   int ncomp, ninst, nsys, ntiles, nv;
@@ -64,25 +65,33 @@ template <typename R> struct SolveArgs {
   const double* A64[3];
   const R* Ain[3];
   const R* dinv[3];
-  // two-level data (pressure phase)
-  const R* Binv;         // [nslices][32 cols][32 rows]
-  const float* Einv;     // per system D_s x D_s (symmetric), at sys_eoff[s]
-  const int* sys_eoff;
-  const int* sys_D;      // coarse size = tiles of the system
-  const int* sys_sl0;    // first slice of the system
-  const int* sys_sps;    // slices per tile (= per coarse subdomain)
-  int dmax;              // max D over systems (smem stride)
-  int binv_smem;         // 1: this block's B^-1 slices are staged in shared memory
+  // multigrid (pressure phase), layout of MgHost
+  const int *toff1, *toff2, *toff3;     // [ntiles+1]
+  const int *lsys1, *lsys2, *lsys3;     // system of each level-l dof
+  const int *r01_ptr, *r01_col, *r12_ptr, *r12_col, *r13_ptr, *r13_col;
+  const R *r01_val, *r12_val, *r13_val;
+  const R* j0;                          // [nell]
+  const int *p0_ptr, *p0_len, *p0_col;  // SELL per slice, columns into the block's level-1 list
+  const R* p0_val;
+  const int *blk_s1, *s1_sys, *s1_jptr, *s1_jcol, *s1_pptr, *s1_pcol;
+  const R *s1_jval, *s1_pval;
+  const int *blk_s2, *s2_sys, *s2_jptr, *s2_jcol, *s2_pptr, *s2_pcol;
+  const R *s2_jval, *s2_pval;
+  const int *blk_s3, *s3_sys, *s3_eoff, *blk_e;
+  const float* s3_E;
+  const int *sys_D3, *sys_off3;
+  int dmax, s1max, s2max, s3max;
+  R *b1, *b2, *b3;
   double* x[3];
   const double* b[3];
   const unsigned char* isd[3];
   const double* g[3];    // Dirichlet values preset in x (nullptr -> 0)
   const double* tol_i;   // per instance
   const int* maxit_i;    // per instance
-  // workspace per component slot, nv entries each
-  R *e, *r, *z, *p, *q;  // p: 2 buffers; z = B^-1 r (two-level) or D^-1 r
+  // workspace per component slot, nv entries each; r and p: 2 buffers
+  R *e, *r, *z, *p, *q;
   double* r64;
-  double* part;          // [2][ntiles][3], by iteration parity
+  double* part;          // [2][ntiles][3], by phase parity
   int* active;
   int* out_it;           // [nsys] iterations
   double* out_res;       // [nsys] final residual norm
@@ -99,26 +108,25 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return fma(a, b, c); }
+
+template <int GL, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+  for (int o = GL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(PFEM2_FULL_MASK, v, o);
+  return v;
+}
+
 struct LocalSys {
-  int sys, state, it, outer, par, first, owner, maxit, act;
-  int D, sl0, sps;
-  double tol, intol, res, rz_prev, alpha, beta, rzc;
+  int sys, state, it, outer, par, rpar, first, owner, maxit, act, chk;
+  double tol, intol, res, rz_prev, alpha, beta;
   double sum[2];
 };
 
-// z = B^-1 r on one SELL slice: lane i holds r_i, returns z_i
-template <typename R>
-__device__ __forceinline__ R block_jacobi32(const R* __restrict__ Binv, int slice, R ri, int lane) {
-  const R* B = Binv + (size_t)slice * 1024;
-  R acc = R(0);
-#pragma unroll 8
-  for (int j = 0; j < 32; ++j) acc += B[j * 32 + lane] * __shfl_sync(PFEM2_FULL_MASK, ri, j);
-  return acc;
-}
-
-template <typename R, bool TWO>
+template <typename R, bool MG>
 __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
-  extern __shared__ unsigned char dyn_smem[];
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ LocalSys ls[kMaxLocalSys];
   __shared__ double red[kWarps][2];
   __shared__ int s_nls, s_sys0;
@@ -126,9 +134,6 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
   const size_t nv = (size_t)a.nv;
   const int t_lo = a.blk_t0[blockIdx.x], t_hi = a.blk_t0[blockIdx.x + 1];
   unsigned bar_gen = 0;
-  // two-level shared memory: per local system E^-1 (dmax^2 floats), y and Z^T r (dmax doubles each)
-  float* sE = reinterpret_cast<float*>(dyn_smem);
-  const int nE = a.dmax * a.dmax;
 
   // ---- local systems of this block
   if (threadIdx.x == 0) {
@@ -145,48 +150,42 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       const int s = s0 + k, inst = s % a.ninst;
       L.sys = s;
       L.state = S_OUT_A;
-      L.it = L.outer = L.par = 0;
+      L.it = L.outer = L.par = L.rpar = L.chk = 0;
       L.first = 1;
       L.owner = a.sys_t0[s] >= t_lo && a.sys_t0[s] < t_hi;
       L.maxit = a.maxit_i[inst];
       L.tol = a.tol_i[inst];
       L.intol = 0.5 * L.tol;
-      L.res = L.rz_prev = L.alpha = L.beta = L.rzc = 0.0;
+      L.res = L.rz_prev = L.alpha = L.beta = 0.0;
+      L.sum[0] = L.sum[1] = 0.0;
       L.act = ACT_NONE;
-      if (TWO) {
-        L.D = a.sys_D[s];
-        L.sl0 = a.sys_sl0[s];
-        L.sps = a.sys_sps[s];
-      } else {
-        L.D = 0; L.sl0 = 0; L.sps = 1;
-      }
     }
   }
   __syncthreads();
   const int nls = s_nls, sys0 = s_sys0;
-  float* sEk[kMaxLocalSys];
-  double* sYk[kMaxLocalSys];
-  double* sSk[kMaxLocalSys];
-  const R* Bsrc = a.Binv;  // B^-1 of slice s at Bsrc + (s - bsl0) * 1024
-  int bsl0 = 0;
-  if (TWO) {
-    double* ybase = reinterpret_cast<double*>(sE + (size_t)nls * nE + ((nls * nE) & 1));
-    for (int k = 0; k < nls; ++k) {
-      sEk[k] = sE + (size_t)k * nE;
-      sYk[k] = ybase + (size_t)k * 3 * a.dmax;
-      sSk[k] = sYk[k] + 2 * a.dmax;
-      const float* src = a.Einv + a.sys_eoff[ls[k].sys];
-      const int n2 = ls[k].D * ls[k].D;
-      for (int i = threadIdx.x; i < n2; i += kSolveThreads) sEk[k][i] = src[i];
-    }
-    if (a.binv_smem && t_hi > t_lo) {
-      R* sB = reinterpret_cast<R*>(ybase + (size_t)nls * 3 * a.dmax);
-      bsl0 = a.tiles[t_lo].s0;
-      const int nsl = a.tiles[t_hi - 1].s1 - bsl0;
-      const R* g = a.Binv + (size_t)bsl0 * 1024;
-      for (int i = threadIdx.x; i < nsl * 1024; i += kSolveThreads) sB[i] = g[i];
-      Bsrc = sB;
-    }
+  // multigrid shared memory: x1 | x2 | x3 | b3 per local system (R), coarse-inverse rows (float)
+  R* sx1 = reinterpret_cast<R*>(dyn_smem);
+  R* sx2 = sx1 + a.s1max;
+  R* sx3 = sx2 + a.s2max;
+  R* sb3 = sx3 + a.s3max;
+  float* sE = reinterpret_cast<float*>(sb3 + (size_t)nls * a.dmax);
+  int s1_lo = 0, s1_hi = 0, s2_lo = 0, s2_hi = 0, s3_lo = 0, s3_hi = 0, o1lo = 0, o1hi = 0, o2lo = 0, o2hi = 0,
+      o3lo = 0, o3hi = 0;
+  if (MG) {
+    s1_lo = a.blk_s1[blockIdx.x];
+    s1_hi = a.blk_s1[blockIdx.x + 1];
+    s2_lo = a.blk_s2[blockIdx.x];
+    s2_hi = a.blk_s2[blockIdx.x + 1];
+    s3_lo = a.blk_s3[blockIdx.x];
+    s3_hi = a.blk_s3[blockIdx.x + 1];
+    o1lo = a.toff1[t_lo];
+    o1hi = a.toff1[t_hi];
+    o2lo = a.toff2[t_lo];
+    o2hi = a.toff2[t_hi];
+    o3lo = a.toff3[t_lo];
+    o3hi = a.toff3[t_hi];
+    const int e0 = a.blk_e[blockIdx.x], ne = a.blk_e[blockIdx.x + 1] - e0;
+    for (int i = threadIdx.x; i < ne; i += kSolveThreads) sE[i] = a.s3_E[e0 + i];
   }
 
   // ---- init: Dirichlet values preset in x, e = 0, p = 0
@@ -221,25 +220,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
     const bool phaseA = (iter & 1) == 0;
     const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 3;
     PFEM2_PROF(5);
-    // ---- Z^T r of the systems about to run phase A (warps 1..), loaded while
-    // warp 0 sums the scalar partials
-    if (TWO && phaseA && warp > 0) {
-      for (int k = 0; k < nls; ++k) {
-        if (ls[k].state != S_A) continue;
-        const int D = ls[k].D, t0 = a.sys_t0[ls[k].sys];
-        float* sf = reinterpret_cast<float*>(sYk[k] + a.dmax);
-        for (int d = threadIdx.x - 32; d < D; d += kSolveThreads - 32) {
-          const double v = __ldcg(prev + (size_t)(t0 + d) * 3 + 2);
-          sSk[k][d] = v;
-          sf[d] = (float)v;
-        }
-      }
-    }
     // ---- sums of the previous phase's partials (warp 0, fixed order)
     if (warp == 0) {
       for (int k = 0; k < nls; ++k) {
         const int st = ls[k].state;
-        if (st == S_DONE || st == S_OUT_A) continue;
+        if (st == S_DONE || st == S_OUT_A || st == S_UZ || (st == S_D && !ls[k].chk)) continue;
         const int t0 = a.sys_t0[ls[k].sys], t1 = a.sys_t0[ls[k].sys + 1];
         double s0 = 0.0, s1 = 0.0;
 #pragma unroll 4
@@ -257,78 +242,102 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
     }
     __syncthreads();
     PFEM2_PROF(0);
-    // ---- coarse correction y = E^-1 Z^T r for systems about to run phase A
-    if (TWO && phaseA) {
-      for (int k = 0; k < nls; ++k) {
-        if (ls[k].state != S_A) continue;
-        const int D = ls[k].D, t0 = a.sys_t0[ls[k].sys];
-        const float* sf = reinterpret_cast<const float*>(sYk[k] + a.dmax);  // FP32 copy of Z^T r
-        (void)t0;
-        for (int j = threadIdx.x; j < D; j += kSolveThreads) {
-          // y_j = sum_d E^-1[d][j] s_d (E^-1 symmetric: column reads are conflict free)
-          const float* Ej = sEk[k] + j;
-          float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-          int d = 0;
-          for (; d + 3 < D; d += 4) {
-            a0 = fmaf(Ej[(d + 0) * D], sf[d + 0], a0);
-            a1 = fmaf(Ej[(d + 1) * D], sf[d + 1], a1);
-            a2 = fmaf(Ej[(d + 2) * D], sf[d + 2], a2);
-            a3 = fmaf(Ej[(d + 3) * D], sf[d + 3], a3);
-          }
-          for (; d < D; ++d) a0 = fmaf(Ej[d * D], sf[d], a0);
-          sYk[k][j] = (double)((a0 + a1) + (a2 + a3));
-        }
-        __syncthreads();
-        if (warp == 0) {
-          double c = 0.0;
-          for (int d = lane; d < D; d += 32) c += sSk[k][d] * sYk[k][d];
-          c = warp_sum(c);
-          if (lane == 0) ls[k].rzc = c;
-        }
-      }
-    }
-    __syncthreads();
-    PFEM2_PROF(1);
     // ---- decisions (thread 0; identical in every block owning the system)
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
         LocalSys& L = ls[k];
         int act = ACT_NONE;
-        if (phaseA) {
-          if (L.state == S_OUT_A) {
-            act = ACT_OUT_A;
-            L.state = S_OUT_B;
-          } else if (L.state == S_A) {
-            const double rz = L.sum[0] + (TWO ? L.rzc : 0.0), rr = sqrt(L.sum[1]);
-            if (rr <= L.intol || L.it >= L.maxit || !(rr == rr)) {
-              act = ACT_OUT_A;  // reliable update in FP64
+        if (!MG) {
+          if (phaseA) {
+            if (L.state == S_OUT_A) {
+              act = ACT_OUT_A;
               L.state = S_OUT_B;
-            } else {
+            } else if (L.state == S_A) {
+              const double rz = L.sum[0], rr = sqrt(L.sum[1]);
+              if (rr <= L.intol || L.it >= L.maxit || !(rr == rr)) {
+                act = ACT_OUT_A;  // reliable update in FP64
+                L.state = S_OUT_B;
+              } else {
+                L.beta = L.first ? 0.0 : (L.rz_prev != 0.0 ? rz / L.rz_prev : 0.0);
+                L.rz_prev = rz;
+                L.first = 0;
+                act = ACT_A;
+                L.state = S_B;
+              }
+            }
+          } else {
+            if (L.state == S_OUT_B) {
+              L.res = sqrt(L.sum[0]);
+              L.outer += 1;
+              if (L.res <= L.tol || L.it >= L.maxit || !(L.res == L.res)) {
+                act = ACT_OUT_DONE;
+                L.state = S_DONE;
+              } else {
+                L.intol = fmax(a.eta * L.res, 0.5 * L.tol);
+                L.first = 1;  // CG restarts from the true residual
+                act = ACT_OUT_B;
+                L.state = S_A;
+              }
+            } else if (L.state == S_B) {
+              L.alpha = L.sum[0] != 0.0 ? L.rz_prev / L.sum[0] : 0.0;
+              L.it += 1;
+              act = ACT_B;
+              L.state = S_A;
+            }
+          }
+        } else {
+          switch (L.state) {
+            case S_OUT_A:
+              act = ACT_OUT_A;
+              L.state = S_OUT_B;
+              break;
+            case S_OUT_B:
+              L.res = sqrt(L.sum[0]);
+              L.outer += 1;
+              if (L.res <= L.tol || L.it >= L.maxit || !(L.res == L.res)) {
+                act = ACT_OUT_DONE;
+                L.state = S_DONE;
+              } else {
+                L.intol = fmax(a.eta * L.res, 0.5 * L.tol);
+                L.first = 1;  // CG restarts from the true residual
+                L.chk = 0;
+                act = ACT_OUT_B;
+                L.state = S_D;
+              }
+              break;
+            case S_D: {
+              const double rr = sqrt(L.sum[0]);
+              if (L.chk && (rr <= L.intol || L.it >= L.maxit || !(rr == rr))) {
+                act = ACT_OUT_A;  // reliable update in FP64
+                L.state = S_OUT_B;
+              } else {
+                act = ACT_D;
+                L.state = S_UZ;
+              }
+              break;
+            }
+            case S_UZ:
+              act = ACT_UZ;
+              L.state = S_A;
+              break;
+            case S_A: {
+              const double rz = L.sum[0];
               L.beta = L.first ? 0.0 : (L.rz_prev != 0.0 ? rz / L.rz_prev : 0.0);
               L.rz_prev = rz;
               L.first = 0;
               act = ACT_A;
               L.state = S_B;
+              break;
             }
-          }
-        } else {
-          if (L.state == S_OUT_B) {
-            L.res = sqrt(L.sum[0]);
-            L.outer += 1;
-            if (L.res <= L.tol || L.it >= L.maxit || !(L.res == L.res)) {
-              act = ACT_OUT_DONE;
-              L.state = S_DONE;
-            } else {
-              L.intol = fmax(a.eta * L.res, 0.5 * L.tol);
-              L.first = 1;  // CG restarts from the true residual
-              act = ACT_OUT_B;
-              L.state = S_A;
-            }
-          } else if (L.state == S_B) {
-            L.alpha = L.sum[0] != 0.0 ? L.rz_prev / L.sum[0] : 0.0;
-            L.it += 1;
-            act = ACT_B;
-            L.state = S_A;
+            case S_B:
+              L.alpha = L.sum[0] != 0.0 ? L.rz_prev / L.sum[0] : 0.0;
+              L.it += 1;
+              L.chk = 1;
+              act = ACT_B;
+              L.state = S_D;
+              break;
+            default:
+              break;
           }
         }
         L.act = act;
@@ -336,18 +345,142 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
     }
     __syncthreads();
     PFEM2_PROF(2);
-    // ---- work on the own tiles
+    // ---- coarse-level work of the block (multigrid; pressure = component 0)
+    if (MG) {
+      bool any_b = false, any_d = false, any_uz = false;
+      for (int k = 0; k < nls; ++k) {
+        const int act = ls[k].act;
+        any_b |= act == ACT_B || act == ACT_OUT_B;
+        any_d |= act == ACT_D;
+        any_uz |= act == ACT_UZ;
+      }
+      if (any_b) {
+        // b1 = R01 r' on the own level-1 rows (8 lanes per row); after a
+        // reliable update r' = r64, else r' = r - alpha q formed on the fly
+        constexpr int GL = 8, NG = kSolveThreads / GL;
+        const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+        for (int base = o1lo; base < o1hi; base += NG) {
+          const int i = base + grp;
+          R acc = R(0);
+          int act = ACT_NONE;
+          if (i < o1hi) {
+            const LocalSys& L = ls[__ldg(a.lsys1 + i) - sys0];
+            act = L.act;
+            const int k1 = __ldg(a.r01_ptr + i + 1);
+            if (act == ACT_B) {
+              const R al = R(L.alpha);
+              const R* rr = a.r + (size_t)L.rpar * nv;
+#pragma unroll 4
+              for (int k = __ldg(a.r01_ptr + i) + sub; k < k1; k += GL) {
+                const int j = __ldg(a.r01_col + k);
+                acc += __ldg(a.r01_val + k) * fma_r(-al, __ldcg(a.q + j), __ldcg(rr + j));
+              }
+            } else if (act == ACT_OUT_B) {
+#pragma unroll 4
+              for (int k = __ldg(a.r01_ptr + i) + sub; k < k1; k += GL)
+                acc += __ldg(a.r01_val + k) * R(__ldcg(a.r64 + __ldg(a.r01_col + k)));
+            }
+          }
+          acc = group_sum<GL>(acc);
+          if (sub == 0 && (act == ACT_B || act == ACT_OUT_B)) a.b1[i] = acc;
+        }
+      }
+      if (any_d) {
+        // b2 = R12 b1, b3 = R13 b1 on the own level-2 / level-3 rows (warp per row)
+        const int n2 = o2hi - o2lo, n3 = o3hi - o3lo;
+        for (int w = warp; w < n2 + n3; w += kWarps) {
+          const bool l2 = w < n2;
+          const int i = l2 ? o2lo + w : o3lo + (w - n2);
+          if (ls[__ldg((l2 ? a.lsys2 : a.lsys3) + i) - sys0].act != ACT_D) continue;
+          const int* ptr = l2 ? a.r12_ptr : a.r13_ptr;
+          const int* cl = l2 ? a.r12_col : a.r13_col;
+          const R* vl = l2 ? a.r12_val : a.r13_val;
+          R acc = R(0);
+          const int k1 = __ldg(ptr + i + 1);
+#pragma unroll 4
+          for (int k = __ldg(ptr + i) + lane; k < k1; k += 32) acc += __ldg(vl + k) * __ldcg(a.b1 + __ldg(cl + k));
+          acc = warp_sum(acc);
+          if (lane == 0) (l2 ? a.b2 : a.b3)[i] = acc;
+        }
+      }
+      if (any_uz) {
+        // b3 of the local systems
+        for (int k = 0; k < nls; ++k) {
+          if (ls[k].act != ACT_UZ) continue;
+          const int s = ls[k].sys, D = __ldg(a.sys_D3 + s), o = __ldg(a.sys_off3 + s);
+          for (int d = threadIdx.x; d < D; d += kSolveThreads) sb3[k * a.dmax + d] = __ldcg(a.b3 + o + d);
+        }
+        __syncthreads();
+        // x3 = E^-1 b3 on the block's level-3 list (warp per row, shared memory)
+        for (int j = s3_lo + warp; j < s3_hi; j += kWarps) {
+          const int s = __ldg(a.s3_sys + j), k = s - sys0;
+          if (ls[k].act != ACT_UZ) continue;
+          const int D = __ldg(a.sys_D3 + s);
+          const float* E = sE + __ldg(a.s3_eoff + j);
+          const R* bb = sb3 + k * a.dmax;
+          R acc = R(0);
+          for (int d = lane; d < D; d += 32) acc += R(E[d]) * bb[d];
+          acc = warp_sum(acc);
+          if (lane == 0) sx3[j - s3_lo] = acc;
+        }
+        __syncthreads();
+        // x2 = J2 b2 + Pt2 x3 on the level-2 list (4 lanes per row)
+        {
+          constexpr int GL = 4, NG = kSolveThreads / GL;
+          const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+          for (int base = s2_lo; base < s2_hi; base += NG) {
+            const int j = base + grp;
+            R acc = R(0);
+            bool on = false;
+            if (j < s2_hi && ls[__ldg(a.s2_sys + j) - sys0].act == ACT_UZ) {
+              on = true;
+              const int ja = __ldg(a.s2_jptr + j), jb = __ldg(a.s2_jptr + j + 1);
+#pragma unroll 4
+              for (int k = ja + sub; k < jb; k += GL) acc += __ldg(a.s2_jval + k) * __ldcg(a.b2 + __ldg(a.s2_jcol + k));
+              const int pa = __ldg(a.s2_pptr + j), pb = __ldg(a.s2_pptr + j + 1);
+              for (int k = pa + sub; k < pb; k += GL) acc += __ldg(a.s2_pval + k) * sx3[__ldg(a.s2_pcol + k)];
+            }
+            acc = group_sum<GL>(acc);
+            if (on && sub == 0) sx2[j - s2_lo] = acc;
+          }
+        }
+        __syncthreads();
+        // x1 = J1 b1 + Pt1 x2 on the level-1 list (4 lanes per row)
+        {
+          constexpr int GL = 4, NG = kSolveThreads / GL;
+          const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+          for (int base = s1_lo; base < s1_hi; base += NG) {
+            const int j = base + grp;
+            R acc = R(0);
+            bool on = false;
+            if (j < s1_hi && ls[__ldg(a.s1_sys + j) - sys0].act == ACT_UZ) {
+              on = true;
+              const int ja = __ldg(a.s1_jptr + j), jb = __ldg(a.s1_jptr + j + 1);
+#pragma unroll 4
+              for (int k = ja + sub; k < jb; k += GL) acc += __ldg(a.s1_jval + k) * __ldcg(a.b1 + __ldg(a.s1_jcol + k));
+              const int pa = __ldg(a.s1_pptr + j), pb = __ldg(a.s1_pptr + j + 1);
+              for (int k = pa + sub; k < pb; k += GL) acc += __ldg(a.s1_pval + k) * sx2[__ldg(a.s1_pcol + k)];
+            }
+            acc = group_sum<GL>(acc);
+            if (on && sub == 0) sx1[j - s1_lo] = acc;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    PFEM2_PROF(1);
+    // ---- level-0 work on the own tiles
     for (int t = t_lo; t < t_hi; ++t) {
       const Tile T = a.tiles[t];
       const int k = T.comp;
       const int lk = T.sys - sys0;
       const LocalSys& L = ls[lk];
       const int act = L.act;
-      if (act == ACT_NONE) continue;
-      double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+      if (act == ACT_NONE || act == ACT_D) continue;
+      double v0 = 0.0, v1 = 0.0;
       const R* dinv = a.dinv[k];
       R* e = a.e + k * nv;
-      R* r = a.r + k * nv;
+      R* r = a.r + (2 * k + L.rpar) * nv;
       R* z = a.z + k * nv;
       R* q = a.q + k * nv;
       double* r64 = a.r64 + k * nv;
@@ -374,12 +507,13 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
           e[row] = R(0);
           if (act == ACT_OUT_B) {
             const R rr = R(r64[row]);
-            const R zz = TWO ? block_jacobi32<R>(Bsrc, sl - bsl0, rr, lane) : rr * dinv[row];
             r[row] = rr;
-            z[row] = zz;
-            v0 += (double)rr * (double)zz;
-            v1 += (double)rr * (double)rr;
-            v2 += (double)rr;
+            if (!MG) {
+              const R zz = rr * dinv[row];
+              z[row] = zz;
+              v0 += (double)rr * (double)zz;
+              v1 += (double)rr * (double)rr;
+            }
           }
         }
       } else if (act == ACT_A) {
@@ -387,7 +521,6 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         R* pn = a.p + (2 * k + L.par) * nv;
         const R* po = a.p + (2 * k + (L.par ^ 1)) * nv;
         const R* A = a.Ain[k];
-        const double* y = TWO ? sYk[lk] : nullptr;
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
           const int base = a.sl_ptr[sl], len = a.sl_len[sl];
@@ -395,13 +528,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
           for (int j = 0; j < len; ++j) {
             const int ei = base + j * 32 + lane;
             const int col = __ldg(a.sl_col + ei);
-            R zc = __ldcg(z + col);
-            if (TWO) zc += R(y[((col >> 5) - L.sl0) / L.sps]);
-            acc += A[ei] * (zc + beta * __ldcg(po + col));
+            acc += A[ei] * fma_r(beta, __ldcg(po + col), __ldcg(z + col));
           }
-          R zr = z[row];
-          if (TWO) zr += R(y[(sl - L.sl0) / L.sps]);
-          const R pp = zr + beta * po[row];
+          const R pp = fma_r(beta, po[row], z[row]);
           pn[row] = pp;
           q[row] = acc;
           v0 += (double)pp * (double)acc;
@@ -409,40 +538,58 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       } else if (act == ACT_B) {
         const R alpha = R(L.alpha);
         const R* pn = a.p + (2 * k + L.par) * nv;
+        R* rn = MG ? a.r + (2 * k + (L.rpar ^ 1)) * nv : r;
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
           e[row] += alpha * pn[row];
-          const R rr = r[row] - alpha * q[row];
-          const R zz = TWO ? block_jacobi32<R>(Bsrc, sl - bsl0, rr, lane) : rr * dinv[row];
-          r[row] = rr;
-          z[row] = zz;
-          v0 += (double)rr * (double)zz;
-          v1 += (double)rr * (double)rr;
-          v2 += (double)rr;
+          const R rr = fma_r(-alpha, q[row], r[row]);
+          rn[row] = rr;
+          if (MG) {
+            v0 += (double)rr * (double)rr;
+          } else {
+            const R zz = rr * dinv[row];
+            z[row] = zz;
+            v0 += (double)rr * (double)zz;
+            v1 += (double)rr * (double)rr;
+          }
+        }
+      } else if (MG && act == ACT_UZ) {
+        // z = J0 r + Pt0 x1
+        const R* J = a.j0;
+        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+          const int row = sl * 32 + lane;
+          const int base = a.sl_ptr[sl], len = a.sl_len[sl];
+          R acc = R(0);
+          for (int j = 0; j < len; ++j) {
+            const int ei = base + j * 32 + lane;
+            acc += __ldg(J + ei) * __ldcg(r + __ldg(a.sl_col + ei));
+          }
+          const int pb = __ldg(a.p0_ptr + sl), pl = __ldg(a.p0_len + sl);
+          for (int j = 0; j < pl; ++j) {
+            const int ei = pb + j * 32 + lane;
+            acc += __ldg(a.p0_val + ei) * sx1[__ldg(a.p0_col + ei)];
+          }
+          z[row] = acc;
+          v0 += (double)__ldcg(r + row) * (double)acc;
         }
       }
-      // deterministic block reduction into this iteration's parity buffer
+      // deterministic block reduction into this phase's parity buffer
       v0 = warp_sum(v0);
       v1 = warp_sum(v1);
-      v2 = warp_sum(v2);
       if (lane == 0) {
         red[warp][0] = v0;
         red[warp][1] = v1;
       }
-      __shared__ double red2[kWarps];
-      if (lane == 0) red2[warp] = v2;
       __syncthreads();
       if (threadIdx.x == 0) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        double s0 = 0.0, s1 = 0.0;
         for (int wv = 0; wv < kWarps; ++wv) {
           s0 += red[wv][0];
           s1 += red[wv][1];
-          s2 += red2[wv];
         }
         double* dst = a.part + ((size_t)(iter & 1) * a.ntiles + t) * 3;
         dst[0] = s0;
         dst[1] = s1;
-        dst[2] = s2;
       }
       __syncthreads();
     }
@@ -451,7 +598,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
         LocalSys& L = ls[k];
-        if (L.act == ACT_B) L.par ^= 1;
+        if (L.act == ACT_B) {
+          L.par ^= 1;
+          if (MG) L.rpar ^= 1;
+        }
         if (L.act == ACT_OUT_DONE && L.owner) {
           a.out_it[L.sys] = L.it;
           a.out_res[L.sys] = L.res;
@@ -477,15 +627,25 @@ struct KrylovWs {
   int* blk_t0[2];
   int ntiles[2], nsys[2], grid[2];
   std::vector<Tile> h_tiles0;
-  std::vector<int> h_sys_t0_0;
-  // two-level data of the pressure phase (phase 0)
-  bool two_level = false;
-  int dmax = 0, nls_max = 1;
-  size_t smem_two = 0;
-  int binv_smem = 0;
-  void* Binv = nullptr;
-  float* Einv = nullptr;
-  int *sys_eoff = nullptr, *sys_D = nullptr, *sys_sl0 = nullptr, *sys_sps = nullptr;
+  std::vector<int> h_sys_t0_0, h_blk_t0_0;
+  // multigrid of the pressure phase (phase 0)
+  bool mg = false;
+  int nls0 = 1;
+  size_t smem_mg = 0;
+  int dmax = 1, s1max = 0, s2max = 0, s3max = 0;
+  int n1 = 0, n2 = 0, n3 = 0;
+  int *toff[4] = {}, *lsys[4] = {};
+  int *r01_ptr = nullptr, *r01_col = nullptr, *r12_ptr = nullptr, *r12_col = nullptr, *r13_ptr = nullptr,
+      *r13_col = nullptr;
+  void *r01_val = nullptr, *r12_val = nullptr, *r13_val = nullptr, *j0 = nullptr;
+  int *p0_ptr = nullptr, *p0_len = nullptr, *p0_col = nullptr;
+  void* p0_val = nullptr;
+  int *blk_s[3] = {}, *s_sys[3] = {}, *s_jptr[3] = {}, *s_jcol[3] = {}, *s_pptr[3] = {}, *s_pcol[3] = {};
+  void *s_jval[3] = {}, *s_pval[3] = {};
+  int *blk_s3 = nullptr, *s3_sys = nullptr, *s3_eoff = nullptr, *blk_e = nullptr;
+  float* s3_E = nullptr;
+  int *sys_D3 = nullptr, *sys_off3 = nullptr;
+  void *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
   void *e = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p = nullptr;
   double* r64 = nullptr;
   double* part = nullptr;
@@ -494,7 +654,40 @@ struct KrylovWs {
   double* out_res[3];
   int* out_outer[3];
   unsigned long long* prof = nullptr;  // [3 solve kinds][6]
+  std::vector<void*> allocs;            // every device allocation of the workspace
 };
+
+template <typename T>
+static pfem2_status ws_alloc(KrylovWs* w, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  PFEM2_CUDA(cudaMalloc((void**)p, sizeof(T) * n));
+  PFEM2_CUDA(cudaMemset(*p, 0, sizeof(T) * n));
+  w->allocs.push_back(*p);
+  return PFEM2_OK;
+}
+
+template <typename T>
+static pfem2_status ws_upload(KrylovWs* w, T** p, const std::vector<T>& v) {
+  PFEM2_TRY(ws_alloc(w, p, v.size()));
+  if (!v.empty()) PFEM2_CUDA(cudaMemcpy(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return PFEM2_OK;
+}
+
+// FP64 host values as the inner type R (float for the mixed path)
+static pfem2_status ws_upload_r(KrylovWs* w, bool mixed, void** p, const std::vector<double>& v) {
+  if (mixed) {
+    std::vector<float> f(v.begin(), v.end());
+    float* d;
+    PFEM2_TRY(ws_upload(w, &d, f));
+    *p = d;
+  } else {
+    double* d;
+    PFEM2_TRY(ws_upload(w, &d, v));
+    *p = d;
+  }
+  return PFEM2_OK;
+}
 
 static int max_local_systems(const std::vector<Tile>& tiles, const std::vector<int>& bt0) {
   int worst = 0;
@@ -503,13 +696,21 @@ static int max_local_systems(const std::vector<Tile>& tiles, const std::vector<i
   return worst;
 }
 
-template <typename R, bool TWO>
+template <typename R, bool MG>
 static int occupancy(size_t smem) {
   int occ = 0;
-  // one process-wide upper bound, so contexts with different coarse sizes coexist
-  if (TWO) cudaFuncSetAttribute((const void*)k_krylov<R, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_krylov<R, TWO>, kSolveThreads, smem) != cudaSuccess) return 0;
+  // one process-wide upper bound, so contexts with different hierarchies coexist
+  if (MG) cudaFuncSetAttribute((const void*)k_krylov<R, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_krylov<R, MG>, kSolveThreads, smem) != cudaSuccess) return 0;
   return occ;
+}
+
+void krylov_free(Ctx& c) {
+  KrylovWs* w = (KrylovWs*)c.kws;
+  if (!w) return;
+  for (void* p : w->allocs) cudaFree(p);
+  delete w;
+  c.kws = nullptr;
 }
 
 pfem2_status krylov_setup(Ctx& c) {
@@ -525,24 +726,21 @@ pfem2_status krylov_setup(Ctx& c) {
     std::vector<Tile> tiles;
     std::vector<int> st0(ncomp * ni + 1, 0);
     if (ph == 0) {
-      // pressure: tiles = coarse subdomains; about one per block of the
-      // persistent grid (balanced work), at most dcap per system
-      // (a batch: subdomains of ~8 slices, at most dcap per system, so every
-      // instance gets a coarse space of its own size)
+      // pressure: tiles = the aggregation domains of the multigrid; about
+      // one per block of the persistent grid (balanced work), at most dcap
+      // per system (a batch: tiles of ~8 slices, at most dcap per system,
+      // so every instance gets a coarse space of its own size)
       const int dcap = ni == 1 ? 160 : 96;
       const int nb = bps * c.num_sms;
       long long tot_sl = 0;
       for (int i = 0; i < ni; ++i) tot_sl += c.inst[i].nv_pad / kSlice;
-      w->dmax = 1;
       for (int i = 0; i < ni; ++i) {
         st0[i] = (int)tiles.size();
         const int sl0 = c.inst[i].v_off / kSlice, nsl = c.inst[i].nv_pad / kSlice;
         const long long share = ni == 1 ? std::max<long long>(1, (long long)nb * nsl / tot_sl) : (nsl + 7) / 8;
         int D = (int)std::min<long long>(std::min<long long>(share, dcap), nsl);
         const int sps = (nsl + D - 1) / D;
-        D = (nsl + sps - 1) / sps;
         for (int a = 0; a < nsl; a += sps) tiles.push_back(Tile{i, 0, sl0 + a, sl0 + std::min(nsl, a + sps)});
-        w->dmax = std::max(w->dmax, D);
       }
       st0[ni] = (int)tiles.size();
     } else {
@@ -560,17 +758,9 @@ pfem2_status krylov_setup(Ctx& c) {
       st0[ncomp * ni] = (int)tiles.size();
     }
     const int T = (int)tiles.size();
-    int occ;
-    size_t smem = 0;
-    if (ph == 0) {
-      // shared memory for the coarse inverses: sized after the chunking below,
-      // first with one local system to bound the grid
-      w->nls_max = 1;
-      smem = (size_t)w->dmax * w->dmax * 4 + 8 + 3 * (size_t)w->dmax * 8;
-      occ = c.mixed ? occupancy<float, true>(smem) : occupancy<double, true>(smem);
-    } else {
-      occ = c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0);
-    }
+    // the multigrid grid is sized before its shared memory is known (one
+    // block per SM); krylov_setup_precond checks residency afterwards
+    const int occ = ph == 0 ? 1 : (c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0));
     if (occ < 1) {
       set_error("krylov: the solver kernel cannot be resident");
       return PFEM2_CUDA_ERROR;
@@ -584,178 +774,129 @@ pfem2_status krylov_setup(Ctx& c) {
       return PFEM2_INVALID_ARG;
     }
     if (ph == 0) {
-      w->nls_max = nls;
-      w->smem_two = (size_t)nls * w->dmax * w->dmax * 4 + 8 + 3 * (size_t)nls * w->dmax * 8;
-      int maxsl = 0;
-      for (int b = 0; b < G; ++b)
-        if (bt0[b + 1] > bt0[b]) maxsl = std::max(maxsl, tiles[bt0[b + 1] - 1].s1 - tiles[bt0[b]].s0);
-      const size_t bj = (size_t)maxsl * 1024 * rs;
-      if (w->smem_two + bj <= 220 * 1024) {
-        w->smem_two += bj;
-        w->binv_smem = 1;
-      }
-      if (w->smem_two > 220 * 1024) {
-        set_error("krylov: coarse inverses of the pressure systems exceed shared memory");
-        return PFEM2_INVALID_ARG;
-      }
-      const int occ2 = c.mixed ? occupancy<float, true>(w->smem_two) : occupancy<double, true>(w->smem_two);
-      if (occ2 * c.num_sms < G) {
-        set_error("krylov: the two-level solver grid cannot be resident");
-        return PFEM2_CUDA_ERROR;
-      }
+      w->nls0 = nls;
       w->h_tiles0 = tiles;
       w->h_sys_t0_0 = st0;
+      w->h_blk_t0_0 = bt0;
     }
     w->ntiles[ph] = T;
     w->nsys[ph] = (int)st0.size() - 1;
     w->grid[ph] = G;
-    PFEM2_CUDA(cudaMalloc(&w->tiles[ph], sizeof(Tile) * T));
-    PFEM2_CUDA(cudaMemcpy(w->tiles[ph], tiles.data(), sizeof(Tile) * T, cudaMemcpyHostToDevice));
-    PFEM2_CUDA(cudaMalloc(&w->sys_t0[ph], sizeof(int) * st0.size()));
-    PFEM2_CUDA(cudaMemcpy(w->sys_t0[ph], st0.data(), sizeof(int) * st0.size(), cudaMemcpyHostToDevice));
-    PFEM2_CUDA(cudaMalloc(&w->blk_t0[ph], sizeof(int) * bt0.size()));
-    PFEM2_CUDA(cudaMemcpy(w->blk_t0[ph], bt0.data(), sizeof(int) * bt0.size(), cudaMemcpyHostToDevice));
+    PFEM2_TRY(ws_upload(w, &w->tiles[ph], tiles));
+    PFEM2_TRY(ws_upload(w, &w->sys_t0[ph], st0));
+    PFEM2_TRY(ws_upload(w, &w->blk_t0[ph], bt0));
     maxtiles = std::max(maxtiles, T);
     maxsys = std::max(maxsys, w->nsys[ph]);
   }
-  void** vecs[] = {&w->e, &w->r, &w->z, &w->q};
-  for (void** v : vecs) {
-    PFEM2_CUDA(cudaMalloc(v, rs * nv * dim));
-    PFEM2_CUDA(cudaMemset(*v, 0, rs * nv * dim));
+  if (c.mixed) {
+    float *e, *r, *z, *q, *p;
+    PFEM2_TRY(ws_alloc(w, &e, nv * dim));
+    PFEM2_TRY(ws_alloc(w, &r, 2 * nv * dim));
+    PFEM2_TRY(ws_alloc(w, &z, nv * dim));
+    PFEM2_TRY(ws_alloc(w, &q, nv * dim));
+    PFEM2_TRY(ws_alloc(w, &p, 2 * nv * dim));
+    w->e = e; w->r = r; w->z = z; w->q = q; w->p = p;
+  } else {
+    double *e, *r, *z, *q, *p;
+    PFEM2_TRY(ws_alloc(w, &e, nv * dim));
+    PFEM2_TRY(ws_alloc(w, &r, 2 * nv * dim));
+    PFEM2_TRY(ws_alloc(w, &z, nv * dim));
+    PFEM2_TRY(ws_alloc(w, &q, nv * dim));
+    PFEM2_TRY(ws_alloc(w, &p, 2 * nv * dim));
+    w->e = e; w->r = r; w->z = z; w->q = q; w->p = p;
   }
-  PFEM2_CUDA(cudaMalloc(&w->p, rs * nv * dim * 2));
-  PFEM2_CUDA(cudaMemset(w->p, 0, rs * nv * dim * 2));
-  PFEM2_CUDA(cudaMalloc(&w->r64, sizeof(double) * nv * dim));
-  PFEM2_CUDA(cudaMemset(w->r64, 0, sizeof(double) * nv * dim));
-  PFEM2_CUDA(cudaMalloc(&w->part, sizeof(double) * 6 * maxtiles));
-  PFEM2_CUDA(cudaMemset(w->part, 0, sizeof(double) * 6 * maxtiles));
-  PFEM2_CUDA(cudaMalloc(&w->active, sizeof(int)));
-  if (getenv("PFEM2_SOLVER_PROFILE")) {
-    PFEM2_CUDA(cudaMalloc(&w->prof, sizeof(unsigned long long) * 18));
-    PFEM2_CUDA(cudaMemset(w->prof, 0, sizeof(unsigned long long) * 18));
-  }
+  (void)rs;
+  PFEM2_TRY(ws_alloc(w, &w->r64, nv * dim));
+  PFEM2_TRY(ws_alloc(w, &w->part, 6 * (size_t)maxtiles));
+  PFEM2_TRY(ws_alloc(w, &w->active, 1));
+  if (getenv("PFEM2_SOLVER_PROFILE")) PFEM2_TRY(ws_alloc(w, &w->prof, 18));
   for (int k = 0; k < 3; ++k) {
-    PFEM2_CUDA(cudaMalloc(&w->out_it[k], sizeof(int) * maxsys));
-    PFEM2_CUDA(cudaMalloc(&w->out_res[k], sizeof(double) * maxsys));
-    PFEM2_CUDA(cudaMalloc(&w->out_outer[k], sizeof(int) * maxsys));
-    PFEM2_CUDA(cudaMemset(w->out_it[k], 0, sizeof(int) * maxsys));
-    PFEM2_CUDA(cudaMemset(w->out_res[k], 0, sizeof(double) * maxsys));
-    PFEM2_CUDA(cudaMemset(w->out_outer[k], 0, sizeof(int) * maxsys));
+    PFEM2_TRY(ws_alloc(w, &w->out_it[k], maxsys));
+    PFEM2_TRY(ws_alloc(w, &w->out_res[k], maxsys));
+    PFEM2_TRY(ws_alloc(w, &w->out_outer[k], maxsys));
   }
   return PFEM2_OK;
 }
 
-// in-place inverse of an SPD matrix (Cholesky, then L^-T L^-1); false if not SPD
-static bool spd_inverse(std::vector<double>& M, int n) {
-  std::vector<double> L((size_t)n * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    double d = M[(size_t)j * n + j];
-    for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
-    if (!(d > 0.0)) return false;
-    d = std::sqrt(d);
-    L[(size_t)j * n + j] = d;
-    for (int i = j + 1; i < n; ++i) {
-      double s = M[(size_t)i * n + j];
-      for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
-      L[(size_t)i * n + j] = s / d;
-    }
-  }
-  // Linv (lower)
-  std::vector<double> Li((size_t)n * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
-    for (int i = j + 1; i < n; ++i) {
-      double s = 0.0;
-      for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
-      Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
-    }
-  }
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j <= i; ++j) {
-      double s = 0.0;
-      for (int k = i; k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
-      M[(size_t)i * n + j] = s;
-      M[(size_t)j * n + i] = s;
-    }
-  return true;
-}
-
-// block-Jacobi inverses of the 32x32 slice blocks and the coarse inverses
-// E^-1 = (Z^T A Z)^-1 of the pressure matrix (after Dirichlet elimination).
+// The multigrid hierarchy of the pressure matrix (after Dirichlet
+// elimination), built on the host and uploaded in the kernel's layout.
 pfem2_status krylov_setup_precond(Ctx& c) {
   KrylovWs* w = (KrylovWs*)c.kws;
-  const int ni = (int)c.inst.size();
+  if (!c.two_level) return PFEM2_OK;
   std::vector<double> A(c.nell);
   std::vector<int> col(c.nell), len(c.nslices);
   PFEM2_CUDA(cudaMemcpy(A.data(), c.A64[3], sizeof(double) * c.nell, cudaMemcpyDeviceToHost));
   PFEM2_CUDA(cudaMemcpy(col.data(), c.sl_col, sizeof(int) * c.nell, cudaMemcpyDeviceToHost));
   PFEM2_CUDA(cudaMemcpy(len.data(), c.sl_len, sizeof(int) * c.nslices, cudaMemcpyDeviceToHost));
-  const std::vector<int>& sp = c.h_sl_ptr;
-  // block Jacobi
-  std::vector<double> B(1024);
-  std::vector<double> bj64;
-  std::vector<float> bj32;
-  if (c.mixed) bj32.resize((size_t)c.nslices * 1024);
-  else bj64.resize((size_t)c.nslices * 1024);
-  for (int s = 0; s < c.nslices; ++s) {
-    std::fill(B.begin(), B.end(), 0.0);
-    for (int l = 0; l < 32; ++l)
-      for (int j = 0; j < len[s]; ++j) {
-        const int e = sp[s] + j * 32 + l;
-        const int cc = col[e];
-        if (cc / 32 == s) B[(size_t)l * 32 + (cc % 32)] += A[e];
-      }
-    if (!spd_inverse(B, 32)) {
-      set_error("krylov: a diagonal block of the pressure matrix is not SPD");
-      return PFEM2_MESH_ERROR;
-    }
-    for (int jj = 0; jj < 32; ++jj)
-      for (int i = 0; i < 32; ++i) {
-        const double v = B[(size_t)i * 32 + jj];
-        if (c.mixed) bj32[(size_t)s * 1024 + jj * 32 + i] = (float)v;
-        else bj64[(size_t)s * 1024 + jj * 32 + i] = v;
-      }
+  MgHost H;
+  PFEM2_TRY(mg_build(c, A, col, len, w->h_tiles0, w->h_sys_t0_0, w->h_blk_t0_0, H));
+  const size_t rs = c.mixed ? sizeof(float) : sizeof(double);
+  w->dmax = H.dmax;
+  w->s1max = H.s1max;
+  w->s2max = H.s2max;
+  w->s3max = H.s3max;
+  w->smem_mg = rs * ((size_t)H.s1max + H.s2max + H.s3max + (size_t)w->nls0 * H.dmax) + sizeof(float) * H.emax;
+  if (w->smem_mg > 200 * 1024) {
+    set_error("krylov: the pressure multigrid's per-block data exceed shared memory");
+    return PFEM2_INVALID_ARG;
   }
-  const size_t bbytes = (size_t)c.nslices * 1024 * (c.mixed ? 4 : 8);
-  PFEM2_CUDA(cudaMalloc(&w->Binv, bbytes));
-  PFEM2_CUDA(cudaMemcpy(w->Binv, c.mixed ? (void*)bj32.data() : (void*)bj64.data(), bbytes, cudaMemcpyHostToDevice));
-  // coarse inverses per system (tile = subdomain)
-  const std::vector<Tile>& tiles = w->h_tiles0;
-  const std::vector<int>& st0 = w->h_sys_t0_0;
-  std::vector<int> eoff(ni), Dv(ni), sl0v(ni), spsv(ni);
-  std::vector<float> Einv;
-  std::vector<int> sub_of_slice(c.nslices, -1);
-  for (int i = 0; i < ni; ++i) {
-    const int t0 = st0[i], t1 = st0[i + 1], D = t1 - t0;
-    Dv[i] = D;
-    sl0v[i] = tiles[t0].s0;
-    spsv[i] = tiles[t0].s1 - tiles[t0].s0;
-    for (int t = t0; t < t1; ++t)
-      for (int s = tiles[t].s0; s < tiles[t].s1; ++s) sub_of_slice[s] = t - t0;
-    std::vector<double> E((size_t)D * D, 0.0);
-    for (int t = t0; t < t1; ++t)
-      for (int s = tiles[t].s0; s < tiles[t].s1; ++s)
-        for (int l = 0; l < 32; ++l)
-          for (int j = 0; j < len[s]; ++j) {
-            const int e = sp[s] + j * 32 + l;
-            E[(size_t)(t - t0) * D + sub_of_slice[col[e] / 32]] += A[e];
-          }
-    if (!spd_inverse(E, D)) {
-      set_error("krylov: the coarse pressure matrix is not SPD");
-      return PFEM2_MESH_ERROR;
-    }
-    eoff[i] = (int)Einv.size();
-    for (double v : E) Einv.push_back((float)v);
+  const int occ = c.mixed ? occupancy<float, true>(w->smem_mg) : occupancy<double, true>(w->smem_mg);
+  if (occ * c.num_sms < w->grid[0]) {
+    set_error("krylov: the multigrid solver grid cannot be resident");
+    return PFEM2_CUDA_ERROR;
   }
-  PFEM2_CUDA(cudaMalloc(&w->Einv, sizeof(float) * Einv.size()));
-  PFEM2_CUDA(cudaMemcpy(w->Einv, Einv.data(), sizeof(float) * Einv.size(), cudaMemcpyHostToDevice));
-  int** dst[] = {&w->sys_eoff, &w->sys_D, &w->sys_sl0, &w->sys_sps};
-  std::vector<int>* src[] = {&eoff, &Dv, &sl0v, &spsv};
-  for (int k = 0; k < 4; ++k) {
-    PFEM2_CUDA(cudaMalloc(dst[k], sizeof(int) * ni));
-    PFEM2_CUDA(cudaMemcpy(*dst[k], src[k]->data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
+  w->n1 = H.n[1];
+  w->n2 = H.n[2];
+  w->n3 = H.n[3];
+  for (int l = 1; l < kMgLevels; ++l) {
+    PFEM2_TRY(ws_upload(w, &w->toff[l], H.toff[l]));
+    PFEM2_TRY(ws_upload(w, &w->lsys[l], H.lsys[l]));
   }
-  w->two_level = true;
+  PFEM2_TRY(ws_upload(w, &w->r01_ptr, H.r01_ptr));
+  PFEM2_TRY(ws_upload(w, &w->r01_col, H.r01_col));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r01_val, H.r01_val));
+  PFEM2_TRY(ws_upload(w, &w->r12_ptr, H.r12_ptr));
+  PFEM2_TRY(ws_upload(w, &w->r12_col, H.r12_col));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r12_val, H.r12_val));
+  PFEM2_TRY(ws_upload(w, &w->r13_ptr, H.r13_ptr));
+  PFEM2_TRY(ws_upload(w, &w->r13_col, H.r13_col));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r13_val, H.r13_val));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->j0, H.j0));
+  PFEM2_TRY(ws_upload(w, &w->p0_ptr, H.p0_ptr));
+  PFEM2_TRY(ws_upload(w, &w->p0_len, H.p0_len));
+  PFEM2_TRY(ws_upload(w, &w->p0_col, H.p0_col));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->p0_val, H.p0_val));
+  for (int l = 1; l <= 2; ++l) {
+    PFEM2_TRY(ws_upload(w, &w->blk_s[l], H.blk_s[l]));
+    PFEM2_TRY(ws_upload(w, &w->s_sys[l], H.s_sys[l]));
+    PFEM2_TRY(ws_upload(w, &w->s_jptr[l], H.s_jptr[l]));
+    PFEM2_TRY(ws_upload(w, &w->s_jcol[l], H.s_jcol[l]));
+    PFEM2_TRY(ws_upload_r(w, c.mixed, &w->s_jval[l], H.s_jval[l]));
+    PFEM2_TRY(ws_upload(w, &w->s_pptr[l], H.s_pptr[l]));
+    PFEM2_TRY(ws_upload(w, &w->s_pcol[l], H.s_pcol[l]));
+    PFEM2_TRY(ws_upload_r(w, c.mixed, &w->s_pval[l], H.s_pval[l]));
+  }
+  PFEM2_TRY(ws_upload(w, &w->blk_s3, H.blk_s3));
+  PFEM2_TRY(ws_upload(w, &w->s3_sys, H.s3_sys));
+  PFEM2_TRY(ws_upload(w, &w->s3_eoff, H.s3_eoff));
+  PFEM2_TRY(ws_upload(w, &w->blk_e, H.blk_e));
+  PFEM2_TRY(ws_upload(w, &w->s3_E, H.s3_E));
+  PFEM2_TRY(ws_upload(w, &w->sys_D3, H.sys_D3));
+  PFEM2_TRY(ws_upload(w, &w->sys_off3, H.sys_off3));
+  if (c.mixed) {
+    float *b1, *b2, *b3;
+    PFEM2_TRY(ws_alloc(w, &b1, H.n[1]));
+    PFEM2_TRY(ws_alloc(w, &b2, H.n[2]));
+    PFEM2_TRY(ws_alloc(w, &b3, H.n[3]));
+    w->b1 = b1; w->b2 = b2; w->b3 = b3;
+  } else {
+    double *b1, *b2, *b3;
+    PFEM2_TRY(ws_alloc(w, &b1, H.n[1]));
+    PFEM2_TRY(ws_alloc(w, &b2, H.n[2]));
+    PFEM2_TRY(ws_alloc(w, &b3, H.n[3]));
+    w->b1 = b1; w->b2 = b2; w->b3 = b3;
+  }
+  w->mg = true;
   return PFEM2_OK;
 }
 
@@ -775,7 +916,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   const int ph = which == 1 ? 0 : 1;
   const int ncomp = which == 1 ? 1 : c.dim;
   const int ni = (int)c.inst.size();
-  const bool two = which == 1 && w->two_level && c.two_level;
+  const bool mg = which == 1 && w->mg && c.two_level;
   SolveArgs<R> a{};
   a.ncomp = ncomp;
   a.ninst = ni;
@@ -788,14 +929,25 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.sl_ptr = c.sl_ptr;
   a.sl_len = c.sl_len;
   a.sl_col = c.sl_col;
-  a.Binv = (const R*)w->Binv;
-  a.Einv = w->Einv;
-  a.sys_eoff = w->sys_eoff;
-  a.sys_D = w->sys_D;
-  a.sys_sl0 = w->sys_sl0;
-  a.sys_sps = w->sys_sps;
-  a.dmax = w->dmax;
-  a.binv_smem = w->binv_smem;
+  if (mg) {
+    a.toff1 = w->toff[1]; a.toff2 = w->toff[2]; a.toff3 = w->toff[3];
+    a.lsys1 = w->lsys[1]; a.lsys2 = w->lsys[2]; a.lsys3 = w->lsys[3];
+    a.r01_ptr = w->r01_ptr; a.r01_col = w->r01_col; a.r01_val = (const R*)w->r01_val;
+    a.r12_ptr = w->r12_ptr; a.r12_col = w->r12_col; a.r12_val = (const R*)w->r12_val;
+    a.r13_ptr = w->r13_ptr; a.r13_col = w->r13_col; a.r13_val = (const R*)w->r13_val;
+    a.j0 = (const R*)w->j0;
+    a.p0_ptr = w->p0_ptr; a.p0_len = w->p0_len; a.p0_col = w->p0_col; a.p0_val = (const R*)w->p0_val;
+    a.blk_s1 = w->blk_s[1]; a.s1_sys = w->s_sys[1]; a.s1_jptr = w->s_jptr[1]; a.s1_jcol = w->s_jcol[1];
+    a.s1_jval = (const R*)w->s_jval[1]; a.s1_pptr = w->s_pptr[1]; a.s1_pcol = w->s_pcol[1];
+    a.s1_pval = (const R*)w->s_pval[1];
+    a.blk_s2 = w->blk_s[2]; a.s2_sys = w->s_sys[2]; a.s2_jptr = w->s_jptr[2]; a.s2_jcol = w->s_jcol[2];
+    a.s2_jval = (const R*)w->s_jval[2]; a.s2_pptr = w->s_pptr[2]; a.s2_pcol = w->s_pcol[2];
+    a.s2_pval = (const R*)w->s_pval[2];
+    a.blk_s3 = w->blk_s3; a.s3_sys = w->s3_sys; a.s3_eoff = w->s3_eoff; a.blk_e = w->blk_e; a.s3_E = w->s3_E;
+    a.sys_D3 = w->sys_D3; a.sys_off3 = w->sys_off3;
+    a.dmax = w->dmax; a.s1max = w->s1max; a.s2max = w->s2max; a.s3max = w->s3max;
+    a.b1 = (R*)w->b1; a.b2 = (R*)w->b2; a.b3 = (R*)w->b3;
+  }
   for (int k = 0; k < 3; ++k) {
     const int kk = k < ncomp ? k : 0;
     const int mtx = which == 0 ? kk : (which == 1 ? 3 : 4 + kk);
@@ -831,7 +983,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.eta = c.mixed ? c.refine_eta : 0.0;
   int mx = 0;
   for (auto& in : c.inst) mx = std::max(mx, in.cs.max_iter > 0 ? in.cs.max_iter : 10000);
-  a.iter_cap = 2 * mx + 64;
+  a.iter_cap = (mg ? 4 : 2) * mx + 256;
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
@@ -839,9 +991,9 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   k_init_solve<<<1, 32, 0, c.stream>>>(a.nsys, w->active, c.barrier, c.d_err);
   c.launches++;
   void* args[] = {&a};
-  if (two)
+  if (mg)
     PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, true>, dim3(w->grid[ph]), dim3(kSolveThreads),
-                                           args, w->smem_two, c.stream));
+                                           args, w->smem_mg, c.stream));
   else
     PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, false>, dim3(w->grid[ph]), dim3(kSolveThreads),
                                            args, 0, c.stream));
