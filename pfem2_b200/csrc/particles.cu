@@ -200,15 +200,24 @@ __global__ void __launch_bounds__(256) k_advect(
       x[d] = xi[d * cap + p];
       up[d] = u[d * cap + p];
     }
+    // vertex ids and velocities of the current cell, reloaded only when the
+    // particle changes cell (most stay for all S sub-steps)
+    int gvx[NV];
+    R vv[NV][DIM];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
     if (FUSE) {
       shape_values<DIM, R>(x, N);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        int g = __ldg(cv + (size_t)c * NV + v);
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
+        for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + gvx[v]);
       }
     }
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
     const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
     CellGeo<DIM, R> G = geo[c];
     LocalCell<DIM, R> L;
@@ -223,9 +232,8 @@ __global__ void __launch_bounds__(256) k_advect(
       for (int d = 0; d < DIM; ++d) uf[d] = R(0);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        int g = __ldg(cv + (size_t)c * NV + v);
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * __ldg(Vr + (size_t)d * nv + g);
+        for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * vv[v][d];
       }
       R xo[DIM], xn[DIM], x2[DIM];
       local_map<DIM, R>(L, x, xo);
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(256) k_advect(
         if (v == 0) best = dot;
         else if (dot > best) { best = dot; bv = v; }
       }
-      const int gv = __ldg(cv + (size_t)c * NV + bv);
+      const int gv = gvx[bv];
       R vp[DIM], vpn = R(0);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
@@ -308,7 +316,16 @@ __global__ void __launch_bounds__(256) k_advect(
           }
         }
       }
-      if (!found) alive = false;
+      if (!found) {
+        alive = false;
+      } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
+      }
     }
     if (!alive) {
       c = -1;
