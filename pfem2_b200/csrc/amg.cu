@@ -411,11 +411,13 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
   };
   for (int s = 0; s < ni; ++s) {
     std::vector<Level>& L = sysL[s];
+    const Csr P01 = spgemm(L[0].Pt2, L[1].Pt2);
     append_rows(transpose(L[0].Pt2), c.inst[s].v_off, H.r01_ptr, H.r01_col, H.r01_val);
-    append_rows(transpose(L[1].Pt2), goff[1][s], H.r12_ptr, H.r12_col, H.r12_val);
-    append_rows(transpose(spgemm(L[1].Pt2, L[2].Pt2)), goff[1][s], H.r13_ptr, H.r13_col, H.r13_val);
+    append_rows(transpose(P01), c.inst[s].v_off, H.r02_ptr, H.r02_col, H.r02_val);
     H.sys_D3.push_back(L[3].A.n);
     H.sys_off3.push_back(goff[3][s]);
+    H.sys_n2.push_back(L[2].A.n);
+    H.sys_off2.push_back(goff[2][s]);
     H.dmax = std::max(H.dmax, L[3].A.n);
   }
   // ---- per-block lists
@@ -434,8 +436,43 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
   H.p0_len.assign(c.nslices, 0);
   std::vector<std::vector<int>> p0c(c.nslices);
   std::vector<std::vector<double>> p0v(c.nslices);
+  for (int l = 1; l <= 2; ++l) H.lk[l].assign(H.n[l], 0);
+  std::vector<std::vector<int>> g3_rows(H.n[3]);
+  H.c3_blk.assign(1, 0);
   for (int b = 0; b < G; ++b) {
     const int t_lo = bt0[b], t_hi = bt0[b + 1];
+    // systems of a block are consecutive; lists store the index among them
+    const int sys_first = t_hi > t_lo ? sys_of_tile[t_lo] : 0;
+    for (int l = 1; l <= 2; ++l)
+      for (int g = H.toff[l][t_lo]; g < H.toff[l][t_hi]; ++g) H.lk[l][g] = H.lsys[l][g] - sys_first;
+    if (t_hi > t_lo) {
+      int n2 = 0;
+      for (int s = sys_of_tile[t_lo]; s <= sys_of_tile[t_hi - 1]; ++s) n2 += sysL[s][2].A.n;
+      H.b2max = std::max(H.b2max, n2);
+    }
+    // contributions of the own level-2 rows to b3 = Pt2^T b2: one row per
+    // touched level-3 dof, columns = own level-2 rows (relative index)
+    {
+      const int o2lo = H.toff[2][t_lo], o2hi = H.toff[2][t_hi];
+      std::vector<std::pair<int, std::pair<int, double>>> ent;  // (level-3 dof, (own row, value))
+      for (int g = o2lo; g < o2hi; ++g) {
+        const int s = H.lsys[2][g], a = g - goff[2][s];
+        const Csr& P = sysL[s][2].Pt2;
+        for (int e = P.ptr[a]; e < P.ptr[a + 1]; ++e) ent.push_back({goff[3][s] + P.col[e], {g - o2lo, P.val[e]}});
+      }
+      std::stable_sort(ent.begin(), ent.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+      for (size_t k = 0; k < ent.size(); ++k) {
+        if (k == 0 || ent[k].first != ent[k - 1].first) {
+          const int d = ent[k].first;
+          g3_rows[d].push_back((int)H.c3_lk.size());
+          H.c3_lk.push_back(H.lsys[3][d] - sys_first);
+          H.c3_ptr.push_back((int)H.c3_col.size());
+        }
+        H.c3_col.push_back(ent[k].second.first);
+        H.c3_val.push_back(ent[k].second.second);
+      }
+      H.c3_blk.push_back((int)H.c3_lk.size());
+    }
     // S1: own level-1 dofs, then the halo the level-0 prolongation reads
     std::vector<int> S1, S2, S3;
     for (int g = H.toff[1][t_lo]; g < H.toff[1][t_hi]; ++g) S1.push_back(g);
@@ -478,9 +515,11 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
       for (int g : *Sl[l]) {
         const int s = H.lsys[l][g], a = g - goff[l][s];
         const Level& V = sysL[s][l];
-        H.s_sys[l].push_back(s);
+        H.s_sys[l].push_back(s - sys_first);
         for (int e = V.J.ptr[a]; e < V.J.ptr[a + 1]; ++e) {
-          H.s_jcol[l].push_back(goff[l][s] + V.J.col[e]);
+          // level 1: global ids into b1; level 2: the system's own index
+          // into the block's shared copy of b2
+          H.s_jcol[l].push_back((l == 1 ? goff[l][s] : 0) + V.J.col[e]);
           H.s_jval[l].push_back(V.J.val[e]);
         }
         H.s_jptr[l].push_back((int)H.s_jcol[l].size());
@@ -495,14 +534,24 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
     H.s1max = std::max(H.s1max, (int)S1.size());
     H.s2max = std::max(H.s2max, (int)S2.size());
     H.s3max = std::max(H.s3max, (int)S3.size());
-    // level-3 entries: packed rows of the coarse inverse
+    // level-3 entries: the coarse-inverse rows of each system's entries,
+    // stored transposed ([d][entry]) so that the entries read consecutive
+    // shared-memory words
     int eb = 0;
-    for (int g : S3) {
-      const int s = H.lsys[3][g], r = g - goff[3][s], D = H.sys_D3[s];
-      H.s3_sys.push_back(s);
-      H.s3_eoff.push_back(eb);
-      for (int d = 0; d < D; ++d) H.s3_E.push_back((float)Einv[s][(size_t)r * D + d]);
-      eb += D;
+    for (size_t a = 0; a < S3.size();) {
+      const int s = H.lsys[3][S3[a]], D = H.sys_D3[s];
+      size_t b = a;
+      while (b < S3.size() && H.lsys[3][S3[b]] == s) ++b;
+      const int n = (int)(b - a);
+      for (size_t j = a; j < b; ++j) {
+        H.s3_sys.push_back(s - sys_first);
+        H.s3_eoff.push_back(eb + (int)(j - a));
+        H.s3_estr.push_back(n);
+      }
+      for (int d = 0; d < D; ++d)
+        for (size_t j = a; j < b; ++j) H.s3_E.push_back((float)Einv[s][(size_t)(S3[j] - goff[3][s]) * D + d]);
+      eb += D * n;
+      a = b;
     }
     H.blk_s3.push_back((int)H.s3_sys.size());
     H.blk_e.push_back((int)H.s3_E.size());
@@ -533,6 +582,12 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
     for (int g : S1) loc1[g] = -1;
     for (int g : S2) loc2[g] = -1;
     for (int g : S3) loc3[g] = -1;
+  }
+  H.c3_ptr.push_back((int)H.c3_col.size());
+  H.g3_ptr.assign(1, 0);
+  for (int d = 0; d < H.n[3]; ++d) {
+    for (int r : g3_rows[d]) H.g3_row.push_back(r);
+    H.g3_ptr.push_back((int)H.g3_row.size());
   }
   for (int sl = 0; sl < c.nslices; ++sl) {
     H.p0_ptr[sl + 1] = H.p0_ptr[sl] + H.p0_len[sl] * kSlice;

@@ -27,9 +27,19 @@ struct MgHost {
   int n[kMgLevels] = {0, 0, 0, 0};        // dofs per level over all systems
   std::vector<int> toff[kMgLevels];       // [l][ntiles+1] first level-l dof of each tile (l >= 1)
   std::vector<int> lsys[kMgLevels];       // [l][n_l] system of each level-l dof (l >= 1)
-  // restrictions (CSR over the rows of the coarse level, global columns)
-  std::vector<int> r01_ptr, r01_col, r12_ptr, r12_col, r13_ptr, r13_col;
-  std::vector<double> r01_val, r12_val, r13_val;
+  std::vector<int> lk[3];                 // [1..2][n_l] index of that system among its block's systems
+  // restrictions from level 0 (CSR over the rows of level l, global
+  // level-0 columns): R0l = (Pt_0 ... Pt_{l-1})^T, l = 1, 2
+  std::vector<int> r01_ptr, r01_col, r02_ptr, r02_col;
+  std::vector<double> r01_val, r02_val;
+  // b3 = Pt_2^T b2 in two steps: every block adds up the contributions of
+  // its own level-2 rows to the level-3 dofs they touch (CSR rows c3,
+  // columns = own level-2 row - first own row, grouped per block by c3_blk,
+  // c3_lk = the dof's system among the block's systems); each level-3 dof
+  // then sums its contribution rows g3_row[g3_ptr[d] .. g3_ptr[d+1]) in
+  // block order
+  std::vector<int> c3_blk, c3_ptr, c3_col, c3_lk, g3_ptr, g3_row;
+  std::vector<double> c3_val;
   // level-0 smoother J_0 on the SELL pattern of A
   std::vector<double> j0;
   // post-smoothed prolongator of level 0 on SELL slices; columns are the
@@ -37,16 +47,21 @@ struct MgHost {
   std::vector<int> p0_ptr, p0_len, p0_col;
   std::vector<double> p0_val;
   // per-block lists of the level-1 and level-2 dofs a block evaluates
-  // (own dofs and the halo its prolongation reads): J rows with global
-  // columns, Pt rows with columns into the block's next-level list
+  // (own dofs and the halo its prolongation reads): J rows (level 1:
+  // global columns; level 2: the system's level-2 index), Pt rows with
+  // columns into the block's next-level list
   std::vector<int> blk_s[3];              // [1..2][G+1] list offsets; [0] unused
+  // (s_sys, s3_sys: index of the entry's system among the block's systems)
   std::vector<int> s_sys[3], s_jptr[3], s_jcol[3], s_pptr[3], s_pcol[3];
   std::vector<double> s_jval[3], s_pval[3];
-  // per-block level-3 list: system, dense-inverse row packed per block
-  std::vector<int> blk_s3, s3_sys, s3_eoff, blk_e;
+  // per-block level-3 list: system, and where its column of the block's
+  // transposed coarse-inverse rows starts (stride s3_estr)
+  std::vector<int> blk_s3, s3_sys, s3_eoff, s3_estr, blk_e;
   std::vector<float> s3_E;
   std::vector<int> sys_D3, sys_off3;      // coarse size and first level-3 dof per system
+  std::vector<int> sys_n2, sys_off2;      // level-2 size and first level-2 dof per system
   int s1max = 0, s2max = 0, s3max = 0, emax = 0, dmax = 1;
+  int b2max = 0;                          // level-2 dofs of the local systems of a block
   // diagnostics
   std::vector<double> w;                  // smoother weight per system and level
 };

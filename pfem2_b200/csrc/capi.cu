@@ -585,13 +585,10 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   cudaSetDevice(c.device);
   cudaStreamSynchronize(c.stream);
   if (const char* path = getenv("PFEM2_SOLVER_PROFILE")) {
-    // solver sub-phase times of block 0, appended as one line per context
-    unsigned long long pr[18] = {};
-    krylov_profile(c, pr);
+    // solver phase profile (kind action:phases:mean us:max us:wait us), appended per context
+    const std::string pr = krylov_profile(c);
     if (FILE* f = fopen(path, "a")) {
-      fprintf(f, "prec=%s", c.mixed ? "mixed" : "fp64");
-      for (int k = 0; k < 18; ++k) fprintf(f, " %llu", pr[k]);
-      fprintf(f, "\n");
+      fprintf(f, "prec=%s\n%s", c.mixed ? "mixed" : "fp64", pr.c_str());
       fclose(f);
     }
   }

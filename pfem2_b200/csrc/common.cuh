@@ -303,6 +303,40 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& gb, unsigned& gl, c
   return s_ok != 0;
 }
 
+// Release/acquire grid barrier on an arrival counter that is never reset
+// within a launch: barrier k is passed once the counter reaches
+// gridDim.x * k. Thread 0 arrives with a gpu-scope release add and polls
+// with gpu-scope acquire loads (no separate fences); the CTA barriers on
+// both sides extend the ordering to the other threads of the block. `k`
+// is the caller's barrier count (0 after the reset that precedes every
+// launch). The poll gives up after PFEM2_BARRIER_SPIN_LIMIT tries or when
+// another block has flagged an error, sets gb.err = 1 and returns false.
+__device__ __forceinline__ bool grid_sync_ra(const GridBarrier& gb, unsigned& k) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    ++k;
+    const unsigned target = gridDim.x * k;
+    unsigned v;
+    asm volatile("atom.add.release.gpu.u32 %0, [%1], 1;" : "=r"(v) : "l"(gb.count) : "memory");
+    int ok = 1;
+    unsigned spins = 0;
+    while (true) {
+      asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(gb.count) : "memory");
+      if ((int)(v - target) >= 0) break;
+      if (++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)gb.err) {
+        atomicExch(gb.err, 1);
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

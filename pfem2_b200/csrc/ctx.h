@@ -40,6 +40,8 @@ struct Tile {
   int sys;        // system id inside the phase
   int comp;       // component slot (vector block)
   int s0, s1;     // slice range
+  int slot;       // partial-sum slot (the slots of a system are contiguous)
+  int lk;         // index of the system among the systems of the tile's block
 };
 
 struct Ctx {
@@ -213,6 +215,6 @@ void krylov_free(Ctx& c);
 // which: 0 prediction (dim systems per instance), 1 pressure, 2 correction
 pfem2_status krylov_solve(Ctx& c, int which);
 pfem2_status krylov_read_stats(Ctx& c);
-void krylov_profile(Ctx& c, unsigned long long* out18);
+std::string krylov_profile(Ctx& c);
 
 }  // namespace pfem2

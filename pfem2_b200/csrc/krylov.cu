@@ -20,13 +20,16 @@
 //   A  p' = z + beta p ; q = A p'                 (p double buffered) | (p', q)
 //   B  e += alpha p' ; r -= alpha q ; z = D^-1 r                     | (r, z), (r, r)
 // The pressure systems are preconditioned with one multigrid V(1,1) cycle
-// in additive form (amg.h) and take four:
+// in additive form (amg.h) and take three:
 //   B   e += alpha p' ; r' = r - alpha q (r double buffered) ;
-//       b1 = R01 r' (level-1 rows of the block, r' formed on the fly)  | (r', r')
-//   D   b2 = R12 b1 ; b3 = R13 b1
-//   UZ  x3 = E^-1 b3, x2 = J2 b2 + Pt2 x3, x1 = J1 b1 + Pt1 x2 on the
-//       block's own and halo coarse dofs (shared memory, redundant across
-//       blocks), z = J0 r + Pt0 x1 on the own rows                  | (r, z)
+//       b_l = R0l r' on the block's own level-l rows, l = 1, 2, with r'
+//       formed on the fly from r and q                              | (r', r')
+//       and the own level-2 rows' contributions to b3 = Pt2^T b2
+//   UZ  first every global read: b2 of the block's systems, b3 (summing
+//       the blocks' contributions), J1 b1 on its level-1 list, J0 r on
+//       its own rows; then in shared memory J2 b2, x3 = E^-1 b3,
+//       x2 = J2 b2 + Pt2 x3, x1 = J1 b1 + Pt1 x2 (own and halo coarse
+//       dofs, redundant across blocks); z = J0 r + Pt0 x1           | (r, z)
 //   A   p' = z + beta p ; q = A p'                                  | (p', q)
 // so the coarse levels never need a barrier of their own.
 //
@@ -51,37 +54,68 @@ constexpr int kSolveThreads = 384;  // 12 warps
 constexpr int kWarps = kSolveThreads / 32;
 constexpr int kMaxLocalSys = 16;
 
-enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_D = 5, S_UZ = 6 };
-enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_D = 6, ACT_UZ = 7 };
+enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_UZ = 5 };
+enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_UZ = 6 };
+
+constexpr int kMaxBlockTiles = 64;
+
+// categories of per-block static data copied into shared memory at kernel
+// start (every grid barrier's GPU-scope fence invalidates L1, so static
+// indices read from global memory would cost an L2 round trip per phase)
+enum {
+  ST_L0META = 1,  // slice pointers / lengths of the block's slice range
+  ST_L0COL = 2,   // SELL columns of that range
+  ST_MGIDX = 4,   // multigrid row pointers and local system indices
+  ST_MGCOL = 8,   // multigrid columns
+  ST_MGVAL = 16,  // values of the multigrid operators applied to shared vectors
+  ST_MIRROR = 32, // multigrid: shared copies of the block's own rows of r, z, p, q, e
+};
+
+// a read-only array seen either in global memory (base 0) or through a
+// staged shared-memory copy of its range [base, ...)
+template <typename T>
+struct SV {
+  const T* p;
+  int base;
+  __device__ __forceinline__ T operator[](int i) const { return p[i - base]; }
+};
 
 template <typename R> struct SolveArgs {
   int ncomp, ninst, nsys, ntiles, nv;
   const Tile* tiles;
-  const int* sys_t0;     // [nsys+1] first tile of each system
-  const int* blk_t0;     // [grid+1] first tile of each block
+  const int* sys_slot0;   // [nsys+1] first partial slot of each system
+  const int* sys_owner;   // [nsys] block that reports the system's result
+  const int* blk_t0;      // [grid+1] first tile of each block
+  const int* blk_sys;     // systems of each block, at blk_sys_off[b]
+  const int* blk_sys_off;
+  const int* blk_sl;      // [2 grid] slice range [s0, s1) of each block's tiles
   const int* sl_ptr;
   const int* sl_len;
   const int* sl_col;
   const double* A64[3];
   const R* Ain[3];
   const R* dinv[3];
+  int stage;              // ST_* categories staged in shared memory
   // multigrid (pressure phase), layout of MgHost
-  const int *toff1, *toff2, *toff3;     // [ntiles+1]
-  const int *lsys1, *lsys2, *lsys3;     // system of each level-l dof
-  const int *r01_ptr, *r01_col, *r12_ptr, *r12_col, *r13_ptr, *r13_col;
-  const R *r01_val, *r12_val, *r13_val;
+  const int *toff1, *toff2;             // [ntiles+1]
+  const int *lk1, *lk2;                 // local system index of each level-1/2 dof (in its owner block)
+  const int *r01_ptr, *r01_col, *r02_ptr, *r02_col;
+  const R *r01_val, *r02_val;
+  const int *c3_blk, *c3_ptr, *c3_col, *c3_lk, *g3_ptr, *g3_row;
+  const R* c3_val;
+  R* contrib;                           // [c3 rows] contributions to b3
   const R* j0;                          // [nell]
   const int *p0_ptr, *p0_len, *p0_col;  // SELL per slice, columns into the block's level-1 list
   const R* p0_val;
-  const int *blk_s1, *s1_sys, *s1_jptr, *s1_jcol, *s1_pptr, *s1_pcol;
+  const int *blk_s1, *s1_lk, *s1_jptr, *s1_jcol, *s1_pptr, *s1_pcol;
   const R *s1_jval, *s1_pval;
-  const int *blk_s2, *s2_sys, *s2_jptr, *s2_jcol, *s2_pptr, *s2_pcol;
+  const int *blk_s2, *s2_lk, *s2_jptr, *s2_jcol, *s2_pptr, *s2_pcol;
   const R *s2_jval, *s2_pval;
-  const int *blk_s3, *s3_sys, *s3_eoff, *blk_e;
+  const int *blk_s3, *s3_lk, *s3_eoff, *s3_estr, *blk_e;
   const float* s3_E;
-  const int *sys_D3, *sys_off3;
-  int dmax, s1max, s2max, s3max;
-  R *b1, *b2, *b3;
+  const int *sys_D3, *sys_off3, *sys_n2, *sys_off2;
+  int dmax, s1max, s2max, s3max, b2max, o2max, emax;
+  R *b1, *b2;
   double* x[3];
   const double* b[3];
   const unsigned char* isd[3];
@@ -91,7 +125,7 @@ template <typename R> struct SolveArgs {
   // workspace per component slot, nv entries each; r and p: 2 buffers
   R *e, *r, *z, *p, *q;
   double* r64;
-  double* part;          // [2][ntiles][3], by phase parity
+  double* part;          // [2 parities][2 sums][ntiles slots]
   int* active;
   int* out_it;           // [nsys] iterations
   double* out_res;       // [nsys] final residual norm
@@ -99,7 +133,7 @@ template <typename R> struct SolveArgs {
   double eta;
   int iter_cap;
   GridBarrier gb;
-  unsigned long long* prof;  // optional: ns spent per sub-phase by block 0 (PFEM2_SOLVER_PROFILE)
+  unsigned long long* prof;  // optional [grid][8 actions][3]: phases, work ns, barrier-wait ns (PFEM2_SOLVER_PROFILE)
 };
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -118,59 +152,163 @@ __device__ __forceinline__ T group_sum(T v) {
   return v;
 }
 
+// acc + sum over the entries of a SELL row of val(ei) * x(col), in entry
+// order, with the loads of CH entries issued before their products are
+// accumulated (one memory round trip per CH entries instead of one per entry)
+template <typename T, int CH = 8, typename Cols, typename Val, typename X>
+__device__ __forceinline__ T sell_dot(T acc, Cols cols, int base, int len, int lane, Val val, X x) {
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    T av[CH], xv[CH];
+#pragma unroll
+    for (int u = 0; u < CH; ++u) {
+      const int j = j0 + u;
+      if (j < len) {
+        const int ei = base + j * 32 + lane;
+        av[u] = val(ei);
+        xv[u] = x(cols[ei]);
+      } else {
+        av[u] = T(0);
+        xv[u] = T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < CH; ++u) acc = fma_r(av[u], xv[u], acc);
+  }
+  return acc;
+}
+
+// x[col] from the shared mirror m of the block's own rows [own0, own0 +
+// nown) when there is one, else from global memory: one generic load, no
+// branch (plain loads see the other blocks' writes of the previous phase,
+// which the grid barrier's acquire ordered before them)
+template <typename R>
+__device__ __forceinline__ R ldm(const R* g, const R* m, int col, int own0, int nown) {
+  const unsigned o = (unsigned)(col - own0);
+  const R* src = (m != nullptr && o < (unsigned)nown) ? m + o : g + col;
+  return *src;
+}
+
+// acc + sum over CSR entries [k0, k1) of val(k) * x(col(k)), the lanes of a
+// group of GL taking every GL-th entry, loads issued CH entries at a time
+template <int GL, int CH, typename T, typename Cols, typename Val, typename X>
+__device__ __forceinline__ T csr_dot(T acc, int k0, int k1, int sub, Cols cols, Val val, X x) {
+  for (int kb = k0 + sub; kb < k1; kb += CH * GL) {
+    T av[CH], xv[CH];
+#pragma unroll
+    for (int u = 0; u < CH; ++u) {
+      const int k = kb + u * GL;
+      if (k < k1) {
+        av[u] = val[k];
+        xv[u] = x(cols[k]);
+      } else {
+        av[u] = T(0);
+        xv[u] = T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < CH; ++u) acc = fma_r(av[u], xv[u], acc);
+  }
+  return acc;
+}
+
 struct LocalSys {
   int sys, state, it, outer, par, rpar, first, owner, maxit, act, chk;
+  int t0, t1;                       // partial slots of the system
+  int D3, off3, n2, off2, b2off;    // multigrid: coarse sizes and offsets
   double tol, intol, res, rz_prev, alpha, beta;
   double sum[2];
 };
 
+// copies src[lo, hi) into shared memory at `cur` (16-byte aligned pieces)
+// and returns the view of that range; the caller syncs before reading it
+__device__ __forceinline__ size_t al16_dev(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <typename T>
+__device__ __forceinline__ SV<T> stage_range(unsigned char*& cur, const T* src, int lo, int hi) {
+  T* dst = reinterpret_cast<T*>(cur);
+  for (int i = threadIdx.x; i < hi - lo; i += blockDim.x) dst[i] = src[lo + i];
+  cur += ((size_t)(hi - lo) * sizeof(T) + 15) & ~(size_t)15;
+  return SV<T>{dst, lo};
+}
+
+template <typename T>
+__device__ __forceinline__ SV<T> maybe_stage(bool on, unsigned char*& cur, const T* src, int lo, int hi) {
+  return on ? stage_range(cur, src, lo, hi) : SV<T>{src, 0};
+}
+
 template <typename R, bool MG>
-__global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
+__global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ LocalSys ls[kMaxLocalSys];
+  __shared__ Tile stile[kMaxBlockTiles];
   __shared__ double red[kWarps][2];
-  __shared__ int s_nls, s_sys0;
+  __shared__ int s_nls;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t nv = (size_t)a.nv;
   const int t_lo = a.blk_t0[blockIdx.x], t_hi = a.blk_t0[blockIdx.x + 1];
+  const int ntl = t_hi - t_lo;
+  const bool tiles_staged = ntl <= kMaxBlockTiles;
   unsigned bar_gen = 0;
 
   // ---- local systems of this block
   if (threadIdx.x == 0) {
-    int n = 0, s0 = -1;
-    if (t_hi > t_lo) {
-      s0 = a.tiles[t_lo].sys;
-      n = a.tiles[t_hi - 1].sys - s0 + 1;
-    }
+    const int o = a.blk_sys_off[blockIdx.x];
+    int n = a.blk_sys_off[blockIdx.x + 1] - o;
     if (n > kMaxLocalSys) n = kMaxLocalSys;  // the host guarantees n <= kMaxLocalSys
     s_nls = n;
-    s_sys0 = s0;
+    int b2off = 0;
     for (int k = 0; k < n; ++k) {
       LocalSys& L = ls[k];
-      const int s = s0 + k, inst = s % a.ninst;
+      const int s = a.blk_sys[o + k], inst = s % a.ninst;
       L.sys = s;
       L.state = S_OUT_A;
       L.it = L.outer = L.par = L.rpar = L.chk = 0;
       L.first = 1;
-      L.owner = a.sys_t0[s] >= t_lo && a.sys_t0[s] < t_hi;
+      L.owner = a.sys_owner[s] == (int)blockIdx.x;
+      L.t0 = a.sys_slot0[s];
+      L.t1 = a.sys_slot0[s + 1];
       L.maxit = a.maxit_i[inst];
       L.tol = a.tol_i[inst];
       L.intol = 0.5 * L.tol;
       L.res = L.rz_prev = L.alpha = L.beta = 0.0;
       L.sum[0] = L.sum[1] = 0.0;
       L.act = ACT_NONE;
+      L.D3 = L.off3 = L.n2 = L.off2 = L.b2off = 0;
+      if (MG) {
+        L.D3 = a.sys_D3[s];
+        L.off3 = a.sys_off3[s];
+        L.n2 = a.sys_n2[s];
+        L.off2 = a.sys_off2[s];
+        L.b2off = b2off;
+        b2off += L.n2;
+      }
     }
   }
+  if (tiles_staged)
+    for (int i = threadIdx.x; i < ntl; i += kSolveThreads) stile[i] = a.tiles[t_lo + i];
   __syncthreads();
-  const int nls = s_nls, sys0 = s_sys0;
-  // multigrid shared memory: x1 | x2 | x3 | b3 per local system (R), coarse-inverse rows (float)
+  const int nls = s_nls;
+  auto tile_at = [&](int t) -> Tile { return tiles_staged ? stile[t - t_lo] : a.tiles[t]; };
+
+  // ---- shared memory: multigrid vectors, then the staged static data
   R* sx1 = reinterpret_cast<R*>(dyn_smem);
   R* sx2 = sx1 + a.s1max;
   R* sx3 = sx2 + a.s2max;
   R* sb3 = sx3 + a.s3max;
-  float* sE = reinterpret_cast<float*>(sb3 + (size_t)nls * a.dmax);
-  int s1_lo = 0, s1_hi = 0, s2_lo = 0, s2_hi = 0, s3_lo = 0, s3_hi = 0, o1lo = 0, o1hi = 0, o2lo = 0, o2hi = 0,
-      o3lo = 0, o3hi = 0;
+  R* sb2 = sb3 + (size_t)nls * a.dmax;
+  R* sb2o = sb2 + a.b2max;  // own level-2 rows during B (systems may be in UZ meanwhile)
+  float* sE = reinterpret_cast<float*>(sb2o + a.o2max);
+  unsigned char* cur =
+      reinterpret_cast<unsigned char*>(sE) + (((size_t)a.emax * sizeof(float) + 15) & ~(size_t)15);
+  const int bs0 = a.blk_sl[2 * blockIdx.x], bs1 = a.blk_sl[2 * blockIdx.x + 1];
+  const SV<int> SLp = maybe_stage<int>(a.stage & ST_L0META, cur, a.sl_ptr, bs0, bs1 + 1);
+  const SV<int> SLl = maybe_stage<int>(a.stage & ST_L0META, cur, a.sl_len, bs0, bs1);
+  const SV<int> SLc = maybe_stage<int>(a.stage & ST_L0COL, cur, a.sl_col, a.sl_ptr[bs0], a.sl_ptr[bs1]);
+  int s1_lo = 0, s1_hi = 0, s2_lo = 0, s2_hi = 0, s3_lo = 0, s3_hi = 0, o1lo = 0, o1hi = 0, o2lo = 0, o2hi = 0;
+  SV<int> LK1{}, LK2{}, R01P{}, R01C{}, R02P{}, R02C{}, S1K{}, J1P{}, J1C{}, P1P{}, P1C{}, S2K{}, J2P{}, J2C{}, P2P{},
+      P2C{}, S3K{}, S3E{}, S3S{}, C3K{}, C3P{}, C3C{}, G3P{}, G3R{}, P0P{}, P0L{}, P0C{};
+  SV<R> P1V{}, J2V{}, P2V{}, C3V{}, P0V{};
+  int c3lo = 0, c3hi = 0;
   if (MG) {
     s1_lo = a.blk_s1[blockIdx.x];
     s1_hi = a.blk_s1[blockIdx.x + 1];
@@ -182,15 +320,65 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
     o1hi = a.toff1[t_hi];
     o2lo = a.toff2[t_lo];
     o2hi = a.toff2[t_hi];
-    o3lo = a.toff3[t_lo];
-    o3hi = a.toff3[t_hi];
     const int e0 = a.blk_e[blockIdx.x], ne = a.blk_e[blockIdx.x + 1] - e0;
     for (int i = threadIdx.x; i < ne; i += kSolveThreads) sE[i] = a.s3_E[e0 + i];
+    const bool si = a.stage & ST_MGIDX, sc = a.stage & ST_MGCOL, sv = a.stage & ST_MGVAL;
+    // level-3 rows of the block's systems (consecutive systems, consecutive rows)
+    const int r3lo = nls > 0 ? ls[0].off3 : 0, r3hi = nls > 0 ? ls[nls - 1].off3 + ls[nls - 1].D3 : 0;
+    c3lo = a.c3_blk[blockIdx.x];
+    c3hi = a.c3_blk[blockIdx.x + 1];
+    LK1 = maybe_stage<int>(si, cur, a.lk1, o1lo, o1hi);
+    R01P = maybe_stage<int>(si, cur, a.r01_ptr, o1lo, o1hi + 1);
+    LK2 = maybe_stage<int>(si, cur, a.lk2, o2lo, o2hi);
+    R02P = maybe_stage<int>(si, cur, a.r02_ptr, o2lo, o2hi + 1);
+    S1K = maybe_stage<int>(si, cur, a.s1_lk, s1_lo, s1_hi);
+    J1P = maybe_stage<int>(si, cur, a.s1_jptr, s1_lo, s1_hi + 1);
+    P1P = maybe_stage<int>(si, cur, a.s1_pptr, s1_lo, s1_hi + 1);
+    S2K = maybe_stage<int>(si, cur, a.s2_lk, s2_lo, s2_hi);
+    J2P = maybe_stage<int>(si, cur, a.s2_jptr, s2_lo, s2_hi + 1);
+    P2P = maybe_stage<int>(si, cur, a.s2_pptr, s2_lo, s2_hi + 1);
+    S3K = maybe_stage<int>(si, cur, a.s3_lk, s3_lo, s3_hi);
+    S3E = maybe_stage<int>(si, cur, a.s3_eoff, s3_lo, s3_hi);
+    S3S = maybe_stage<int>(si, cur, a.s3_estr, s3_lo, s3_hi);
+    C3K = maybe_stage<int>(si, cur, a.c3_lk, c3lo, c3hi);
+    C3P = maybe_stage<int>(si, cur, a.c3_ptr, c3lo, c3hi + 1);
+    G3P = maybe_stage<int>(si, cur, a.g3_ptr, r3lo, r3hi + 1);
+    G3R = maybe_stage<int>(si, cur, a.g3_row, a.g3_ptr[r3lo], a.g3_ptr[r3hi]);
+    P0P = maybe_stage<int>(si, cur, a.p0_ptr, bs0, bs1 + 1);
+    P0L = maybe_stage<int>(si, cur, a.p0_len, bs0, bs1);
+    R01C = maybe_stage<int>(sc, cur, a.r01_col, a.r01_ptr[o1lo], a.r01_ptr[o1hi]);
+    R02C = maybe_stage<int>(sc, cur, a.r02_col, a.r02_ptr[o2lo], a.r02_ptr[o2hi]);
+    J1C = maybe_stage<int>(sc, cur, a.s1_jcol, a.s1_jptr[s1_lo], a.s1_jptr[s1_hi]);
+    P1C = maybe_stage<int>(sc, cur, a.s1_pcol, a.s1_pptr[s1_lo], a.s1_pptr[s1_hi]);
+    J2C = maybe_stage<int>(sc, cur, a.s2_jcol, a.s2_jptr[s2_lo], a.s2_jptr[s2_hi]);
+    P2C = maybe_stage<int>(sc, cur, a.s2_pcol, a.s2_pptr[s2_lo], a.s2_pptr[s2_hi]);
+    C3C = maybe_stage<int>(sc, cur, a.c3_col, a.c3_ptr[c3lo], a.c3_ptr[c3hi]);
+    P0C = maybe_stage<int>(sc, cur, a.p0_col, a.p0_ptr[bs0], a.p0_ptr[bs1]);
+    P1V = maybe_stage<R>(sv, cur, a.s1_pval, a.s1_pptr[s1_lo], a.s1_pptr[s1_hi]);
+    J2V = maybe_stage<R>(sv, cur, a.s2_jval, a.s2_jptr[s2_lo], a.s2_jptr[s2_hi]);
+    P2V = maybe_stage<R>(sv, cur, a.s2_pval, a.s2_pptr[s2_lo], a.s2_pptr[s2_hi]);
+    C3V = maybe_stage<R>(sv, cur, a.c3_val, a.c3_ptr[c3lo], a.c3_ptr[c3hi]);
+    P0V = maybe_stage<R>(sv, cur, a.p0_val, a.p0_ptr[bs0], a.p0_ptr[bs1]);
+  }
+  const SV<R> R01V{a.r01_val, 0}, R02V{a.r02_val, 0}, J1V{a.s1_jval, 0};
+  // shared mirrors of the own rows of the pressure vectors (multigrid)
+  const int own0 = bs0 * 32, nown = (bs1 - bs0) * 32;
+  R *mr[2] = {nullptr, nullptr}, *mz = nullptr, *mp[2] = {nullptr, nullptr}, *mq = nullptr, *me = nullptr;
+  if (MG && (a.stage & ST_MIRROR)) {
+    R* m = reinterpret_cast<R*>(cur);
+    mr[0] = m;
+    mr[1] = m + nown;
+    mz = m + 2 * nown;
+    mp[0] = m + 3 * nown;
+    mp[1] = m + 4 * nown;
+    mq = m + 5 * nown;
+    me = m + 6 * nown;
+    cur += al16_dev((size_t)7 * nown * sizeof(R));
   }
 
   // ---- init: Dirichlet values preset in x, e = 0, p = 0
   for (int t = t_lo; t < t_hi; ++t) {
-    const Tile T = a.tiles[t];
+    const Tile T = tile_at(t);
     const int k = T.comp;
     for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
       const int row = sl * 32 + lane;
@@ -198,39 +386,51 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       a.e[k * nv + row] = R(0);
       a.p[(2 * k) * nv + row] = R(0);
       a.p[(2 * k + 1) * nv + row] = R(0);
+      if (me) {
+        me[row - own0] = R(0);
+        mp[0][row - own0] = R(0);
+        mp[1][row - own0] = R(0);
+      }
     }
   }
-  bool stop = false;
-  if (!grid_sync(a.gb, bar_gen)) return;
+  __shared__ int s_stop;
+  if (!grid_sync_ra(a.gb, bar_gen)) return;
 
-  const bool prof = a.prof != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
-  unsigned long long tp[6] = {0, 0, 0, 0, 0, 0}, tlast = prof ? gtimer() : 0;
-#define PFEM2_PROF(k)                       \
-  if (prof) {                               \
-    const unsigned long long tn = gtimer(); \
-    tp[k] += tn - tlast;                    \
-    tlast = tn;                             \
-  }
+  // optional profile of every block: per action of its first local system,
+  // the phases run, the time from the end of the last barrier to the
+  // arrival at the next one (work) and the wait there
+  const bool prof = a.prof != nullptr && threadIdx.x == 0;
+  unsigned long long pacc[8][3] = {}, t_phase = prof ? gtimer() : 0;
+  int plabel = ACT_NONE;
   for (int iter = 0;; ++iter) {
-    if (stop) break;  // published by the last barrier: every system is done
     if (iter >= a.iter_cap) {
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.gb.err, 2);
       break;
     }
     const bool phaseA = (iter & 1) == 0;
-    const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 3;
-    PFEM2_PROF(5);
-    // ---- sums of the previous phase's partials (warp 0, fixed order)
+    const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 2;
+    // ---- sums of the previous phase's partials (warp 0, fixed order), and
+    // the count of systems still running (0: every system is done)
     if (warp == 0) {
+      if (lane == 0) s_stop = *(volatile const int*)a.active <= 0;
       for (int k = 0; k < nls; ++k) {
         const int st = ls[k].state;
-        if (st == S_DONE || st == S_OUT_A || st == S_UZ || (st == S_D && !ls[k].chk)) continue;
-        const int t0 = a.sys_t0[ls[k].sys], t1 = a.sys_t0[ls[k].sys + 1];
+        if (st == S_DONE || st == S_OUT_A || (st == S_UZ && !ls[k].chk)) continue;
+        const int t0 = ls[k].t0, t1 = ls[k].t1;
         double s0 = 0.0, s1 = 0.0;
-#pragma unroll 4
-        for (int t = t0 + lane; t < t1; t += 32) {
-          s0 += __ldcg(prev + (size_t)t * 3);
-          s1 += __ldcg(prev + (size_t)t * 3 + 1);
+        for (int tb = t0; tb < t1; tb += 256) {
+          double v0[8], v1[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int t = tb + u * 32 + lane;
+            v0[u] = t < t1 ? __ldcg(prev + t) : 0.0;
+            v1[u] = t < t1 ? __ldcg(prev + a.ntiles + t) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            s0 += v0[u];
+            s1 += v1[u];
+          }
         }
         s0 = warp_sum(s0);
         s1 = warp_sum(s1);
@@ -241,7 +441,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       }
     }
     __syncthreads();
-    PFEM2_PROF(0);
+    if (s_stop) break;
     // ---- decisions (thread 0; identical in every block owning the system)
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
@@ -302,24 +502,20 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
                 L.first = 1;  // CG restarts from the true residual
                 L.chk = 0;
                 act = ACT_OUT_B;
-                L.state = S_D;
+                L.state = S_UZ;
               }
               break;
-            case S_D: {
+            case S_UZ: {
               const double rr = sqrt(L.sum[0]);
               if (L.chk && (rr <= L.intol || L.it >= L.maxit || !(rr == rr))) {
                 act = ACT_OUT_A;  // reliable update in FP64
                 L.state = S_OUT_B;
               } else {
-                act = ACT_D;
-                L.state = S_UZ;
+                act = ACT_UZ;
+                L.state = S_A;
               }
               break;
             }
-            case S_UZ:
-              act = ACT_UZ;
-              L.state = S_A;
-              break;
             case S_A: {
               const double rz = L.sum[0];
               L.beta = L.first ? 0.0 : (L.rz_prev != 0.0 ? rz / L.rz_prev : 0.0);
@@ -334,7 +530,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
               L.it += 1;
               L.chk = 1;
               act = ACT_B;
-              L.state = S_D;
+              L.state = S_UZ;
               break;
             default:
               break;
@@ -342,89 +538,128 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         }
         L.act = act;
       }
+      plabel = nls > 0 ? ls[0].act : ACT_NONE;
     }
     __syncthreads();
-    PFEM2_PROF(2);
     // ---- coarse-level work of the block (multigrid; pressure = component 0)
     if (MG) {
-      bool any_b = false, any_d = false, any_uz = false;
+      bool any_b = false, any_uz = false;
       for (int k = 0; k < nls; ++k) {
         const int act = ls[k].act;
         any_b |= act == ACT_B || act == ACT_OUT_B;
-        any_d |= act == ACT_D;
         any_uz |= act == ACT_UZ;
       }
       if (any_b) {
-        // b1 = R01 r' on the own level-1 rows (8 lanes per row); after a
-        // reliable update r' = r64, else r' = r - alpha q formed on the fly
-        constexpr int GL = 8, NG = kSolveThreads / GL;
-        const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
-        for (int base = o1lo; base < o1hi; base += NG) {
-          const int i = base + grp;
-          R acc = R(0);
-          int act = ACT_NONE;
-          if (i < o1hi) {
-            const LocalSys& L = ls[__ldg(a.lsys1 + i) - sys0];
-            act = L.act;
-            const int k1 = __ldg(a.r01_ptr + i + 1);
-            if (act == ACT_B) {
-              const R al = R(L.alpha);
-              const R* rr = a.r + (size_t)L.rpar * nv;
-#pragma unroll 4
-              for (int k = __ldg(a.r01_ptr + i) + sub; k < k1; k += GL) {
-                const int j = __ldg(a.r01_col + k);
-                acc += __ldg(a.r01_val + k) * fma_r(-al, __ldcg(a.q + j), __ldcg(rr + j));
+        // b_l = R0l r' on the own level-l rows; after a reliable update
+        // r' = r64, else r' = r - alpha q formed on the fly. Level 1: 8 lanes
+        // per row; level 2 (long rows): a warp per row.
+        {
+          constexpr int GL = 8, NG = kSolveThreads / GL;
+          const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+          for (int base = o1lo; base < o1hi; base += NG) {
+            const int i = base + grp;
+            R acc = R(0);
+            int act = ACT_NONE;
+            if (i < o1hi) {
+              const LocalSys& L = ls[LK1[i]];
+              act = L.act;
+              const int k0 = R01P[i], k1 = R01P[i + 1];
+              if (act == ACT_B) {
+                const R al = R(L.alpha);
+                const R* rr = a.r + (size_t)L.rpar * nv;
+                const R* mrr = mr[L.rpar];
+                acc = csr_dot<GL, 8, R>(acc, k0, k1, sub, R01C, R01V, [&](int j) {
+                  return fma_r(-al, ldm(a.q, mq, j, own0, nown), ldm(rr, mrr, j, own0, nown));
+                });
+              } else if (act == ACT_OUT_B) {
+                acc = csr_dot<GL, 8, R>(acc, k0, k1, sub, R01C, R01V, [&](int j) { return R(__ldcg(a.r64 + j)); });
               }
-            } else if (act == ACT_OUT_B) {
-#pragma unroll 4
-              for (int k = __ldg(a.r01_ptr + i) + sub; k < k1; k += GL)
-                acc += __ldg(a.r01_val + k) * R(__ldcg(a.r64 + __ldg(a.r01_col + k)));
             }
+            acc = group_sum<GL>(acc);
+            if (sub == 0 && (act == ACT_B || act == ACT_OUT_B)) a.b1[i] = acc;
           }
-          acc = group_sum<GL>(acc);
-          if (sub == 0 && (act == ACT_B || act == ACT_OUT_B)) a.b1[i] = acc;
         }
-      }
-      if (any_d) {
-        // b2 = R12 b1, b3 = R13 b1 on the own level-2 / level-3 rows (warp per row)
-        const int n2 = o2hi - o2lo, n3 = o3hi - o3lo;
-        for (int w = warp; w < n2 + n3; w += kWarps) {
-          const bool l2 = w < n2;
-          const int i = l2 ? o2lo + w : o3lo + (w - n2);
-          if (ls[__ldg((l2 ? a.lsys2 : a.lsys3) + i) - sys0].act != ACT_D) continue;
-          const int* ptr = l2 ? a.r12_ptr : a.r13_ptr;
-          const int* cl = l2 ? a.r12_col : a.r13_col;
-          const R* vl = l2 ? a.r12_val : a.r13_val;
+        for (int i = o2lo + warp; i < o2hi; i += kWarps) {
+          const LocalSys& L = ls[LK2[i]];
+          const int act = L.act;
+          if (act != ACT_B && act != ACT_OUT_B) continue;
+          const int k0 = R02P[i], k1 = R02P[i + 1];
           R acc = R(0);
-          const int k1 = __ldg(ptr + i + 1);
-#pragma unroll 4
-          for (int k = __ldg(ptr + i) + lane; k < k1; k += 32) acc += __ldg(vl + k) * __ldcg(a.b1 + __ldg(cl + k));
+          if (act == ACT_B) {
+            const R al = R(L.alpha);
+            const R* rr = a.r + (size_t)L.rpar * nv;
+            const R* mrr = mr[L.rpar];
+            acc = csr_dot<32, 8, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) {
+              return fma_r(-al, ldm(a.q, mq, j, own0, nown), ldm(rr, mrr, j, own0, nown));
+            });
+          } else {
+            acc = csr_dot<32, 8, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) { return R(__ldcg(a.r64 + j)); });
+          }
           acc = warp_sum(acc);
-          if (lane == 0) (l2 ? a.b2 : a.b3)[i] = acc;
+          if (lane == 0) {
+            a.b2[i] = acc;
+            sb2o[i - o2lo] = acc;
+          }
+        }
+        __syncthreads();
+        // contributions of the own level-2 rows to b3 (thread per row)
+        for (int rr = c3lo + threadIdx.x; rr < c3hi; rr += kSolveThreads) {
+          const int act = ls[C3K[rr]].act;
+          if (act != ACT_B && act != ACT_OUT_B) continue;
+          a.contrib[rr] = csr_dot<1, 4, R>(R(0), C3P[rr], C3P[rr + 1], 0, C3C, C3V, [&](int c) { return sb2o[c]; });
         }
       }
       if (any_uz) {
-        // b3 of the local systems
+        // every global read first: b2 of the local systems, J1 b1 on the
+        // level-1 list, J0 r on the own rows (into z)
         for (int k = 0; k < nls; ++k) {
           if (ls[k].act != ACT_UZ) continue;
-          const int s = ls[k].sys, D = __ldg(a.sys_D3 + s), o = __ldg(a.sys_off3 + s);
-          for (int d = threadIdx.x; d < D; d += kSolveThreads) sb3[k * a.dmax + d] = __ldcg(a.b3 + o + d);
+          const int n = ls[k].n2, o = ls[k].off2;
+          for (int d = threadIdx.x; d < n; d += kSolveThreads) sb2[ls[k].b2off + d] = __ldcg(a.b2 + o + d);
+          const int D = ls[k].D3, o3 = ls[k].off3;
+          for (int d = threadIdx.x; d < D; d += kSolveThreads) {
+            const int q0 = G3P[o3 + d], q1 = G3P[o3 + d + 1];
+            R acc = R(0);
+            for (int qb = q0; qb < q1; qb += 8) {
+              R v[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) v[u] = qb + u < q1 ? __ldcg(a.contrib + G3R[qb + u]) : R(0);
+#pragma unroll
+              for (int u = 0; u < 8; ++u) acc += v[u];
+            }
+            sb3[k * a.dmax + d] = acc;
+          }
+        }
+        {
+          constexpr int GL = 2, NG = kSolveThreads / GL;
+          const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+          for (int base = s1_lo; base < s1_hi; base += NG) {
+            const int j = base + grp;
+            R acc = R(0);
+            bool on = false;
+            if (j < s1_hi && ls[S1K[j]].act == ACT_UZ) {
+              on = true;
+              acc = csr_dot<GL, 8, R>(acc, J1P[j], J1P[j + 1], sub, J1C, J1V, [&](int c) { return __ldcg(a.b1 + c); });
+            }
+            acc = group_sum<GL>(acc);
+            if (on && sub == 0) sx1[j - s1_lo] = acc;
+          }
+        }
+        for (int t = t_lo; t < t_hi; ++t) {
+          const Tile T = tile_at(t);
+          if (ls[T.lk].act != ACT_UZ) continue;
+          const R* r = a.r + (size_t)ls[T.lk].rpar * nv;
+          const R* mrr = mr[ls[T.lk].rpar];
+          for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+            const R v = sell_dot<R>(
+                R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return __ldg(a.j0 + ei); },
+                [&](int col) { return ldm(r, mrr, col, own0, nown); });
+            if (mz) mz[sl * 32 + lane - own0] = v;
+            else a.z[sl * 32 + lane] = v;
+          }
         }
         __syncthreads();
-        // x3 = E^-1 b3 on the block's level-3 list (warp per row, shared memory)
-        for (int j = s3_lo + warp; j < s3_hi; j += kWarps) {
-          const int s = __ldg(a.s3_sys + j), k = s - sys0;
-          if (ls[k].act != ACT_UZ) continue;
-          const int D = __ldg(a.sys_D3 + s);
-          const float* E = sE + __ldg(a.s3_eoff + j);
-          const R* bb = sb3 + k * a.dmax;
-          R acc = R(0);
-          for (int d = lane; d < D; d += 32) acc += R(E[d]) * bb[d];
-          acc = warp_sum(acc);
-          if (lane == 0) sx3[j - s3_lo] = acc;
-        }
-        __syncthreads();
-        // x2 = J2 b2 + Pt2 x3 on the level-2 list (4 lanes per row)
+        // J2 b2 on the level-2 list (4 lanes per row, shared memory)
         {
           constexpr int GL = 4, NG = kSolveThreads / GL;
           const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
@@ -432,51 +667,75 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
             const int j = base + grp;
             R acc = R(0);
             bool on = false;
-            if (j < s2_hi && ls[__ldg(a.s2_sys + j) - sys0].act == ACT_UZ) {
-              on = true;
-              const int ja = __ldg(a.s2_jptr + j), jb = __ldg(a.s2_jptr + j + 1);
-#pragma unroll 4
-              for (int k = ja + sub; k < jb; k += GL) acc += __ldg(a.s2_jval + k) * __ldcg(a.b2 + __ldg(a.s2_jcol + k));
-              const int pa = __ldg(a.s2_pptr + j), pb = __ldg(a.s2_pptr + j + 1);
-              for (int k = pa + sub; k < pb; k += GL) acc += __ldg(a.s2_pval + k) * sx3[__ldg(a.s2_pcol + k)];
+            if (j < s2_hi) {
+              const LocalSys& L = ls[S2K[j]];
+              if (L.act == ACT_UZ) {
+                on = true;
+                const R* b2k = sb2 + L.b2off;
+                acc = csr_dot<GL, 8, R>(acc, J2P[j], J2P[j + 1], sub, J2C, J2V, [&](int c) { return b2k[c]; });
+              }
             }
             acc = group_sum<GL>(acc);
             if (on && sub == 0) sx2[j - s2_lo] = acc;
           }
         }
         __syncthreads();
-        // x1 = J1 b1 + Pt1 x2 on the level-1 list (4 lanes per row)
+        // x3 = E^-1 b3 on the level-3 list (4 lanes per entry, transposed rows)
         {
           constexpr int GL = 4, NG = kSolveThreads / GL;
+          const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+          for (int base = s3_lo; base < s3_hi; base += NG) {
+            const int j = base + grp;
+            R acc = R(0);
+            const int k = j < s3_hi ? S3K[j] : 0;
+            const bool on = j < s3_hi && ls[k].act == ACT_UZ;
+            if (on) {
+              const int D = ls[k].D3, str = S3S[j];
+              const float* E = sE + S3E[j];
+              const R* bb = sb3 + k * a.dmax;
+              for (int d = sub; d < D; d += GL) acc = fma_r(R(E[d * str]), bb[d], acc);
+            }
+            acc = group_sum<GL>(acc);
+            if (on && sub == 0) sx3[j - s3_lo] = acc;
+          }
+        }
+        __syncthreads();
+        // x2 += Pt2 x3, then x1 += Pt1 x2 (shared memory)
+        {
+          constexpr int GL = 4, NG = kSolveThreads / GL;
+          const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
+          for (int base = s2_lo; base < s2_hi; base += NG) {
+            const int j = base + grp;
+            R acc = R(0);
+            const bool on = j < s2_hi && ls[S2K[j]].act == ACT_UZ;
+            if (on) acc = csr_dot<GL, 8, R>(acc, P2P[j], P2P[j + 1], sub, P2C, P2V, [&](int c) { return sx3[c]; });
+            acc = group_sum<GL>(acc);
+            if (on && sub == 0) sx2[j - s2_lo] += acc;
+          }
+        }
+        __syncthreads();
+        {
+          constexpr int GL = 2, NG = kSolveThreads / GL;
           const int sub = threadIdx.x % GL, grp = threadIdx.x / GL;
           for (int base = s1_lo; base < s1_hi; base += NG) {
             const int j = base + grp;
             R acc = R(0);
-            bool on = false;
-            if (j < s1_hi && ls[__ldg(a.s1_sys + j) - sys0].act == ACT_UZ) {
-              on = true;
-              const int ja = __ldg(a.s1_jptr + j), jb = __ldg(a.s1_jptr + j + 1);
-#pragma unroll 4
-              for (int k = ja + sub; k < jb; k += GL) acc += __ldg(a.s1_jval + k) * __ldcg(a.b1 + __ldg(a.s1_jcol + k));
-              const int pa = __ldg(a.s1_pptr + j), pb = __ldg(a.s1_pptr + j + 1);
-              for (int k = pa + sub; k < pb; k += GL) acc += __ldg(a.s1_pval + k) * sx2[__ldg(a.s1_pcol + k)];
-            }
+            const bool on = j < s1_hi && ls[S1K[j]].act == ACT_UZ;
+            if (on) acc = csr_dot<GL, 8, R>(acc, P1P[j], P1P[j + 1], sub, P1C, P1V, [&](int c) { return sx2[c]; });
             acc = group_sum<GL>(acc);
-            if (on && sub == 0) sx1[j - s1_lo] = acc;
+            if (on && sub == 0) sx1[j - s1_lo] += acc;
           }
         }
       }
       __syncthreads();
     }
-    PFEM2_PROF(1);
     // ---- level-0 work on the own tiles
     for (int t = t_lo; t < t_hi; ++t) {
-      const Tile T = a.tiles[t];
+      const Tile T = tile_at(t);
       const int k = T.comp;
-      const int lk = T.sys - sys0;
-      const LocalSys& L = ls[lk];
+      const LocalSys& L = ls[T.lk];
       const int act = L.act;
-      if (act == ACT_NONE || act == ACT_D) continue;
+      if (act == ACT_NONE) continue;
       double v0 = 0.0, v1 = 0.0;
       const R* dinv = a.dinv[k];
       R* e = a.e + k * nv;
@@ -489,13 +748,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         const double* xk = a.x[k];
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
-          const int base = a.sl_ptr[sl], len = a.sl_len[sl];
-          double acc = 0.0;
-          for (int j = 0; j < len; ++j) {
-            const int ei = base + j * 32 + lane;
-            const int col = __ldg(a.sl_col + ei);
-            acc += A[ei] * (__ldcg(xk + col) + (double)__ldcg(e + col));
-          }
+          const double acc = sell_dot<double>(
+              0.0, SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
+              [&](int col) { return __ldcg(xk + col) + (double)ldm(e, me, col, own0, nown); });
           const double rr = a.b[k][row] - acc;
           r64[row] = rr;
           v0 += rr * rr;
@@ -503,11 +758,13 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
       } else if (act == ACT_OUT_B || act == ACT_OUT_DONE) {
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
-          a.x[k][row] += (double)e[row];
+          a.x[k][row] += (double)(me ? me[row - own0] : e[row]);
           e[row] = R(0);
+          if (me) me[row - own0] = R(0);
           if (act == ACT_OUT_B) {
             const R rr = R(r64[row]);
             r[row] = rr;
+            if (me) mr[L.rpar][row - own0] = rr;
             if (!MG) {
               const R zz = rr * dinv[row];
               z[row] = zz;
@@ -523,16 +780,17 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         const R* A = a.Ain[k];
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
-          const int base = a.sl_ptr[sl], len = a.sl_len[sl];
-          R acc = R(0);
-          for (int j = 0; j < len; ++j) {
-            const int ei = base + j * 32 + lane;
-            const int col = __ldg(a.sl_col + ei);
-            acc += A[ei] * fma_r(beta, __ldcg(po + col), __ldcg(z + col));
-          }
-          const R pp = fma_r(beta, po[row], z[row]);
+          const R* mpo = mp[L.par ^ 1];
+          const R acc = sell_dot<R>(
+              R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
+              [&](int col) { return fma_r(beta, ldm(po, mpo, col, own0, nown), ldm(z, mz, col, own0, nown)); });
+          const R pp = me ? fma_r(beta, mpo[row - own0], mz[row - own0]) : fma_r(beta, po[row], z[row]);
           pn[row] = pp;
           q[row] = acc;
+          if (me) {
+            mp[L.par][row - own0] = pp;
+            mq[row - own0] = acc;
+          }
           v0 += (double)pp * (double)acc;
         }
       } else if (act == ACT_B) {
@@ -541,8 +799,18 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         R* rn = MG ? a.r + (2 * k + (L.rpar ^ 1)) * nv : r;
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
-          e[row] += alpha * pn[row];
-          const R rr = fma_r(-alpha, q[row], r[row]);
+          R rr;
+          if (me) {
+            const int o = row - own0;
+            const R ee = me[o] + alpha * mp[L.par][o];
+            me[o] = ee;
+            e[row] = ee;
+            rr = fma_r(-alpha, mq[o], mr[L.rpar][o]);
+            mr[L.rpar ^ 1][o] = rr;
+          } else {
+            e[row] += alpha * pn[row];
+            rr = fma_r(-alpha, q[row], r[row]);
+          }
           rn[row] = rr;
           if (MG) {
             v0 += (double)rr * (double)rr;
@@ -554,23 +822,15 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
           }
         }
       } else if (MG && act == ACT_UZ) {
-        // z = J0 r + Pt0 x1
-        const R* J = a.j0;
+        // z = J0 r (first stage) + Pt0 x1
         for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
           const int row = sl * 32 + lane;
-          const int base = a.sl_ptr[sl], len = a.sl_len[sl];
-          R acc = R(0);
-          for (int j = 0; j < len; ++j) {
-            const int ei = base + j * 32 + lane;
-            acc += __ldg(J + ei) * __ldcg(r + __ldg(a.sl_col + ei));
-          }
-          const int pb = __ldg(a.p0_ptr + sl), pl = __ldg(a.p0_len + sl);
-          for (int j = 0; j < pl; ++j) {
-            const int ei = pb + j * 32 + lane;
-            acc += __ldg(a.p0_val + ei) * sx1[__ldg(a.p0_col + ei)];
-          }
+          const R acc = sell_dot<R>(
+              mz ? mz[row - own0] : z[row], P0C, P0P[sl], P0L[sl], lane, [&](int ei) { return P0V[ei]; },
+              [&](int col) { return sx1[col]; });
           z[row] = acc;
-          v0 += (double)__ldcg(r + row) * (double)acc;
+          if (mz) mz[row - own0] = acc;
+          v0 += (double)(mz ? mr[L.rpar][row - own0] : __ldcg(r + row)) * (double)acc;
         }
       }
       // deterministic block reduction into this phase's parity buffer
@@ -587,13 +847,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
           s0 += red[wv][0];
           s1 += red[wv][1];
         }
-        double* dst = a.part + ((size_t)(iter & 1) * a.ntiles + t) * 3;
+        double* dst = a.part + (size_t)(iter & 1) * a.ntiles * 2 + T.slot;
         dst[0] = s0;
-        dst[1] = s1;
+        dst[a.ntiles] = s1;
       }
       __syncthreads();
     }
-    PFEM2_PROF(3);
     // ---- bookkeeping
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
@@ -611,41 +870,57 @@ __global__ void __launch_bounds__(kSolveThreads) k_krylov(SolveArgs<R> a) {
         L.act = ACT_NONE;
       }
     }
-    PFEM2_PROF(3);
-    if (!grid_sync(a.gb, bar_gen, a.active, &stop)) return;
-    PFEM2_PROF(4);
+    unsigned long long t_arrive = 0;
+    if (prof) t_arrive = gtimer();
+    if (!grid_sync_ra(a.gb, bar_gen)) return;
+    if (prof) {
+      const unsigned long long tn = gtimer();
+      pacc[plabel][0] += 1;
+      pacc[plabel][1] += t_arrive - t_phase;
+      pacc[plabel][2] += tn - t_arrive;
+      t_phase = tn;
+    }
   }
   if (prof)
-    for (int k = 0; k < 6; ++k) atomicAdd(a.prof + k, tp[k]);
-#undef PFEM2_PROF
+    for (int k = 0; k < 8; ++k)
+      for (int j = 0; j < 3; ++j) atomicAdd(a.prof + ((size_t)blockIdx.x * 8 + k) * 3 + j, pacc[k][j]);
 }
 
 // ------------------------------------------------------------------ host
 struct KrylovWs {
   Tile* tiles[2];
-  int* sys_t0[2];
+  int* sys_slot0[2];
+  int* sys_owner[2];
   int* blk_t0[2];
+  int* blk_sys[2];
+  int* blk_sys_off[2];
+  int* blk_sl[2];
   int ntiles[2], nsys[2], grid[2];
+  int stage[2] = {0, 0};   // staged categories per phase
+  size_t smem[2] = {0, 0}; // dynamic shared memory per phase
   std::vector<Tile> h_tiles0;
   std::vector<int> h_sys_t0_0, h_blk_t0_0;
+  std::vector<int> h_blk_sl[2];
+  size_t l0_meta[2] = {0, 0}, l0_col[2] = {0, 0};  // max bytes per block of the level-0 categories
   // multigrid of the pressure phase (phase 0)
   bool mg = false;
   int nls0 = 1;
-  size_t smem_mg = 0;
-  int dmax = 1, s1max = 0, s2max = 0, s3max = 0;
+  int dmax = 1, s1max = 0, s2max = 0, s3max = 0, b2max = 0, o2max = 0, emax = 0;
   int n1 = 0, n2 = 0, n3 = 0;
-  int *toff[4] = {}, *lsys[4] = {};
-  int *r01_ptr = nullptr, *r01_col = nullptr, *r12_ptr = nullptr, *r12_col = nullptr, *r13_ptr = nullptr,
-      *r13_col = nullptr;
-  void *r01_val = nullptr, *r12_val = nullptr, *r13_val = nullptr, *j0 = nullptr;
+  std::string mg_info;                   // hierarchy summary for the profile
+  int *toff[4] = {}, *lk[3] = {};
+  int *r01_ptr = nullptr, *r01_col = nullptr, *r02_ptr = nullptr, *r02_col = nullptr;
+  void *r01_val = nullptr, *r02_val = nullptr, *j0 = nullptr;
+  int *c3_blk = nullptr, *c3_ptr = nullptr, *c3_col = nullptr, *c3_lk = nullptr, *g3_ptr = nullptr, *g3_row = nullptr;
+  void *c3_val = nullptr, *contrib = nullptr;
   int *p0_ptr = nullptr, *p0_len = nullptr, *p0_col = nullptr;
   void* p0_val = nullptr;
-  int *blk_s[3] = {}, *s_sys[3] = {}, *s_jptr[3] = {}, *s_jcol[3] = {}, *s_pptr[3] = {}, *s_pcol[3] = {};
+  int *blk_s[3] = {}, *s_lk[3] = {}, *s_jptr[3] = {}, *s_jcol[3] = {}, *s_pptr[3] = {}, *s_pcol[3] = {};
   void *s_jval[3] = {}, *s_pval[3] = {};
-  int *blk_s3 = nullptr, *s3_sys = nullptr, *s3_eoff = nullptr, *blk_e = nullptr;
+  int *blk_s3 = nullptr, *s3_lk = nullptr, *s3_eoff = nullptr, *s3_estr = nullptr, *blk_e = nullptr;
   float* s3_E = nullptr;
-  int *sys_D3 = nullptr, *sys_off3 = nullptr;
-  void *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
+  int *sys_D3 = nullptr, *sys_off3 = nullptr, *sys_n2 = nullptr, *sys_off2 = nullptr;
+  void *b1 = nullptr, *b2 = nullptr;
   void *e = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p = nullptr;
   double* r64 = nullptr;
   double* part = nullptr;
@@ -653,7 +928,7 @@ struct KrylovWs {
   int* out_it[3];
   double* out_res[3];
   int* out_outer[3];
-  unsigned long long* prof = nullptr;  // [3 solve kinds][6]
+  unsigned long long* prof[3] = {};     // per solve kind: [grid][8 actions][3]
   std::vector<void*> allocs;            // every device allocation of the workspace
 };
 
@@ -689,18 +964,16 @@ static pfem2_status ws_upload_r(KrylovWs* w, bool mixed, void** p, const std::ve
   return PFEM2_OK;
 }
 
-static int max_local_systems(const std::vector<Tile>& tiles, const std::vector<int>& bt0) {
-  int worst = 0;
-  for (size_t b = 0; b + 1 < bt0.size(); ++b)
-    if (bt0[b + 1] > bt0[b]) worst = std::max(worst, tiles[bt0[b + 1] - 1].sys - tiles[bt0[b]].sys + 1);
-  return worst;
-}
+static size_t al16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// shared-memory budget of the solver kernel (dynamic part)
+constexpr size_t kSmemBudget = 200 * 1024;
 
 template <typename R, bool MG>
 static int occupancy(size_t smem) {
   int occ = 0;
   // one process-wide upper bound, so contexts with different hierarchies coexist
-  if (MG) cudaFuncSetAttribute((const void*)k_krylov<R, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute((const void*)k_krylov<R, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_krylov<R, MG>, kSolveThreads, smem) != cudaSuccess) return 0;
   return occ;
 }
@@ -718,13 +991,12 @@ pfem2_status krylov_setup(Ctx& c) {
   c.kws = w;
   const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
-  const size_t rs = c.mixed ? sizeof(float) : sizeof(double);
   const int bps = std::max(1, c.solve_blocks_per_sm);
   int maxtiles = 0, maxsys = 0;
   for (int ph = 0; ph < 2; ++ph) {
     const int ncomp = ph == 0 ? 1 : dim;
+    const int nsys = ncomp * ni;
     std::vector<Tile> tiles;
-    std::vector<int> st0(ncomp * ni + 1, 0);
     if (ph == 0) {
       // pressure: tiles = the aggregation domains of the multigrid; about
       // one per block of the persistent grid (balanced work), at most dcap
@@ -735,29 +1007,31 @@ pfem2_status krylov_setup(Ctx& c) {
       long long tot_sl = 0;
       for (int i = 0; i < ni; ++i) tot_sl += c.inst[i].nv_pad / kSlice;
       for (int i = 0; i < ni; ++i) {
-        st0[i] = (int)tiles.size();
         const int sl0 = c.inst[i].v_off / kSlice, nsl = c.inst[i].nv_pad / kSlice;
         const long long share = ni == 1 ? std::max<long long>(1, (long long)nb * nsl / tot_sl) : (nsl + 7) / 8;
         int D = (int)std::min<long long>(std::min<long long>(share, dcap), nsl);
         const int sps = (nsl + D - 1) / D;
-        for (int a = 0; a < nsl; a += sps) tiles.push_back(Tile{i, 0, sl0 + a, sl0 + std::min(nsl, a + sps)});
+        for (int a = 0; a < nsl; a += sps) tiles.push_back(Tile{i, 0, sl0 + a, sl0 + std::min(nsl, a + sps), 0, 0});
       }
-      st0[ni] = (int)tiles.size();
     } else {
+      // velocity components: tiles ordered (instance, slice run, component)
+      // so that the slices of a block form one contiguous range
       const long long slices = (long long)c.nslices * ncomp;
       const long long target = 2LL * bps * c.num_sms;
       int ts = (int)std::max<long long>(8, (slices + target - 1) / target);
       if (c.tile_slices > 0) ts = c.tile_slices;
-      for (int k = 0; k < ncomp; ++k)
-        for (int i = 0; i < ni; ++i) {
-          const int sidx = k * ni + i;
-          st0[sidx] = (int)tiles.size();
-          const int sl0 = c.inst[i].v_off / kSlice, sl1 = (c.inst[i].v_off + c.inst[i].nv_pad) / kSlice;
-          for (int a = sl0; a < sl1; a += ts) tiles.push_back(Tile{sidx, k, a, std::min(sl1, a + ts)});
-        }
-      st0[ncomp * ni] = (int)tiles.size();
+      for (int i = 0; i < ni; ++i) {
+        const int sl0 = c.inst[i].v_off / kSlice, sl1 = (c.inst[i].v_off + c.inst[i].nv_pad) / kSlice;
+        for (int a = sl0; a < sl1; a += ts)
+          for (int k = 0; k < ncomp; ++k) tiles.push_back(Tile{k * ni + i, k, a, std::min(sl1, a + ts), 0, 0});
+      }
     }
     const int T = (int)tiles.size();
+    // partial slots: the tiles of a system, contiguous
+    std::vector<int> slot0(nsys + 1, 0), cnt(nsys, 0);
+    for (const Tile& t : tiles) slot0[t.sys + 1]++;
+    for (int s = 0; s < nsys; ++s) slot0[s + 1] += slot0[s];
+    std::vector<int> owner(nsys, -1);
     // the multigrid grid is sized before its shared memory is known (one
     // block per SM); krylov_setup_precond checks residency afterwards
     const int occ = ph == 0 ? 1 : (c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0));
@@ -766,27 +1040,81 @@ pfem2_status krylov_setup(Ctx& c) {
       return PFEM2_CUDA_ERROR;
     }
     const int G = std::min(T, std::min(occ, bps) * c.num_sms);
-    std::vector<int> bt0(G + 1);
+    std::vector<int> bt0(G + 1), bsys_off(1, 0), bsys, bsl(2 * G, 0);
     for (int b = 0; b <= G; ++b) bt0[b] = (int)((long long)T * b / G);
-    const int nls = max_local_systems(tiles, bt0);
-    if (nls > kMaxLocalSys) {
-      set_error("krylov: more than 16 systems would share one block (instances too small for the batch)");
-      return PFEM2_INVALID_ARG;
+    size_t meta = 0, col = 0;
+    for (int b = 0; b < G; ++b) {
+      std::vector<int> lst;
+      int s0 = 1 << 30, s1 = -1;
+      for (int t = bt0[b]; t < bt0[b + 1]; ++t) {
+        Tile& tl = tiles[t];
+        int k = (int)(std::find(lst.begin(), lst.end(), tl.sys) - lst.begin());
+        if (k == (int)lst.size()) lst.push_back(tl.sys);
+        tl.lk = k;
+        tl.slot = slot0[tl.sys] + cnt[tl.sys]++;
+        if (owner[tl.sys] < 0) owner[tl.sys] = b;
+        s0 = std::min(s0, tl.s0);
+        s1 = std::max(s1, tl.s1);
+      }
+      if ((int)lst.size() > kMaxLocalSys) {
+        set_error("krylov: more than 16 systems would share one block (instances too small for the batch)");
+        return PFEM2_INVALID_ARG;
+      }
+      if (ph == 0 && lst.size() > 1)
+        for (size_t k = 1; k < lst.size(); ++k)
+          if (lst[k] != lst[0] + (int)k) {
+            set_error("krylov: pressure systems of a block must be consecutive");
+            return PFEM2_INVALID_ARG;
+          }
+      bsys.insert(bsys.end(), lst.begin(), lst.end());
+      bsys_off.push_back((int)bsys.size());
+      if (s1 < s0) s0 = s1 = 0;
+      // the block's tiles are ordered so that their slices form one range
+      bsl[2 * b] = s0;
+      bsl[2 * b + 1] = s1;
+      meta = std::max(meta, al16(4 * (size_t)(s1 - s0 + 1)) + al16(4 * (size_t)(s1 - s0)));
+      col = std::max(col, al16(4 * (size_t)(c.h_sl_ptr[s1] - c.h_sl_ptr[s0])));
+      w->nls0 = ph == 0 ? std::max(w->nls0, (int)lst.size()) : w->nls0;
     }
+    w->l0_meta[ph] = meta;
+    w->l0_col[ph] = col;
     if (ph == 0) {
-      w->nls0 = nls;
       w->h_tiles0 = tiles;
-      w->h_sys_t0_0 = st0;
+      w->h_sys_t0_0 = slot0;
       w->h_blk_t0_0 = bt0;
     }
+    // level-0 staging of the velocity solves (the pressure phase decides
+    // once its multigrid data are known)
+    if (ph == 1) {
+      w->stage[1] = 0;
+      w->smem[1] = 0;
+      if (meta <= kSmemBudget) {
+        w->stage[1] |= ST_L0META;
+        w->smem[1] += meta;
+      }
+      if (w->smem[1] + col <= kSmemBudget) {
+        w->stage[1] |= ST_L0COL;
+        w->smem[1] += col;
+      }
+      const int occ2 = c.mixed ? occupancy<float, false>(w->smem[1]) : occupancy<double, false>(w->smem[1]);
+      if (occ2 * c.num_sms < G) {
+        w->stage[1] = 0;
+        w->smem[1] = 0;
+      }
+    }
+    w->h_blk_sl[ph] = bsl;
     w->ntiles[ph] = T;
-    w->nsys[ph] = (int)st0.size() - 1;
+    w->nsys[ph] = nsys;
     w->grid[ph] = G;
     PFEM2_TRY(ws_upload(w, &w->tiles[ph], tiles));
-    PFEM2_TRY(ws_upload(w, &w->sys_t0[ph], st0));
+    PFEM2_TRY(ws_upload(w, &w->sys_slot0[ph], slot0));
+    PFEM2_TRY(ws_upload(w, &w->sys_owner[ph], owner));
     PFEM2_TRY(ws_upload(w, &w->blk_t0[ph], bt0));
+    PFEM2_TRY(ws_upload(w, &w->blk_sys[ph], bsys));
+    PFEM2_TRY(ws_upload(w, &w->blk_sys_off[ph], bsys_off));
+    PFEM2_TRY(ws_upload(w, &w->blk_sl[ph], bsl));
     maxtiles = std::max(maxtiles, T);
-    maxsys = std::max(maxsys, w->nsys[ph]);
+    maxsys = std::max(maxsys, nsys);
   }
   if (c.mixed) {
     float *e, *r, *z, *q, *p;
@@ -805,15 +1133,22 @@ pfem2_status krylov_setup(Ctx& c) {
     PFEM2_TRY(ws_alloc(w, &p, 2 * nv * dim));
     w->e = e; w->r = r; w->z = z; w->q = q; w->p = p;
   }
-  (void)rs;
   PFEM2_TRY(ws_alloc(w, &w->r64, nv * dim));
-  PFEM2_TRY(ws_alloc(w, &w->part, 6 * (size_t)maxtiles));
+  PFEM2_TRY(ws_alloc(w, &w->part, 4 * (size_t)maxtiles));
   PFEM2_TRY(ws_alloc(w, &w->active, 1));
-  if (getenv("PFEM2_SOLVER_PROFILE")) PFEM2_TRY(ws_alloc(w, &w->prof, 18));
+  if (getenv("PFEM2_SOLVER_PROFILE"))
+    for (int k = 0; k < 3; ++k) PFEM2_TRY(ws_alloc(w, &w->prof[k], (size_t)w->grid[k == 1 ? 0 : 1] * 8 * 3));
   for (int k = 0; k < 3; ++k) {
     PFEM2_TRY(ws_alloc(w, &w->out_it[k], maxsys));
     PFEM2_TRY(ws_alloc(w, &w->out_res[k], maxsys));
     PFEM2_TRY(ws_alloc(w, &w->out_outer[k], maxsys));
+  }
+  // pressure phase without multigrid: level-0 staging only
+  w->stage[0] = 0;
+  w->smem[0] = 0;
+  if (w->l0_meta[0] + w->l0_col[0] <= kSmemBudget) {
+    w->stage[0] = ST_L0META | ST_L0COL;
+    w->smem[0] = w->l0_meta[0] + w->l0_col[0];
   }
   return PFEM2_OK;
 }
@@ -835,32 +1170,107 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   w->s1max = H.s1max;
   w->s2max = H.s2max;
   w->s3max = H.s3max;
-  w->smem_mg = rs * ((size_t)H.s1max + H.s2max + H.s3max + (size_t)w->nls0 * H.dmax) + sizeof(float) * H.emax;
-  if (w->smem_mg > 200 * 1024) {
+  w->b2max = H.b2max;
+  w->emax = H.emax;
+  // shared memory: multigrid vectors and coarse-inverse rows, then the
+  // static data staged per category while the budget lasts (maximum over
+  // blocks of each category; the kernel stages them in the same pieces)
+  for (int b = 0; b < w->grid[0]; ++b)
+    w->o2max = std::max(w->o2max, H.toff[2][w->h_blk_t0_0[b + 1]] - H.toff[2][w->h_blk_t0_0[b]]);
+  const size_t base = rs * ((size_t)H.s1max + H.s2max + H.s3max + (size_t)w->nls0 * H.dmax + H.b2max + w->o2max) +
+                      al16(sizeof(float) * H.emax);
+  size_t idx = 0, cols = 0, vals = 0;
+  {
+    const std::vector<int>& bt0 = w->h_blk_t0_0;
+    const std::vector<Tile>& tl = w->h_tiles0;
+    for (int b = 0; b < w->grid[0]; ++b) {
+      const int t_lo = bt0[b], t_hi = bt0[b + 1];
+      const int bs0 = w->h_blk_sl[0][2 * b], bs1 = w->h_blk_sl[0][2 * b + 1];
+      const int o1lo = H.toff[1][t_lo], o1hi = H.toff[1][t_hi], o2lo = H.toff[2][t_lo], o2hi = H.toff[2][t_hi];
+      const int s1lo = H.blk_s[1][b], s1hi = H.blk_s[1][b + 1], s2lo = H.blk_s[2][b], s2hi = H.blk_s[2][b + 1];
+      const int s3lo = H.blk_s3[b], s3hi = H.blk_s3[b + 1];
+      int r3lo = 0, r3hi = 0;
+      if (t_hi > t_lo) {
+        const int sf = tl[t_lo].sys, sl = tl[t_hi - 1].sys;
+        r3lo = H.sys_off3[sf];
+        r3hi = H.sys_off3[sl] + H.sys_D3[sl];
+      }
+      const int c3lo = H.c3_blk[b], c3hi = H.c3_blk[b + 1];
+      const size_t i4 = 4;
+      size_t bi = al16(i4 * (o1hi - o1lo)) + al16(i4 * (o1hi - o1lo + 1)) + al16(i4 * (o2hi - o2lo)) +
+                  al16(i4 * (o2hi - o2lo + 1)) + al16(i4 * (s1hi - s1lo)) + 2 * al16(i4 * (s1hi - s1lo + 1)) +
+                  al16(i4 * (s2hi - s2lo)) + 2 * al16(i4 * (s2hi - s2lo + 1)) + 3 * al16(i4 * (s3hi - s3lo)) +
+                  al16(i4 * (c3hi - c3lo)) + al16(i4 * (c3hi - c3lo + 1)) + al16(i4 * (r3hi - r3lo + 1)) +
+                  al16(i4 * (H.g3_ptr[r3hi] - H.g3_ptr[r3lo])) + al16(i4 * (bs1 - bs0 + 1)) + al16(i4 * (bs1 - bs0));
+      const size_t n01 = H.r01_ptr[o1hi] - H.r01_ptr[o1lo], n02 = H.r02_ptr[o2hi] - H.r02_ptr[o2lo];
+      const size_t nj1 = H.s_jptr[1][s1hi] - H.s_jptr[1][s1lo], np1 = H.s_pptr[1][s1hi] - H.s_pptr[1][s1lo];
+      const size_t nj2 = H.s_jptr[2][s2hi] - H.s_jptr[2][s2lo], np2 = H.s_pptr[2][s2hi] - H.s_pptr[2][s2lo];
+      const size_t n23 = H.c3_ptr[c3hi] - H.c3_ptr[c3lo], np0 = H.p0_ptr[bs1] - H.p0_ptr[bs0];
+      const size_t bc = al16(i4 * n01) + al16(i4 * n02) + al16(i4 * nj1) + al16(i4 * np1) + al16(i4 * nj2) +
+                        al16(i4 * np2) + al16(i4 * n23) + al16(i4 * np0);
+      const size_t bv = al16(rs * np1) + al16(rs * nj2) + al16(rs * np2) + al16(rs * n23) + al16(rs * np0);
+      idx = std::max(idx, bi);
+      cols = std::max(cols, bc);
+      vals = std::max(vals, bv);
+    }
+  }
+  size_t smem = base;
+  int stage = 0;
+  size_t mirror = 0;
+  for (int b = 0; b < w->grid[0]; ++b)
+    mirror = std::max(mirror, al16((size_t)7 * 32 * (w->h_blk_sl[0][2 * b + 1] - w->h_blk_sl[0][2 * b]) * rs));
+  const std::pair<int, size_t> cats[] = {{ST_L0META, w->l0_meta[0]}, {ST_MGIDX, idx}, {ST_MIRROR, mirror},
+                                         {ST_L0COL, w->l0_col[0]}, {ST_MGCOL, cols}, {ST_MGVAL, vals}};
+  for (const auto& cs : cats)
+    if (smem + cs.second <= kSmemBudget) {
+      stage |= cs.first;
+      smem += cs.second;
+    }
+  if (base > kSmemBudget) {
     set_error("krylov: the pressure multigrid's per-block data exceed shared memory");
     return PFEM2_INVALID_ARG;
   }
-  const int occ = c.mixed ? occupancy<float, true>(w->smem_mg) : occupancy<double, true>(w->smem_mg);
+  const int occ = c.mixed ? occupancy<float, true>(smem) : occupancy<double, true>(smem);
   if (occ * c.num_sms < w->grid[0]) {
     set_error("krylov: the multigrid solver grid cannot be resident");
     return PFEM2_CUDA_ERROR;
   }
+  w->stage[0] = stage;
+  w->smem[0] = smem;
+  {
+    char buf[512];
+    snprintf(buf, sizeof(buf),
+             "multigrid: dofs %d %d %d %d; per block max lists S1 %d S2 %d S3 %d; nnz R01 %zu R02 %zu C3 %zu "
+             "J1 %zu P1 %zu J2 %zu P2 %zu P0 %zu; staged 0x%x, %zu bytes of shared memory\n",
+             c.nv, H.n[1], H.n[2], H.n[3], H.s1max, H.s2max, H.s3max, H.r01_col.size(), H.r02_col.size(),
+             H.c3_col.size(), H.s_jcol[1].size(), H.s_pcol[1].size(), H.s_jcol[2].size(), H.s_pcol[2].size(),
+             H.p0_col.size(), stage, smem);
+    w->mg_info = buf;
+  }
   w->n1 = H.n[1];
   w->n2 = H.n[2];
   w->n3 = H.n[3];
-  for (int l = 1; l < kMgLevels; ++l) {
+  for (int l = 1; l <= 2; ++l) {
     PFEM2_TRY(ws_upload(w, &w->toff[l], H.toff[l]));
-    PFEM2_TRY(ws_upload(w, &w->lsys[l], H.lsys[l]));
+    PFEM2_TRY(ws_upload(w, &w->lk[l], H.lk[l]));
   }
   PFEM2_TRY(ws_upload(w, &w->r01_ptr, H.r01_ptr));
   PFEM2_TRY(ws_upload(w, &w->r01_col, H.r01_col));
   PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r01_val, H.r01_val));
-  PFEM2_TRY(ws_upload(w, &w->r12_ptr, H.r12_ptr));
-  PFEM2_TRY(ws_upload(w, &w->r12_col, H.r12_col));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r12_val, H.r12_val));
-  PFEM2_TRY(ws_upload(w, &w->r13_ptr, H.r13_ptr));
-  PFEM2_TRY(ws_upload(w, &w->r13_col, H.r13_col));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r13_val, H.r13_val));
+  PFEM2_TRY(ws_upload(w, &w->r02_ptr, H.r02_ptr));
+  PFEM2_TRY(ws_upload(w, &w->r02_col, H.r02_col));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r02_val, H.r02_val));
+  PFEM2_TRY(ws_upload(w, &w->c3_blk, H.c3_blk));
+  PFEM2_TRY(ws_upload(w, &w->c3_ptr, H.c3_ptr));
+  PFEM2_TRY(ws_upload(w, &w->c3_col, H.c3_col));
+  PFEM2_TRY(ws_upload(w, &w->c3_lk, H.c3_lk));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->c3_val, H.c3_val));
+  PFEM2_TRY(ws_upload(w, &w->g3_ptr, H.g3_ptr));
+  PFEM2_TRY(ws_upload(w, &w->g3_row, H.g3_row));
+  {
+    std::vector<double> zero(std::max<size_t>(1, H.c3_lk.size()), 0.0);
+    PFEM2_TRY(ws_upload_r(w, c.mixed, &w->contrib, zero));
+  }
   PFEM2_TRY(ws_upload_r(w, c.mixed, &w->j0, H.j0));
   PFEM2_TRY(ws_upload(w, &w->p0_ptr, H.p0_ptr));
   PFEM2_TRY(ws_upload(w, &w->p0_len, H.p0_len));
@@ -868,7 +1278,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   PFEM2_TRY(ws_upload_r(w, c.mixed, &w->p0_val, H.p0_val));
   for (int l = 1; l <= 2; ++l) {
     PFEM2_TRY(ws_upload(w, &w->blk_s[l], H.blk_s[l]));
-    PFEM2_TRY(ws_upload(w, &w->s_sys[l], H.s_sys[l]));
+    PFEM2_TRY(ws_upload(w, &w->s_lk[l], H.s_sys[l]));
     PFEM2_TRY(ws_upload(w, &w->s_jptr[l], H.s_jptr[l]));
     PFEM2_TRY(ws_upload(w, &w->s_jcol[l], H.s_jcol[l]));
     PFEM2_TRY(ws_upload_r(w, c.mixed, &w->s_jval[l], H.s_jval[l]));
@@ -877,24 +1287,25 @@ pfem2_status krylov_setup_precond(Ctx& c) {
     PFEM2_TRY(ws_upload_r(w, c.mixed, &w->s_pval[l], H.s_pval[l]));
   }
   PFEM2_TRY(ws_upload(w, &w->blk_s3, H.blk_s3));
-  PFEM2_TRY(ws_upload(w, &w->s3_sys, H.s3_sys));
+  PFEM2_TRY(ws_upload(w, &w->s3_lk, H.s3_sys));
   PFEM2_TRY(ws_upload(w, &w->s3_eoff, H.s3_eoff));
+  PFEM2_TRY(ws_upload(w, &w->s3_estr, H.s3_estr));
   PFEM2_TRY(ws_upload(w, &w->blk_e, H.blk_e));
   PFEM2_TRY(ws_upload(w, &w->s3_E, H.s3_E));
   PFEM2_TRY(ws_upload(w, &w->sys_D3, H.sys_D3));
   PFEM2_TRY(ws_upload(w, &w->sys_off3, H.sys_off3));
+  PFEM2_TRY(ws_upload(w, &w->sys_n2, H.sys_n2));
+  PFEM2_TRY(ws_upload(w, &w->sys_off2, H.sys_off2));
   if (c.mixed) {
-    float *b1, *b2, *b3;
+    float *b1, *b2;
     PFEM2_TRY(ws_alloc(w, &b1, H.n[1]));
     PFEM2_TRY(ws_alloc(w, &b2, H.n[2]));
-    PFEM2_TRY(ws_alloc(w, &b3, H.n[3]));
-    w->b1 = b1; w->b2 = b2; w->b3 = b3;
+    w->b1 = b1; w->b2 = b2;
   } else {
-    double *b1, *b2, *b3;
+    double *b1, *b2;
     PFEM2_TRY(ws_alloc(w, &b1, H.n[1]));
     PFEM2_TRY(ws_alloc(w, &b2, H.n[2]));
-    PFEM2_TRY(ws_alloc(w, &b3, H.n[3]));
-    w->b1 = b1; w->b2 = b2; w->b3 = b3;
+    w->b1 = b1; w->b2 = b2;
   }
   w->mg = true;
   return PFEM2_OK;
@@ -924,29 +1335,36 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.ntiles = w->ntiles[ph];
   a.nv = c.nv;
   a.tiles = w->tiles[ph];
-  a.sys_t0 = w->sys_t0[ph];
+  a.sys_slot0 = w->sys_slot0[ph];
+  a.sys_owner = w->sys_owner[ph];
   a.blk_t0 = w->blk_t0[ph];
+  a.blk_sys = w->blk_sys[ph];
+  a.blk_sys_off = w->blk_sys_off[ph];
+  a.blk_sl = w->blk_sl[ph];
+  a.stage = w->stage[ph];
   a.sl_ptr = c.sl_ptr;
   a.sl_len = c.sl_len;
   a.sl_col = c.sl_col;
   if (mg) {
-    a.toff1 = w->toff[1]; a.toff2 = w->toff[2]; a.toff3 = w->toff[3];
-    a.lsys1 = w->lsys[1]; a.lsys2 = w->lsys[2]; a.lsys3 = w->lsys[3];
+    a.toff1 = w->toff[1]; a.toff2 = w->toff[2];
+    a.lk1 = w->lk[1]; a.lk2 = w->lk[2];
     a.r01_ptr = w->r01_ptr; a.r01_col = w->r01_col; a.r01_val = (const R*)w->r01_val;
-    a.r12_ptr = w->r12_ptr; a.r12_col = w->r12_col; a.r12_val = (const R*)w->r12_val;
-    a.r13_ptr = w->r13_ptr; a.r13_col = w->r13_col; a.r13_val = (const R*)w->r13_val;
+    a.r02_ptr = w->r02_ptr; a.r02_col = w->r02_col; a.r02_val = (const R*)w->r02_val;
+    a.c3_blk = w->c3_blk; a.c3_ptr = w->c3_ptr; a.c3_col = w->c3_col; a.c3_lk = w->c3_lk;
+    a.c3_val = (const R*)w->c3_val; a.g3_ptr = w->g3_ptr; a.g3_row = w->g3_row; a.contrib = (R*)w->contrib;
     a.j0 = (const R*)w->j0;
     a.p0_ptr = w->p0_ptr; a.p0_len = w->p0_len; a.p0_col = w->p0_col; a.p0_val = (const R*)w->p0_val;
-    a.blk_s1 = w->blk_s[1]; a.s1_sys = w->s_sys[1]; a.s1_jptr = w->s_jptr[1]; a.s1_jcol = w->s_jcol[1];
+    a.blk_s1 = w->blk_s[1]; a.s1_lk = w->s_lk[1]; a.s1_jptr = w->s_jptr[1]; a.s1_jcol = w->s_jcol[1];
     a.s1_jval = (const R*)w->s_jval[1]; a.s1_pptr = w->s_pptr[1]; a.s1_pcol = w->s_pcol[1];
     a.s1_pval = (const R*)w->s_pval[1];
-    a.blk_s2 = w->blk_s[2]; a.s2_sys = w->s_sys[2]; a.s2_jptr = w->s_jptr[2]; a.s2_jcol = w->s_jcol[2];
+    a.blk_s2 = w->blk_s[2]; a.s2_lk = w->s_lk[2]; a.s2_jptr = w->s_jptr[2]; a.s2_jcol = w->s_jcol[2];
     a.s2_jval = (const R*)w->s_jval[2]; a.s2_pptr = w->s_pptr[2]; a.s2_pcol = w->s_pcol[2];
     a.s2_pval = (const R*)w->s_pval[2];
-    a.blk_s3 = w->blk_s3; a.s3_sys = w->s3_sys; a.s3_eoff = w->s3_eoff; a.blk_e = w->blk_e; a.s3_E = w->s3_E;
-    a.sys_D3 = w->sys_D3; a.sys_off3 = w->sys_off3;
-    a.dmax = w->dmax; a.s1max = w->s1max; a.s2max = w->s2max; a.s3max = w->s3max;
-    a.b1 = (R*)w->b1; a.b2 = (R*)w->b2; a.b3 = (R*)w->b3;
+    a.blk_s3 = w->blk_s3; a.s3_lk = w->s3_lk; a.s3_eoff = w->s3_eoff; a.s3_estr = w->s3_estr; a.blk_e = w->blk_e; a.s3_E = w->s3_E;
+    a.sys_D3 = w->sys_D3; a.sys_off3 = w->sys_off3; a.sys_n2 = w->sys_n2; a.sys_off2 = w->sys_off2;
+    a.dmax = w->dmax; a.s1max = w->s1max; a.s2max = w->s2max; a.s3max = w->s3max; a.b2max = w->b2max;
+    a.emax = w->emax; a.o2max = w->o2max;
+    a.b1 = (R*)w->b1; a.b2 = (R*)w->b2;
   }
   for (int k = 0; k < 3; ++k) {
     const int kk = k < ncomp ? k : 0;
@@ -983,20 +1401,20 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.eta = c.mixed ? c.refine_eta : 0.0;
   int mx = 0;
   for (auto& in : c.inst) mx = std::max(mx, in.cs.max_iter > 0 ? in.cs.max_iter : 10000);
-  a.iter_cap = (mg ? 4 : 2) * mx + 256;
+  a.iter_cap = (mg ? 3 : 2) * mx + 256;
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
-  a.prof = w->prof ? w->prof + 6 * which : nullptr;
+  a.prof = w->prof[which];
   k_init_solve<<<1, 32, 0, c.stream>>>(a.nsys, w->active, c.barrier, c.d_err);
   c.launches++;
   void* args[] = {&a};
   if (mg)
     PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, true>, dim3(w->grid[ph]), dim3(kSolveThreads),
-                                           args, w->smem_mg, c.stream));
+                                           args, w->smem[ph], c.stream));
   else
     PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, false>, dim3(w->grid[ph]), dim3(kSolveThreads),
-                                           args, 0, c.stream));
+                                           args, w->smem[ph], c.stream));
   c.launches++;
   return PFEM2_OK;
 }
@@ -1040,10 +1458,40 @@ static pfem2_status read_stats_phase(Ctx& c, int which) {
 }
 
 // sub-phase times of block 0 (ns): sums, coarse, decisions, work, barrier, loop
-void krylov_profile(Ctx& c, unsigned long long* out18) {
+std::string krylov_profile(Ctx& c) {
+  // per solve kind and action: phases (block 0), mean and max over blocks
+  // of the work per phase, and block 0's mean barrier wait, in microseconds
   KrylovWs* w = (KrylovWs*)c.kws;
-  if (!w || !w->prof) return;
-  cudaMemcpy(out18, w->prof, sizeof(unsigned long long) * 18, cudaMemcpyDeviceToHost);
+  std::string out;
+  if (!w) return out;
+  static const char* kind[3] = {"prediction", "pressure", "correction"};
+  static const char* act[8] = {"-", "out_a", "out_b", "out_done", "a", "b", "uz", "-"};
+  out += w->mg_info;
+  for (int k = 0; k < 3; ++k) {
+    if (!w->prof[k]) continue;
+    const int G = w->grid[k == 1 ? 0 : 1];
+    std::vector<unsigned long long> h((size_t)G * 24);
+    if (cudaMemcpy(h.data(), w->prof[k], sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return out;
+    char buf[160];
+    out += kind[k];
+    for (int a = 0; a < 8; ++a) {
+      const unsigned long long n0 = h[a * 3];
+      if (n0 == 0) continue;
+      double mean = 0.0, mx = 0.0;
+      for (int b = 0; b < G; ++b) {
+        const double n = (double)h[((size_t)b * 8 + a) * 3];
+        const double wk = n > 0 ? h[((size_t)b * 8 + a) * 3 + 1] / n : 0.0;
+        mean += wk / G;
+        mx = std::max(mx, wk);
+      }
+      snprintf(buf, sizeof(buf), " %s:%llu:%.2f:%.2f:%.2f", act[a], n0, mean * 1e-3, mx * 1e-3,
+               (double)h[a * 3 + 2] / n0 * 1e-3);
+      out += buf;
+    }
+    out += "\n";
+  }
+  return out;
 }
 
 pfem2_status krylov_read_stats(Ctx& c) {

@@ -181,8 +181,16 @@ pfem2_status launch_correct(Ctx& c) {
 // sub-step the particle is located like the reference does: current cell
 // first, then the patch of the "closest" vertex in alignment order; a
 // particle found nowhere is deleted (newcell = -1).
+// resident 256-thread blocks per SM the advection kernel is compiled for:
+// it is latency-bound, so the FP32 2D variant trades its few extra
+// registers for four blocks (32 warps) per SM
+template <int DIM, typename R>
+struct AdvectMinBlocks {
+  static constexpr int value = DIM == 2 ? (sizeof(R) == 4 ? 4 : 2) : (sizeof(R) == 4 ? 2 : 1);
+};
+
 template <int DIM, typename R, bool FUSE>
-__global__ void __launch_bounds__(256) k_advect(
+__global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect(
     const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
     const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
     const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
