@@ -96,6 +96,7 @@ template <typename R> struct SolveArgs {
   const R* Ain[3];
   const R* dinv[3];
   int stage;              // ST_* categories staged in shared memory
+  int ntl_max, items_max; // per block: tiles, (tile, slice) work items
   // multigrid (pressure phase), layout of MgHost
   const int *toff1, *toff2;             // [ntiles+1]
   const int *lk1, *lk2;                 // local system index of each level-1/2 dof (in its owner block)
@@ -290,8 +291,37 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
   const int nls = s_nls;
   auto tile_at = [&](int t) -> Tile { return tiles_staged ? stile[t - t_lo] : a.tiles[t]; };
 
+  // ---- level-0 work items: (tile, slice) pairs in tile order; item0[t] is
+  // the first item of local tile t. Every item's partial sums go to spart,
+  // then each tile sums its items in order (deterministic).
+  double* spart = reinterpret_cast<double*>(dyn_smem);
+  int* item0 = reinterpret_cast<int*>(dyn_smem + al16_dev((size_t)a.items_max * 2 * sizeof(double)));
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int t = 0; t < ntl; ++t) {
+      item0[t] = n;
+      const Tile T = tile_at(t_lo + t);
+      n += T.s1 - T.s0;
+    }
+    item0[ntl] = n;
+  }
+  __syncthreads();
+  const int nitems = item0[ntl];
+  // local tile of item `it` (binary search; tiles are few)
+  auto item_tile = [&](int it) -> int {
+    int lo = 0, hi = ntl - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (item0[mid] <= it) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  };
+  unsigned char* dyn_rest =
+      dyn_smem + al16_dev((size_t)a.items_max * 2 * sizeof(double)) + al16_dev((size_t)(a.ntl_max + 1) * sizeof(int));
+
   // ---- shared memory: multigrid vectors, then the staged static data
-  R* sx1 = reinterpret_cast<R*>(dyn_smem);
+  R* sx1 = reinterpret_cast<R*>(dyn_rest);
   R* sx2 = sx1 + a.s1max;
   R* sx3 = sx2 + a.s2max;
   R* sb3 = sx3 + a.s3max;
@@ -377,10 +407,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
   }
 
   // ---- init: Dirichlet values preset in x, e = 0, p = 0
-  for (int t = t_lo; t < t_hi; ++t) {
-    const Tile T = tile_at(t);
+  for (int it = warp; it < nitems; it += kWarps) {
+    const int tl = item_tile(it);
+    const Tile T = tile_at(t_lo + tl);
     const int k = T.comp;
-    for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+    {
+      const int sl = T.s0 + (it - item0[tl]);
       const int row = sl * 32 + lane;
       if (a.isd[k][row]) a.x[k][row] = a.g[k] ? a.g[k][row] : 0.0;
       a.e[k * nv + row] = R(0);
@@ -645,12 +677,14 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
             if (on && sub == 0) sx1[j - s1_lo] = acc;
           }
         }
-        for (int t = t_lo; t < t_hi; ++t) {
-          const Tile T = tile_at(t);
+        for (int it = warp; it < nitems; it += kWarps) {
+          const int tl = item_tile(it);
+          const Tile T = tile_at(t_lo + tl);
           if (ls[T.lk].act != ACT_UZ) continue;
           const R* r = a.r + (size_t)ls[T.lk].rpar * nv;
           const R* mrr = mr[ls[T.lk].rpar];
-          for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+          {
+            const int sl = T.s0 + (it - item0[tl]);
             const R v = sell_dot<R>(
                 R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return __ldg(a.j0 + ei); },
                 [&](int col) { return ldm(r, mrr, col, own0, nown); });
@@ -729,9 +763,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
       }
       __syncthreads();
     }
-    // ---- level-0 work on the own tiles
-    for (int t = t_lo; t < t_hi; ++t) {
-      const Tile T = tile_at(t);
+    // ---- level-0 work on the own (tile, slice) items, a warp per item
+    for (int it = warp; it < nitems; it += kWarps) {
+      const int tl = item_tile(it);
+      const Tile T = tile_at(t_lo + tl);
+      const int sl = T.s0 + (it - item0[tl]);
       const int k = T.comp;
       const LocalSys& L = ls[T.lk];
       const int act = L.act;
@@ -746,7 +782,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
       if (act == ACT_OUT_A) {
         const double* A = a.A64[k];
         const double* xk = a.x[k];
-        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+        {
           const int row = sl * 32 + lane;
           const double acc = sell_dot<double>(
               0.0, SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
@@ -756,7 +792,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
           v0 += rr * rr;
         }
       } else if (act == ACT_OUT_B || act == ACT_OUT_DONE) {
-        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+        {
           const int row = sl * 32 + lane;
           a.x[k][row] += (double)(me ? me[row - own0] : e[row]);
           e[row] = R(0);
@@ -778,7 +814,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
         R* pn = a.p + (2 * k + L.par) * nv;
         const R* po = a.p + (2 * k + (L.par ^ 1)) * nv;
         const R* A = a.Ain[k];
-        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+        {
           const int row = sl * 32 + lane;
           const R* mpo = mp[L.par ^ 1];
           const R acc = sell_dot<R>(
@@ -797,7 +833,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
         const R alpha = R(L.alpha);
         const R* pn = a.p + (2 * k + L.par) * nv;
         R* rn = MG ? a.r + (2 * k + (L.rpar ^ 1)) * nv : r;
-        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+        {
           const int row = sl * 32 + lane;
           R rr;
           if (me) {
@@ -823,7 +859,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
         }
       } else if (MG && act == ACT_UZ) {
         // z = J0 r (first stage) + Pt0 x1
-        for (int sl = T.s0 + warp; sl < T.s1; sl += kWarps) {
+        {
           const int row = sl * 32 + lane;
           const R acc = sell_dot<R>(
               mz ? mz[row - own0] : z[row], P0C, P0P[sl], P0L[sl], lane, [&](int ei) { return P0V[ei]; },
@@ -833,25 +869,27 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
           v0 += (double)(mz ? mr[L.rpar][row - own0] : __ldcg(r + row)) * (double)acc;
         }
       }
-      // deterministic block reduction into this phase's parity buffer
+      // the item's partial sums (warp order is fixed: deterministic)
       v0 = warp_sum(v0);
       v1 = warp_sum(v1);
       if (lane == 0) {
-        red[warp][0] = v0;
-        red[warp][1] = v1;
+        spart[2 * it] = v0;
+        spart[2 * it + 1] = v1;
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double s0 = 0.0, s1 = 0.0;
-        for (int wv = 0; wv < kWarps; ++wv) {
-          s0 += red[wv][0];
-          s1 += red[wv][1];
-        }
-        double* dst = a.part + (size_t)(iter & 1) * a.ntiles * 2 + T.slot;
-        dst[0] = s0;
-        dst[a.ntiles] = s1;
+    }
+    __syncthreads();
+    // per tile: its items' partials in order, into this phase's parity buffer
+    for (int tl = threadIdx.x; tl < ntl; tl += kSolveThreads) {
+      const Tile T = tile_at(t_lo + tl);
+      if (ls[T.lk].act == ACT_NONE) continue;
+      double s0 = 0.0, s1 = 0.0;
+      for (int it = item0[tl]; it < item0[tl + 1]; ++it) {
+        s0 += spart[2 * it];
+        s1 += spart[2 * it + 1];
       }
-      __syncthreads();
+      double* dst = a.part + (size_t)(iter & 1) * a.ntiles * 2 + T.slot;
+      dst[0] = s0;
+      dst[a.ntiles] = s1;
     }
     // ---- bookkeeping
     if (threadIdx.x == 0) {
@@ -902,6 +940,8 @@ struct KrylovWs {
   std::vector<int> h_sys_t0_0, h_blk_t0_0;
   std::vector<int> h_blk_sl[2];
   size_t l0_meta[2] = {0, 0}, l0_col[2] = {0, 0};  // max bytes per block of the level-0 categories
+  int ntl_max[2] = {0, 0}, items_max[2] = {0, 0};  // per block: tiles, (tile, slice) items
+  size_t items_bytes[2] = {0, 0};                  // shared memory of the item partials and offsets
   // multigrid of the pressure phase (phase 0)
   bool mg = false;
   int nls0 = 1;
@@ -1041,11 +1081,31 @@ pfem2_status krylov_setup(Ctx& c) {
     }
     const int G = std::min(T, std::min(occ, bps) * c.num_sms);
     std::vector<int> bt0(G + 1), bsys_off(1, 0), bsys, bsl(2 * G, 0);
-    for (int b = 0; b <= G; ++b) bt0[b] = (int)((long long)T * b / G);
+    // split the tile sequence where the running slice count crosses
+    // b / G of the total (a tile goes to the block holding its midpoint):
+    // blocks get equal work when tiles differ in size
+    {
+      std::vector<long long> pre(T + 1, 0);
+      for (int u = 0; u < T; ++u) pre[u + 1] = pre[u] + (tiles[u].s1 - tiles[u].s0);
+      bt0[0] = 0;
+      int t = 0;
+      for (int b = 1; b < G; ++b) {
+        const long long goal = pre[T] * b / G;
+        while (t < T && 2 * pre[t] + (pre[t + 1] - pre[t]) < 2 * goal) ++t;
+        // every block keeps at least one tile and leaves one for each later block
+        t = std::min(std::max(t, bt0[b - 1] + 1), T - (G - b));
+        bt0[b] = t;
+      }
+      bt0[G] = T;
+    }
     size_t meta = 0, col = 0;
+    int ntl_max = 0, items_max = 0;
     for (int b = 0; b < G; ++b) {
       std::vector<int> lst;
-      int s0 = 1 << 30, s1 = -1;
+      int s0 = 1 << 30, s1 = -1, items = 0;
+      ntl_max = std::max(ntl_max, bt0[b + 1] - bt0[b]);
+      for (int t = bt0[b]; t < bt0[b + 1]; ++t) items += tiles[t].s1 - tiles[t].s0;
+      items_max = std::max(items_max, items);
       for (int t = bt0[b]; t < bt0[b + 1]; ++t) {
         Tile& tl = tiles[t];
         int k = (int)(std::find(lst.begin(), lst.end(), tl.sys) - lst.begin());
@@ -1078,6 +1138,9 @@ pfem2_status krylov_setup(Ctx& c) {
     }
     w->l0_meta[ph] = meta;
     w->l0_col[ph] = col;
+    w->ntl_max[ph] = ntl_max;
+    w->items_max[ph] = items_max;
+    w->items_bytes[ph] = al16(sizeof(double) * 2 * (size_t)items_max) + al16(sizeof(int) * (size_t)(ntl_max + 1));
     if (ph == 0) {
       w->h_tiles0 = tiles;
       w->h_sys_t0_0 = slot0;
@@ -1087,8 +1150,8 @@ pfem2_status krylov_setup(Ctx& c) {
     // once its multigrid data are known)
     if (ph == 1) {
       w->stage[1] = 0;
-      w->smem[1] = 0;
-      if (meta <= kSmemBudget) {
+      w->smem[1] = w->items_bytes[1];
+      if (w->smem[1] + meta <= kSmemBudget) {
         w->stage[1] |= ST_L0META;
         w->smem[1] += meta;
       }
@@ -1099,7 +1162,7 @@ pfem2_status krylov_setup(Ctx& c) {
       const int occ2 = c.mixed ? occupancy<float, false>(w->smem[1]) : occupancy<double, false>(w->smem[1]);
       if (occ2 * c.num_sms < G) {
         w->stage[1] = 0;
-        w->smem[1] = 0;
+        w->smem[1] = w->items_bytes[1];
       }
     }
     w->h_blk_sl[ph] = bsl;
@@ -1145,10 +1208,10 @@ pfem2_status krylov_setup(Ctx& c) {
   }
   // pressure phase without multigrid: level-0 staging only
   w->stage[0] = 0;
-  w->smem[0] = 0;
-  if (w->l0_meta[0] + w->l0_col[0] <= kSmemBudget) {
+  w->smem[0] = w->items_bytes[0];
+  if (w->smem[0] + w->l0_meta[0] + w->l0_col[0] <= kSmemBudget) {
     w->stage[0] = ST_L0META | ST_L0COL;
-    w->smem[0] = w->l0_meta[0] + w->l0_col[0];
+    w->smem[0] += w->l0_meta[0] + w->l0_col[0];
   }
   return PFEM2_OK;
 }
@@ -1177,7 +1240,8 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   // blocks of each category; the kernel stages them in the same pieces)
   for (int b = 0; b < w->grid[0]; ++b)
     w->o2max = std::max(w->o2max, H.toff[2][w->h_blk_t0_0[b + 1]] - H.toff[2][w->h_blk_t0_0[b]]);
-  const size_t base = rs * ((size_t)H.s1max + H.s2max + H.s3max + (size_t)w->nls0 * H.dmax + H.b2max + w->o2max) +
+  const size_t base = w->items_bytes[0] +
+                      rs * ((size_t)H.s1max + H.s2max + H.s3max + (size_t)w->nls0 * H.dmax + H.b2max + w->o2max) +
                       al16(sizeof(float) * H.emax);
   size_t idx = 0, cols = 0, vals = 0;
   {
@@ -1342,6 +1406,8 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.blk_sys_off = w->blk_sys_off[ph];
   a.blk_sl = w->blk_sl[ph];
   a.stage = w->stage[ph];
+  a.ntl_max = w->ntl_max[ph];
+  a.items_max = w->items_max[ph];
   a.sl_ptr = c.sl_ptr;
   a.sl_len = c.sl_len;
   a.sl_col = c.sl_col;

@@ -61,6 +61,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--stages", action="store_true", help="also report the per-stage device time per step")
     args = ap.parse_args()
     import torch
 
@@ -69,6 +70,9 @@ def main():
     for _ in range(args.warmup):
         s.step()
     s.synchronize()
+    if args.stages:
+        s.enable_stage_timing(True)
+        s.stage_times(reset=True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
@@ -76,8 +80,12 @@ def main():
     e1.record(stream)
     e1.synchronize()
     st = s.stats(False)
-    print(json.dumps({"case": args.case, "steps": args.steps, "ms_per_step": e0.elapsed_time(e1) / args.steps,
-                      "n_particles": st["n_particles"], "iters": st["iters"], "status": st["status"]}))
+    out = {"case": args.case, "steps": args.steps, "ms_per_step": e0.elapsed_time(e1) / args.steps,
+           "n_particles": st["n_particles"], "iters": st["iters"], "status": st["status"]}
+    if args.stages:
+        from pfem2_b200.solver import STAGE_NAMES
+        out["stage_ms_per_step"] = dict(zip(STAGE_NAMES, (t / args.steps for t in s.stage_times())))
+    print(json.dumps(out))
     s.close()
 
 
