@@ -238,7 +238,7 @@ __device__ __forceinline__ SV<T> maybe_stage(bool on, unsigned char*& cur, const
 }
 
 template <typename R, bool MG>
-__global__ void __launch_bounds__(kSolveThreads, 1) k_krylov(SolveArgs<R> a) {
+__global__ void __launch_bounds__(kSolveThreads, MG ? 1 : 2) k_krylov(SolveArgs<R> a) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ LocalSys ls[kMaxLocalSys];
   __shared__ Tile stile[kMaxBlockTiles];
@@ -1057,7 +1057,7 @@ pfem2_status krylov_setup(Ctx& c) {
       // velocity components: tiles ordered (instance, slice run, component)
       // so that the slices of a block form one contiguous range
       const long long slices = (long long)c.nslices * ncomp;
-      const long long target = 2LL * bps * c.num_sms;
+      const long long target = 4LL * bps * c.num_sms;
       int ts = (int)std::max<long long>(8, (slices + target - 1) / target);
       if (c.tile_slices > 0) ts = c.tile_slices;
       for (int i = 0; i < ni; ++i) {
@@ -1074,12 +1074,13 @@ pfem2_status krylov_setup(Ctx& c) {
     std::vector<int> owner(nsys, -1);
     // the multigrid grid is sized before its shared memory is known (one
     // block per SM); krylov_setup_precond checks residency afterwards
-    const int occ = ph == 0 ? 1 : (c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0));
+    // the multigrid kernel runs one block per SM, the Jacobi kernel two
+    const int occ = ph == 0 ? 1 : std::min(2, c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0));
     if (occ < 1) {
       set_error("krylov: the solver kernel cannot be resident");
       return PFEM2_CUDA_ERROR;
     }
-    const int G = std::min(T, std::min(occ, bps) * c.num_sms);
+    const int G = std::min(T, (ph == 0 ? std::min(occ, bps) : occ) * c.num_sms);
     std::vector<int> bt0(G + 1), bsys_off(1, 0), bsys, bsl(2 * G, 0);
     // split the tile sequence where the running slice count crosses
     // b / G of the total (a tile goes to the block holding its midpoint):
