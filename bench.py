@@ -128,14 +128,18 @@ def peaks():
 
 
 def pressure_solve_bytes(s, iters, outer):
-    """Algorithmic bytes of the pressure solves, per the model in DESIGN.md:
-    inner CG iteration (FP32 inner type for the mixed path):
-        SELL SpMV  nnz*(val+col) + n*(x + y)
-        vectors    p = z + beta p (3 n), e += alpha p (3 n), r -= alpha q (3 n), z = D^-1 r (3 n)
+    """Algorithmic bytes of the pressure solves, per the model in DESIGN.md.
+    One inner CG iteration (inner type R: FP32 for the mixed path) reads
+    every operator once with its column indices and streams the vectors:
+        A   q = A (z + beta p)         nnz*(R+4) + n*(z, p in; p, q out)
+        B   e, r' update; b1, b2       n*(e, p, q, r in; e, r' out) + (R01 + R02 + C3)*(R+4) + (n1 + n2)*R
+        UZ  z = J0 r + Pt0 x1, coarse  nnz*(R+4) + P0*(R+4) + (J1+P1+J2+P2)*(R+4) + n*(r in, z out) + n2*R
     FP64 refinement sweep: nnz*(8+4) + n*(x64 + e + b + r64) bytes."""
     info = s.sizes()
     n, nnz, rb = info["rows"], info["nnz"], info["real_bytes"]
-    inner = nnz * (rb + 4) + n * 2 * rb + 12 * n * rb
+    mg = s.solver_sizes()
+    ops = mg["r01"] + mg["r02"] + mg["c3"] + mg["p0"] + mg["j1"] + mg["p1"] + mg["j2"] + mg["p2"]
+    inner = 2 * nnz * (rb + 4) + ops * (rb + 4) + 12 * n * rb + (mg["n1"] + 2 * mg["n2"]) * rb
     outerb = nnz * 12 + n * (8 + rb + 8 + 8)
     return iters * inner + outer * outerb
 
@@ -214,6 +218,10 @@ def run_ours(args, rank, world, local):
     for _ in range(args.steps):
         s.step_and_read(fields, loads, out)
     e2e_s = time.perf_counter() - t0
+    if world > 1:
+        from pfem2_b200.sharding import max_over_ranks
+
+        e2e_s = max_over_ranks(e2e_s)
     e2e = {"value": args.steps / e2e_s * world, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
            "d2h_bytes_per_step": int(out.nbytes + loads.nbytes)}
 
@@ -253,7 +261,7 @@ def run_ours(args, rank, world, local):
     stress = stress_leg(args, local, flush) if args.stress_n > 0 else None
     ensemble = None
     if args.ensemble_n > 0:
-        ensemble = ensemble_leg(args, local, flush, fp64["timesteps_per_s"] if fp64 else None)
+        ensemble = ensemble_leg(args, rank, world, local, flush, fp64["timesteps_per_s"] if fp64 else None)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -372,16 +380,21 @@ def stress_leg(args, local, flush):
     return out
 
 
-def ensemble_leg(args, local, flush, fp64_single):
+def ensemble_leg(args, rank, world, local, flush, fp64_single):
     """many independent channel instances of uneven size in one batch:
-    every stage is one launch for all of them"""
+    every stage is one launch for all of them; with N ranks every rank runs
+    its longest-processing-time share of the instances (no collective but
+    the max-over-ranks time)"""
     import torch
 
     from pfem2_b200 import _abi as A
-    from pfem2_b200 import cases
+    from pfem2_b200 import cases, sharding
     from pfem2_b200.solver import Solver
 
-    specs = cases.ensemble(n=args.ensemble_n)
+    all_specs = cases.ensemble(n=args.ensemble_n)
+    specs = all_specs
+    if world > 1:
+        _, specs = sharding.shard(all_specs, rank, world)
     s = Solver(specs, precision=A.PREC_MIXED, device=local, use_graph=True)
     s.seed_particles(specs[0].q, 2, 0.0)
     stream = torch.cuda.ExternalStream(s.stream(), device=local)
@@ -389,13 +402,16 @@ def ensemble_leg(args, local, flush, fp64_single):
         s.step()
     s.synchronize()
     ms = timed_steps(s, stream, flush, args.extra_steps)
+    if world > 1:
+        ms = sharding.max_over_ranks(ms)
     st = s.stats()
-    cells = sum(sp.mesh.n_cells for sp in specs)
-    inst_steps = len(specs) * args.extra_steps / (ms / 1e3)
+    cells = sum(sp.mesh.n_cells for sp in all_specs)
+    inst_steps = len(all_specs) * args.extra_steps / (ms / 1e3)
     out = {
         "workload": f"{len(specs)} channel-with-disk instances, cells log-uniform 5k-60k, Re log-uniform 20-200, "
                     f"r uniform 0.05-0.15 (seed 2), 5x5 particles/cell, one batch",
-        "instances": len(specs), "cells": cells, "particles": st["n_particles"],
+        "instances": len(all_specs), "cells": cells, "particles_rank0": st["n_particles"],
+        "sharding": f"lpt over {world} ranks" if world > 1 else "one batch",
         "ms_per_batch_step": ms / args.extra_steps, "instance_timesteps_per_s": inst_steps,
         "cell_updates_per_s": cells * args.extra_steps / (ms / 1e3),
         "max_pressure_cg_iters": st["iters"][3],

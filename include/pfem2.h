@@ -237,6 +237,14 @@ pfem2_status pfem2_stage_times(pfem2_ctx* ctx, double* ms, int32_t reset);
 pfem2_status pfem2_enable_stage_timing(pfem2_ctx* ctx, int32_t on);
 /* The CUDA stream (cudaStream_t) all work of the context is issued on. */
 pfem2_status pfem2_get_stream(pfem2_ctx* ctx, void** stream);
+/* Sizes of the pressure solver's multigrid hierarchy after pfem2_setup
+ * (diagnostics; no counterpart in the reference). out[0..3]: unknowns per
+ * level; out[4..11]: stored nonzeros of R01, R02, the b3 contribution rows,
+ * the level-0 prolongator, and the J1, Pt1, J2, Pt2 rows of all blocks'
+ * coarse lists (halo rows counted once per block that evaluates them).
+ * All zero without a hierarchy. */
+#define PFEM2_N_SOLVER_SIZES 12
+pfem2_status pfem2_solver_sizes(pfem2_ctx* ctx, int64_t* out);
 const char* pfem2_last_error(void);
 int32_t pfem2_abi_version(void);
 

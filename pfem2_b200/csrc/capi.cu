@@ -957,6 +957,18 @@ pfem2_status pfem2_stage_times(pfem2_ctx* x, double* ms, int32_t reset) {
   return PFEM2_OK;
 }
 
+pfem2_status pfem2_solver_sizes(pfem2_ctx* x, int64_t* out) {
+  CTX_CHECK(x);
+  if (!out) {
+    set_error("pfem2_solver_sizes: null output");
+    return PFEM2_INVALID_ARG;
+  }
+  long long v[PFEM2_N_SOLVER_SIZES];
+  krylov_sizes(x->c, v);
+  for (int k = 0; k < PFEM2_N_SOLVER_SIZES; ++k) out[k] = v[k];
+  return PFEM2_OK;
+}
+
 pfem2_status pfem2_enable_stage_timing(pfem2_ctx* x, int32_t on) {
   CTX_CHECK(x);
   PFEM2_TRY(collect_stage_times(x->c));

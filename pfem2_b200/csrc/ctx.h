@@ -216,5 +216,6 @@ void krylov_free(Ctx& c);
 pfem2_status krylov_solve(Ctx& c, int which);
 pfem2_status krylov_read_stats(Ctx& c);
 std::string krylov_profile(Ctx& c);
+void krylov_sizes(Ctx& c, long long* out12);
 
 }  // namespace pfem2

@@ -948,6 +948,7 @@ struct KrylovWs {
   int dmax = 1, s1max = 0, s2max = 0, s3max = 0, b2max = 0, o2max = 0, emax = 0;
   int n1 = 0, n2 = 0, n3 = 0;
   std::string mg_info;                   // hierarchy summary for the profile
+  long long mg_sizes[12] = {};           // see pfem2_solver_sizes
   int *toff[4] = {}, *lk[3] = {};
   int *r01_ptr = nullptr, *r01_col = nullptr, *r02_ptr = nullptr, *r02_col = nullptr;
   void *r01_val = nullptr, *r02_val = nullptr, *j0 = nullptr;
@@ -1311,6 +1312,11 @@ pfem2_status krylov_setup_precond(Ctx& c) {
              H.c3_col.size(), H.s_jcol[1].size(), H.s_pcol[1].size(), H.s_jcol[2].size(), H.s_pcol[2].size(),
              H.p0_col.size(), stage, smem);
     w->mg_info = buf;
+    const long long sz[12] = {c.nv, H.n[1], H.n[2], H.n[3], (long long)H.r01_col.size(), (long long)H.r02_col.size(),
+                              (long long)H.c3_col.size(), (long long)H.p0_col.size(), (long long)H.s_jcol[1].size(),
+                              (long long)H.s_pcol[1].size(), (long long)H.s_jcol[2].size(),
+                              (long long)H.s_pcol[2].size()};
+    for (int k = 0; k < 12; ++k) w->mg_sizes[k] = sz[k];
   }
   w->n1 = H.n[1];
   w->n2 = H.n[2];
@@ -1525,6 +1531,11 @@ static pfem2_status read_stats_phase(Ctx& c, int which) {
 }
 
 // sub-phase times of block 0 (ns): sums, coarse, decisions, work, barrier, loop
+void krylov_sizes(Ctx& c, long long* out12) {
+  KrylovWs* w = (KrylovWs*)c.kws;
+  for (int k = 0; k < 12; ++k) out12[k] = (w && w->mg) ? w->mg_sizes[k] : 0;
+}
+
 std::string krylov_profile(Ctx& c) {
   // per solve kind and action: phases (block 0), mean and max over blocks
   // of the work per phase, and block 0's mean barrier wait, in microseconds

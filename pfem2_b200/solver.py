@@ -36,7 +36,7 @@ EXPORTS = [
     "pfem2_step", "pfem2_step_and_read", "pfem2_get_field", "pfem2_set_field", "pfem2_particle_count",
     "pfem2_get_particles", "pfem2_set_particles", "pfem2_get_stats", "pfem2_get_time", "pfem2_synchronize",
     "pfem2_launch_count", "pfem2_stage_times", "pfem2_enable_stage_timing", "pfem2_get_stream",
-    "pfem2_last_error", "pfem2_abi_version", "pfem2_project_noalloc",
+    "pfem2_last_error", "pfem2_abi_version", "pfem2_project_noalloc", "pfem2_solver_sizes",
 ]
 
 
@@ -72,6 +72,7 @@ def load_library(path=LIB_PATH):
         "pfem2_synchronize": [vp],
         "pfem2_launch_count": [vp, C.POINTER(C.c_int64)],
         "pfem2_stage_times": [vp, dp, C.c_int32],
+        "pfem2_solver_sizes": [vp, C.POINTER(C.c_int64)],
         "pfem2_enable_stage_timing": [vp, C.c_int32],
         "pfem2_get_stream": [vp, C.POINTER(vp)],
     }
@@ -256,6 +257,13 @@ class Solver:
 
     def enable_stage_timing(self, on=True):
         self._check(self.L.pfem2_enable_stage_timing(self.h, 1 if on else 0))
+
+    def solver_sizes(self):
+        """Multigrid hierarchy of the pressure solve (pfem2_solver_sizes)."""
+        out = (C.c_int64 * 12)()
+        self._check(self.L.pfem2_solver_sizes(self.h, out))
+        keys = ("n0", "n1", "n2", "n3", "r01", "r02", "c3", "p0", "j1", "p1", "j2", "p2")
+        return dict(zip(keys, (int(v) for v in out)))
 
     def stage_times(self, reset=False):
         ms = np.zeros(N_STAGES)
