@@ -416,6 +416,14 @@ static pfem2_status alloc_particles(Ctx& c, size_t seeded) {
   }
   if (c.newcell) cudaFree(c.newcell);
   PFEM2_CUDA(cudaMalloc(&c.newcell, sizeof(int) * cap));
+  // the advection queue: one region per warp of the fast kernel's grid
+  c.adv_grid = grid_for(c, (long long)cap, 256, 8);
+  if (c.adv_queue) cudaFree(c.adv_queue);
+  if (c.adv_wcount) cudaFree(c.adv_wcount);
+  if (c.adv_qstep) cudaFree(c.adv_qstep);
+  PFEM2_CUDA(cudaMalloc(&c.adv_qstep, (cap + (size_t)c.adv_grid * 257)));
+  PFEM2_CUDA(cudaMalloc(&c.adv_queue, sizeof(int) * (cap + (size_t)c.adv_grid * 257)));
+  PFEM2_CUDA(cudaMalloc(&c.adv_wcount, sizeof(int) * (size_t)c.adv_grid * 8));
   c.pcap = (int)cap;
   c.graph_valid = false;
   return PFEM2_OK;
@@ -573,6 +581,7 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   cudaDeviceProp prop;
   PFEM2_CUDA(cudaGetDeviceProperties(&prop, c.device));
   c.num_sms = prop.multiProcessorCount;
+  if (const char* v = getenv("PFEM2_ADVECT_SPLIT_MIN")) c.adv_split_min = atoll(v);
   PFEM2_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   for (int k = 0; k < 8; ++k) PFEM2_CUDA(cudaEventCreate(&c.ev[k]));
   *out = x;
@@ -599,7 +608,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.d_inst,
                   c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.cell_count, c.d_np, c.d_counters,
-                  c.far_keys, c.scan_tmp, c.barrier, c.d_err, c.newcell};
+                  c.far_keys, c.scan_tmp, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c.mixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);

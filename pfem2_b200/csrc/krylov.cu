@@ -242,7 +242,6 @@ __global__ void __launch_bounds__(kSolveThreads, MG ? 1 : 2) k_krylov(SolveArgs<
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ LocalSys ls[kMaxLocalSys];
   __shared__ Tile stile[kMaxBlockTiles];
-  __shared__ double red[kWarps][2];
   __shared__ int s_nls;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t nv = (size_t)a.nv;

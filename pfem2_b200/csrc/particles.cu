@@ -189,8 +189,245 @@ struct AdvectMinBlocks {
   static constexpr int value = DIM == 2 ? (sizeof(R) == 4 ? 4 : 2) : (sizeof(R) == 4 ? 2 : 1);
 };
 
+constexpr int kAdvWarps = 8;  // warps per block of the advection kernels (256 threads)
+
+constexpr int kAdvLeft = -2;  // advect_steps<.., false>: the particle left its cell
+
+// Sub-steps s0 .. S-1 of the S forward-Euler sub-steps of one particle with
+// the Q1-interpolated mesh velocity (move_particles,
+// TurekBenchmark/pfem2particle.cpp:813-856), starting in cell c0 at
+// reference coordinates x (updated). After a sub-step
+// the point is first tried in the current cell; if it left, FULL runs the
+// reference's search (sort_particles_into_subdomains_and_cells: the vertex
+// of the old cell best aligned with the velocity, then that vertex's cells
+// ordered by alignment with the directions to their centres, :276-507) and
+// returns the new cell, or -1 when no cell of the patch contains the point
+// (the particle is deleted); without FULL it returns kAdvLeft at the first
+// sub-step that leaves the cell, with x still at the start of that
+// sub-step and its index in s_left. Otherwise it returns the cell.
+template <int DIM, typename R, bool FULL>
+__device__ __forceinline__ int advect_steps(int c0, R* x, R dts, int s0, int& s_left, int S,
+                                            const CellGeo<DIM, R>* __restrict__ geo,
+                                            const int* __restrict__ cv, const R* __restrict__ Vr, int nv,
+                                            const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
+                                            const R* __restrict__ v2c_dir) {
+  constexpr int NV = Dims<DIM>::NV;
+  int c = c0;
+  // vertex ids and velocities of the current cell, reloaded only when the
+  // particle changes cell
+  int gvx[NV];
+  R vv[NV][DIM], N[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
+  CellGeo<DIM, R> G = geo[c];
+  LocalCell<DIM, R> L;
+  double x0[DIM];
+  geo_to_local<DIM, R>(G, L, x0);
+  for (int s = s0; s < S; ++s) {
+    shape_values<DIM, R>(x, N);
+    R uf[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) uf[d] = R(0);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * vv[v][d];
+    }
+    R xo[DIM], xn[DIM], x2[DIM];
+    local_map<DIM, R>(L, x, xo);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xn[d] = xo[d] + uf[d] * dts;
+    if (geo_inverse<DIM, R>(G, L, xn, x2) && inside_unit<DIM, R>(x2)) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) x[d] = x2[d];
+      continue;
+    }
+    if (!FULL) {
+      s_left = s;
+      return kAdvLeft;
+    }
+    // closest vertex of the old cell seen along the velocity
+    R un = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) un += uf[d] * uf[d];
+    un = sqrt(un);
+    R best = R(0);
+    int bv = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      R t[DIM], tn = R(0), dot = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        t[d] = L.D[v][d] - xo[d];
+        tn += t[d] * t[d];
+      }
+      tn = sqrt(tn);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) dot += (uf[d] / un) * (t[d] / tn);
+      if (v == 0) best = dot;
+      else if (dot > best) { best = dot; bv = v; }
+    }
+    const int gv = gvx[bv];
+    R vp[DIM], vpn = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      vp[d] = xn[d] - L.D[bv][d];
+      vpn += vp[d] * vp[d];
+    }
+    vpn = sqrt(vpn);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vp[d] /= vpn;
+    const int k0 = __ldg(v2c_ptr + gv);
+    int nk = __ldg(v2c_ptr + gv + 1) - k0;
+    if (nk > kMaxPatch) nk = kMaxPatch;
+    R key[kMaxPatch];
+    int perm[kMaxPatch];
+    for (int i = 0; i < nk; ++i) {
+      R sdot = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) sdot += __ldg(v2c_dir + (size_t)(k0 + i) * DIM + d) * vp[d];
+      key[i] = sdot;
+      // stable insertion by descending alignment (std::sort is an
+      // insertion sort, hence stable, for patches of <= 16 cells)
+      int j = i - 1;
+      while (j >= 0 && sdot > key[perm[j]]) {
+        perm[j + 1] = perm[j];
+        --j;
+      }
+      perm[j + 1] = i;
+    }
+    bool found = false;
+    for (int i = 0; i < nk && !found; ++i) {
+      const int cc = __ldg(v2c_cell + k0 + perm[i]);
+      const CellGeo<DIM, R> Gc = geo[cc];
+      LocalCell<DIM, R> Lc;
+      double xc[DIM];
+      geo_to_local<DIM, R>(Gc, Lc, xc);
+      R t[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) t[d] = xn[d] + R(x0[d] - xc[d]);
+      if (geo_inverse<DIM, R>(Gc, Lc, t, x2) && inside_unit<DIM, R>(x2)) {
+        found = true;
+        c = cc;
+        G = Gc;
+        L = Lc;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          x0[d] = xc[d];
+          x[d] = x2[d];
+        }
+      }
+    }
+    if (!found) return -1;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
+  }
+  return c;
+}
+
+// Advection, first kernel: the particles of a contiguous chunk per block;
+// with FUSE the FLIP correction (correct_particles_velocities) is applied
+// and stored for every particle. A particle that stays in its cell for all
+// sub-steps is finished here; one that leaves is appended, unfinished, to
+// its warp's region of the queue with the sub-step it left in, its
+// reference coordinates stored as they were before that sub-step (the second
+// kernel resumes there with the same arithmetic, so the result does not
+// depend on this split). Warps whose lanes all stay never run the patch
+// search.
 template <int DIM, typename R, bool FUSE>
 __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect(
+    const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
+    const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
+    const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
+    const int* __restrict__ cell_inst, int* __restrict__ queue, unsigned char* __restrict__ qstep,
+    int* __restrict__ wcount) {
+  constexpr int NV = Dims<DIM>::NV;
+  const int n = min(*d_np, (int)cap);
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int wcap = ((chunk + 255) / 256) * 32;  // particles one warp handles at most
+  const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* wq = queue + ((size_t)blockIdx.x * kAdvWarps + warp) * wcap;
+  int nq = 0;
+  for (int base = lo; base < hi; base += 256) {
+    const int p = base + threadIdx.x;
+    bool leave = false;
+    int s_left = 0;
+    if (p < hi) {
+      const int c0 = cell[p];
+      R x[DIM], up[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        x[d] = xi[d * cap + p];
+        up[d] = u[d * cap + p];
+      }
+      if (FUSE) {
+        R N[NV];
+        shape_values<DIM, R>(x, N);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const int g = __ldg(cv + (size_t)c0 * NV + v);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) u[d * cap + p] = up[d];
+      }
+      const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
+      const int c = advect_steps<DIM, R, false>(c0, x, dts, 0, s_left, S, geo, cv, Vr, nv, nullptr, nullptr, nullptr);
+      if (c == kAdvLeft) {
+        leave = true;
+      } else {
+        newcell[p] = c;
+      }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
+    }
+    const unsigned m = __ballot_sync(PFEM2_FULL_MASK, leave);
+    if (leave) {
+      const size_t q = (size_t)(wq - queue) + nq + __popc(m & lanemask_lt());
+      queue[q] = p;
+      qstep[q] = (unsigned char)s_left;
+    }
+    nq += __popc(m);
+  }
+  if (lane == 0) wcount[(size_t)blockIdx.x * kAdvWarps + warp] = nq;
+}
+
+// deletion count and far movers of one advected particle (c: its new cell,
+// -1 when deleted)
+__device__ __forceinline__ void advect_record(int p, int c0, int c, const int* __restrict__ ring_ptr,
+                                              const int* __restrict__ ring_cell,
+                                              unsigned long long* __restrict__ far_keys, int far_cap,
+                                              int* __restrict__ counters) {
+  if (c < 0) {
+    atomicAdd(counters + CNT_DELETED, 1);
+  } else if (c != c0) {
+    // a particle that left the 1-ring of its old cell goes to the far list
+    bool near = false;
+    for (int rr = __ldg(ring_ptr + c0); rr < __ldg(ring_ptr + c0 + 1); ++rr)
+      if (__ldg(ring_cell + rr) == c) { near = true; break; }
+    if (!near) {
+      int slot = atomicAdd(counters + CNT_FAR, 1);
+      if (slot < far_cap) far_keys[slot] = ((unsigned long long)(unsigned)c << 32) | (unsigned)p;
+      else atomicExch(counters + CNT_FAR_OVERFLOW, 1);
+    }
+  }
+}
+
+// Advection in one kernel (used below a particle count where the two-kernel
+// split does not pay for its second pass): correction, every sub-step with
+// the full point location. Same arithmetic as the split.
+template <int DIM, typename R, bool FUSE>
+__global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_one(
     const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
     const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
     const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
@@ -201,159 +438,71 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect(
   const int n = min(*d_np, (int)cap);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const int c0 = cell[p];
-    int c = c0;
-    R x[DIM], up[DIM], N[NV];
+    R x[DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      x[d] = xi[d * cap + p];
-      up[d] = u[d * cap + p];
-    }
-    // vertex ids and velocities of the current cell, reloaded only when the
-    // particle changes cell (most stay for all S sub-steps)
-    int gvx[NV];
-    R vv[NV][DIM];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
+    for (int d = 0; d < DIM; ++d) x[d] = xi[d * cap + p];
     if (FUSE) {
+      R N[NV], up[DIM];
       shape_values<DIM, R>(x, N);
 #pragma unroll
+      for (int d = 0; d < DIM; ++d) up[d] = u[d * cap + p];
+#pragma unroll
       for (int v = 0; v < NV; ++v) {
+        const int g = __ldg(cv + (size_t)c0 * NV + v);
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + gvx[v]);
+        for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
       }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) u[d * cap + p] = up[d];
     }
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
     const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
-    CellGeo<DIM, R> G = geo[c];
-    LocalCell<DIM, R> L;
-    double x0[DIM];
-    geo_to_local<DIM, R>(G, L, x0);
-    (void)S;
-    bool alive = true;
-    for (int s = 0; s < S && alive; ++s) {
-      shape_values<DIM, R>(x, N);
-      R uf[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) uf[d] = R(0);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * vv[v][d];
-      }
-      R xo[DIM], xn[DIM], x2[DIM];
-      local_map<DIM, R>(L, x, xo);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) xn[d] = xo[d] + uf[d] * dts;
-      if (geo_inverse<DIM, R>(G, L, xn, x2) && inside_unit<DIM, R>(x2)) {
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) x[d] = x2[d];
-        continue;
-      }
-      // closest vertex of the old cell seen along the velocity
-      R un = R(0);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) un += uf[d] * uf[d];
-      un = sqrt(un);
-      R best = R(0);
-      int bv = 0;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        R t[DIM], tn = R(0), dot = R(0);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-          t[d] = L.D[v][d] - xo[d];
-          tn += t[d] * t[d];
-        }
-        tn = sqrt(tn);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) dot += (uf[d] / un) * (t[d] / tn);
-        if (v == 0) best = dot;
-        else if (dot > best) { best = dot; bv = v; }
-      }
-      const int gv = gvx[bv];
-      R vp[DIM], vpn = R(0);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        vp[d] = xn[d] - L.D[bv][d];
-        vpn += vp[d] * vp[d];
-      }
-      vpn = sqrt(vpn);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) vp[d] /= vpn;
-      const int k0 = __ldg(v2c_ptr + gv);
-      int nk = __ldg(v2c_ptr + gv + 1) - k0;
-      if (nk > kMaxPatch) nk = kMaxPatch;
-      R key[kMaxPatch];
-      int perm[kMaxPatch];
-      for (int i = 0; i < nk; ++i) {
-        R sdot = R(0);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) sdot += __ldg(v2c_dir + (size_t)(k0 + i) * DIM + d) * vp[d];
-        key[i] = sdot;
-        // stable insertion by descending alignment (std::sort is an
-        // insertion sort, hence stable, for patches of <= 16 cells)
-        int j = i - 1;
-        while (j >= 0 && sdot > key[perm[j]]) {
-          perm[j + 1] = perm[j];
-          --j;
-        }
-        perm[j + 1] = i;
-      }
-      bool found = false;
-      for (int i = 0; i < nk && !found; ++i) {
-        const int cc = __ldg(v2c_cell + k0 + perm[i]);
-        const CellGeo<DIM, R> Gc = geo[cc];
-        LocalCell<DIM, R> Lc;
-        double xc[DIM];
-        geo_to_local<DIM, R>(Gc, Lc, xc);
-        R t[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) t[d] = xn[d] + R(x0[d] - xc[d]);
-        if (geo_inverse<DIM, R>(Gc, Lc, t, x2) && inside_unit<DIM, R>(x2)) {
-          found = true;
-          c = cc;
-          G = Gc;
-          L = Lc;
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            x0[d] = xc[d];
-            x[d] = x2[d];
-          }
-        }
-      }
-      if (!found) {
-        alive = false;
-      } else {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
-#pragma unroll
-        for (int v = 0; v < NV; ++v)
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
-      }
-    }
-    if (!alive) {
-      c = -1;
-      atomicAdd(counters + CNT_DELETED, 1);
-    } else if (c != c0) {
-      // a particle that left the 1-ring of its old cell goes to the far list
-      bool near = false;
-      for (int r = __ldg(ring_ptr + c0); r < __ldg(ring_ptr + c0 + 1); ++r)
-        if (__ldg(ring_cell + r) == c) { near = true; break; }
-      if (!near) {
-        int slot = atomicAdd(counters + CNT_FAR, 1);
-        if (slot < far_cap) far_keys[slot] = ((unsigned long long)(unsigned)c << 32) | (unsigned)p;
-        else atomicExch(counters + CNT_FAR_OVERFLOW, 1);
-      }
-    }
+    int s_left = 0;
+    int c = advect_steps<DIM, R, true>(c0, x, dts, 0, s_left, S, geo, cv, Vr, nv, v2c_ptr, v2c_cell, v2c_dir);
+    if (c < 0) c = -1;
+    advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters);
     newcell[p] = c;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      xi[d * cap + p] = x[d];
-      u[d * cap + p] = up[d];
+    for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
+  }
+}
+
+// Advection, second kernel: the queued particles (a warp per queue region),
+// sub-steps redone from their start with the full point location; deletion
+// count and far movers (left the 1-ring of the old cell) recorded here.
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_advect_left(
+    const int* __restrict__ cell, R* __restrict__ xi, int* __restrict__ newcell, size_t cap,
+    const int* __restrict__ d_np, int fast_grid, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
+    const R* __restrict__ Vr, int nv, int S, const DevInst* __restrict__ inst, const int* __restrict__ cell_inst,
+    const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell, const R* __restrict__ v2c_dir,
+    const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell, const int* __restrict__ queue,
+    const unsigned char* __restrict__ qstep, const int* __restrict__ wcount,
+    unsigned long long* __restrict__ far_keys, int far_cap,
+    int* __restrict__ counters) {
+  const int n = min(*d_np, (int)cap);
+  const int chunk = (n + fast_grid - 1) / fast_grid;
+  const int wcap = ((chunk + 255) / 256) * 32;
+  const int lane = threadIdx.x & 31;
+  const int nreg = fast_grid * kAdvWarps;
+  for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < nreg;
+       r += (int)((gridDim.x * blockDim.x) >> 5)) {
+    const int cnt = wcount[r];
+    for (int i = lane; i < cnt; i += 32) {
+      const size_t q = (size_t)r * wcap + i;
+      const int p = queue[q];
+      const int s0 = qstep[q];
+      const int c0 = cell[p];
+      R x[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) x[d] = xi[d * cap + p];
+      const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
+      int s_left = 0;
+      int c = advect_steps<DIM, R, true>(c0, x, dts, s0, s_left, S, geo, cv, Vr, nv, v2c_ptr, v2c_cell, v2c_dir);
+      if (c < 0) c = -1;
+      advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters);
+      newcell[p] = c;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
     }
   }
 }
@@ -386,21 +535,39 @@ __global__ void k_far_sort(unsigned long long* keys, const int* __restrict__ cou
 template <int DIM, typename R>
 static pfem2_status advect_impl(Ctx& c, bool fuse) {
   int b = c.cur;
-  int grid = grid_for(c, c.pcap, 256, 8);
+  const int G = c.adv_grid;
   int S = c.cfg.movement_steps;
+  if ((long long)c.pcap < c.adv_split_min) {
+    const int grid = grid_for(c, c.pcap, 256, 8);
+    if (fuse)
+      k_advect_one<DIM, R, true><<<grid, 256, 0, c.stream>>>(
+          c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
+          (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
+          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+    else
+      k_advect_one<DIM, R, false><<<grid, 256, 0, c.stream>>>(
+          c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
+          (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
+          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+    c.launches++;
+  } else {
   if (fuse)
-    k_advect<DIM, R, true><<<grid, 256, 0, c.stream>>>(
+    k_advect<DIM, R, true><<<G, 256, 0, c.stream>>>(
         c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
-        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr,
-        (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
-        c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
+        c.adv_queue, c.adv_qstep, c.adv_wcount);
   else
-    k_advect<DIM, R, false><<<grid, 256, 0, c.stream>>>(
+    k_advect<DIM, R, false><<<G, 256, 0, c.stream>>>(
         c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
-        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr,
-        (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
-        c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
+        c.adv_queue, c.adv_qstep, c.adv_wcount);
   c.launches++;
+  k_advect_left<DIM, R><<<G, 256, 0, c.stream>>>(
+      c.pcell[b], (R*)c.pxi[b], c.newcell, (size_t)c.pcap, c.d_np + b, G, (const CellGeo<DIM, R>*)c.cell_geo, c.cv,
+      (const R*)c.Vr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
+      c.ring_cell, c.adv_queue, c.adv_qstep, c.adv_wcount, c.far_keys, c.far_cap, c.d_counters);
+  c.launches++;
+  }
   k_far_sort<<<1, 1024, sizeof(unsigned long long) * c.far_cap, c.stream>>>(c.far_keys, c.d_counters, c.far_cap);
   c.launches++;
   return PFEM2_OK;

@@ -291,3 +291,25 @@ def test_ensemble_batch_runs():
     for i in range(len(specs)):
         v = s.field(A.FIELD_VX, i)
         assert np.all(np.isfinite(v)) and np.abs(v).max() < 10.0
+
+
+def test_advect_split_equals_one_kernel(monkeypatch):
+    """the two-kernel advection (used from ~8M particle slots: fast sub-steps,
+    then the particles that left their cell) equals the one-kernel form bit
+    for bit; forced here on a small case through PFEM2_ADVECT_SPLIT_MIN"""
+    sp = spec_2d(dt=0.02)
+    outs = []
+    for split_min in ("0", str(1 << 40)):
+        monkeypatch.setenv("PFEM2_ADVECT_SPLIT_MIN", split_min)
+        s = Solver(sp, precision=A.PREC_MIXED)
+        s.seed_particles(sp.q, seed=0, jitter=0.1)
+        for _ in range(3):
+            s.step()
+        outs.append((s.particles(), [s.field(f) for f in (A.FIELD_VX, A.FIELD_P)], s.stats()["deleted"]))
+        s.close()
+    (pa, fa, da), (pb, fb, db) = outs
+    for x, y in zip(pa, pb):
+        assert np.array_equal(x, y)
+    for x, y in zip(fa, fb):
+        assert np.array_equal(x, y)
+    assert da == db
