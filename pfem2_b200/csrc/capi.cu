@@ -379,13 +379,11 @@ static pfem2_status do_setup(Ctx& c) {
     c.partial = p;
   }
   for (int b = 0; b < 2; ++b) PFEM2_TRY(dalloc(&c.cell_start[b], nc + 1));
-  PFEM2_TRY(dalloc(&c.cell_count, nc));
+  PFEM2_TRY(dalloc(&c.rebin_tiles, (size_t)nc / 8 + 2));
   PFEM2_TRY(dalloc(&c.d_np, 2));
   PFEM2_TRY(dalloc(&c.d_counters, CNT_N));
   c.far_cap = c.cfg.far_mover_capacity > 0 ? std::min(c.cfg.far_mover_capacity, 4096) : 4096;
   PFEM2_TRY(dalloc(&c.far_keys, c.far_cap));
-  c.scan_tmp_n = (nc + 4095) / 4096 + 1;
-  PFEM2_TRY(dalloc(&c.scan_tmp, c.scan_tmp_n));
   PFEM2_TRY(dalloc(&c.barrier, 2));
   PFEM2_TRY(dalloc(&c.d_err, 1));
   c.list_cap = c.cfg.particles_per_cell_max > 0 ? c.cfg.particles_per_cell_max : (dim == 2 ? 512 : 1024);
@@ -444,6 +442,10 @@ static pfem2_status check_counters(Ctx& c, bool sync) {
   if (cnt[CNT_LIST_OVERFLOW]) {
     set_error("rebin: more incoming particles than the per-cell capacity (particles_per_cell_max)");
     return PFEM2_PARTICLE_OVERFLOW;
+  }
+  if (cnt[CNT_SCAN_TIMEOUT]) {
+    set_error("rebin: a wait of the single-pass scan timed out");
+    return PFEM2_TIMEOUT;
   }
   if (cnt[CNT_FAR_OVERFLOW]) {
     set_error("advect: more far movers than far_mover_capacity");
@@ -607,8 +609,8 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   // device memory is released with the context's allocations; free the big ones
   void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.d_inst,
-                  c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.cell_count, c.d_np, c.d_counters,
-                  c.far_keys, c.scan_tmp, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
+                  c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.rebin_tiles, c.d_np, c.d_counters,
+                  c.far_keys, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c.mixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);

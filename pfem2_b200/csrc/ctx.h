@@ -125,14 +125,13 @@ struct Ctx {
   // environment variable PFEM2_ADVECT_SPLIT_MIN overrides it at creation
   long long adv_split_min = 1LL << 23;
   int* cell_start[2] = {};
-  int* cell_count = nullptr;
+  unsigned long long* rebin_tiles = nullptr;  // ticket + status words of the rebin's single-pass scan
   int* d_np = nullptr;       // [2] particle count of buffer 0/1
   int far_cap = 0;
   unsigned long long* far_keys = nullptr;
   int* d_counters = nullptr;  // see enum Counter
   void* partial = nullptr;    // [nc][NV][dim+1] Real projection partials
-  int* scan_tmp = nullptr;
-  int scan_tmp_n = 0;
+
   int ring_max = 0;
   int list_cap = 0;           // per-cell incoming particle capacity in the rebin pass
   int nbucket_max = 0;
@@ -174,7 +173,8 @@ enum Counter {
   CNT_CAP_OVERFLOW = 5,
   CNT_FAR_OVERFLOW = 6,
   CNT_ZERO_WEIGHT = 7,
-  CNT_N = 8
+  CNT_SCAN_TIMEOUT = 8,
+  CNT_N = 9
 };
 
 // error reporting

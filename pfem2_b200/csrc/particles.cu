@@ -642,23 +642,49 @@ __device__ __forceinline__ int far_lower_bound(const unsigned long long* keys, i
   return lo;
 }
 
-template <int DIM, typename R, int PASS, bool CHECK, bool PROJ>
+// status words of the single-pass scan over tiles of kRebinWarps cells:
+// bits 62-63 = 1 (tile aggregate known) or 2 (inclusive prefix known), the
+// low bits the value
+constexpr unsigned long long kTileAgg = 1ull << 62, kTilePre = 2ull << 62, kTileVal = (1ull << 62) - 1;
+constexpr unsigned kLookbackSpinLimit = 1u << 24;
+
+// One pass: a block takes tiles of kRebinWarps consecutive target cells in
+// ticket order (an atomic counter, so a block waits only on tiles taken by
+// blocks already running), a warp per cell gathers and checks its incoming
+// particles into shared memory, the block publishes the tile's particle
+// count and finds its output offset by looking back over the previous
+// tiles' published counts (decoupled look-back; waits bounded, a timeout is
+// flagged in CNT_SCAN_TIMEOUT), then every warp writes its cell's particles,
+// its new_start entry and its projection partials.
+template <int DIM, typename R, bool CHECK, bool PROJ>
 __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
     const int* __restrict__ old_start, const int* __restrict__ newcell, const R* __restrict__ oxi,
     const R* __restrict__ ou, size_t cap, int* __restrict__ ncell, R* __restrict__ nxi, R* __restrict__ nu,
-    const int* __restrict__ new_start, int* __restrict__ cell_count, int nc, const int* __restrict__ ring_ptr,
+    int* __restrict__ new_start, int* __restrict__ np_out, int nc, const int* __restrict__ ring_ptr,
     const int* __restrict__ ring_cell, const unsigned long long* __restrict__ far_keys, int far_cap,
     const DevInst* __restrict__ inst, const int* __restrict__ cell_inst, const int* __restrict__ cv,
-    const R* __restrict__ Vr, int nv, R* __restrict__ partial, int list_cap, int* __restrict__ counters) {
+    const R* __restrict__ Vr, int nv, R* __restrict__ partial, int list_cap, int* __restrict__ counters,
+    unsigned long long* __restrict__ tiles) {
   constexpr int NV = Dims<DIM>::NV;
   extern __shared__ int smem[];
+  __shared__ int s_tile, s_base;
+  __shared__ int s_cnt[kRebinWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* list = smem + warp * (list_cap + kMaxBuckets);
   int* bcnt = list + list_cap;
   const unsigned lt = lanemask_lt();
   int nfar = counters[CNT_FAR];
   if (nfar > far_cap) nfar = far_cap;
-  for (int c = blockIdx.x * kRebinWarps + warp; c < nc; c += gridDim.x * kRebinWarps) {
+  const int ntiles = (nc + kRebinWarps - 1) / kRebinWarps;
+  unsigned long long* status = tiles + 1;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd(tiles, 1ull);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= ntiles) break;
+    const int c = t * kRebinWarps + warp;
+    int ntot = 0;
+    if (c < nc) {
     // gather the incoming particles of c in (ring cell, segment) order: the
     // ring's segment bounds are loaded across lanes, then the first 32
     // new-cell ids of 8 segments at a time, so the loads overlap
@@ -785,17 +811,56 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
       }
       __syncwarp();
     }
-    const int ntot = n_keep + n_new;
-    if (PASS == 0) {
+      ntot = n_keep + n_new;
+      if (CHECK && lane == 0) {
+        if (n_in - n_keep) atomicAdd(counters + CNT_REMOVED, n_in - n_keep);
+        if (n_new) atomicAdd(counters + CNT_RESEEDED, n_new);
+      }
+    }
+    if (lane == 0) s_cnt[warp] = ntot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long agg = 0;
+      for (int w = 0; w < kRebinWarps; ++w) agg += (unsigned)s_cnt[w];
+      unsigned long long excl = 0;
+      if (t == 0) {
+        atomicExch(status, kTilePre | agg);
+      } else {
+        atomicExch(status + t, kTileAgg | agg);
+        int j = t - 1;
+        unsigned spins = 0;
+        while (j >= 0) {
+          const unsigned long long wd = *(volatile const unsigned long long*)(status + j);
+          if ((wd >> 62) == 0) {
+            if (++spins > kLookbackSpinLimit) {
+              atomicExch(counters + CNT_SCAN_TIMEOUT, 1);
+              break;
+            }
+            __nanosleep(32);
+            continue;
+          }
+          excl += wd & kTileVal;
+          if ((wd >> 62) == 2) break;
+          --j;
+        }
+        atomicExch(status + t, kTilePre | ((excl + agg) & kTileVal));
+      }
+      s_base = (int)excl;
+    }
+    __syncthreads();
+    if (c < nc) {
+      int out = s_base;
+      for (int w = 0; w < warp; ++w) out += s_cnt[w];
       if (lane == 0) {
-        cell_count[c] = ntot;
-        if (CHECK) {
-          if (n_in - n_keep) atomicAdd(counters + CNT_REMOVED, n_in - n_keep);
-          if (n_new) atomicAdd(counters + CNT_RESEEDED, n_new);
+        new_start[c] = out;
+        if (c == nc - 1) {
+          new_start[nc] = out + ntot;
+          *np_out = out + ntot;
         }
       }
-    } else {
-      const int out = new_start[c];
+      const DevInst& I = inst[__ldg(cell_inst + c)];
+      const int q1 = I.q[1], q2 = DIM == 3 ? I.q[2] : 1;
+      const double h0 = 1.0 / I.q[0], h1 = 1.0 / q1, h2 = 1.0 / q2;
       ProjAcc<DIM, R> acc;
       if (PROJ) {
 #pragma unroll
@@ -843,127 +908,22 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
       if (PROJ) proj_store<DIM, R>(acc, partial, c, lane);
     }
     __syncwarp();
+    __syncthreads();
   }
-}
-
-// ------------------------------------------------------------------ scan
-// exclusive scan of cell_count[0..n) into out[0..n], out[n] = total.
-constexpr int kScanThreads = 512;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanThreads * kScanItems;
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restrict__ in, int n, int* __restrict__ sums) {
-  __shared__ int ws[kScanThreads / 32];
-  const int base = blockIdx.x * kScanTile;
-  int s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    int i = base + threadIdx.x + k * kScanThreads;
-    if (i < n) s += in[i];
-  }
-  s = warp_sum(s);
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int v = threadIdx.x < kScanThreads / 32 ? ws[threadIdx.x] : 0;
-    v = warp_sum(v);
-    if (threadIdx.x == 0) sums[blockIdx.x] = v;
-  }
-}
-
-__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
-  __shared__ int ws[kScanThreads / 32 + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(PFEM2_FULL_MASK, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) ws[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    int w = lane < kScanThreads / 32 ? ws[lane] : 0;
-    int z = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(PFEM2_FULL_MASK, z, o);
-      if (lane >= o) z += y;
-    }
-    if (lane < kScanThreads / 32) ws[lane] = z - w;
-    if (lane == kScanThreads / 32 - 1) ws[kScanThreads / 32] = z;
-  }
-  __syncthreads();
-  int res = ws[warp] + x - v;
-  *total = ws[kScanThreads / 32];
-  __syncthreads();
-  return res;
-}
-
-// scans the block sums in place (single block), writes the grand total
-__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int* sums, int nb, int* total_out0, int* total_out1,
-                                                            int* total_out2) {
-  int carry = 0;
-  for (int base = 0; base < nb; base += kScanThreads) {
-    int i = base + threadIdx.x;
-    int v = i < nb ? sums[i] : 0;
-    int tot;
-    int ex = block_exclusive_scan(v, &tot);
-    if (i < nb) sums[i] = carry + ex;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) {
-    *total_out0 = carry;
-    if (total_out1) *total_out1 = carry;
-    if (total_out2) *total_out2 = carry;
-  }
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restrict__ in, int n,
-                                                             const int* __restrict__ sums, int* __restrict__ out) {
-  const int base = blockIdx.x * kScanTile;
-  int vals[kScanItems];
-  int s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    int i = base + threadIdx.x * kScanItems + k;
-    vals[k] = i < n ? in[i] : 0;
-    s += vals[k];
-  }
-  int tot;
-  int ex = block_exclusive_scan(s, &tot) + sums[blockIdx.x];
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    int i = base + threadIdx.x * kScanItems + k;
-    if (i < n) out[i] = ex;
-    ex += vals[k];
-  }
-}
-
-static pfem2_status scan_counts(Ctx& c, const int* in, int n, int* out, int* np_out) {
-  int nb = (n + kScanTile - 1) / kScanTile;
-  k_scan_reduce<<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_tmp);
-  k_scan_sums<<<1, kScanThreads, 0, c.stream>>>(c.scan_tmp, nb, out + n, np_out, nullptr);
-  k_scan_final<<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_tmp, out);
-  c.launches += 3;
-  return PFEM2_OK;
 }
 
 template <int DIM, typename R, bool CHECK, bool PROJ>
 static void rebin_launch(Ctx& c, const int* newcell) {
   const int o = c.cur, nb = 1 - c.cur;
   const size_t smem = (size_t)kRebinWarps * (c.list_cap + kMaxBuckets) * sizeof(int);
+  const int ntiles = (c.nc + kRebinWarps - 1) / kRebinWarps;
   const int grid = grid_for(c, (long long)c.nc * 32, kRebinWarps * 32, 8);
-  k_rebin<DIM, R, 0, CHECK, false><<<grid, kRebinWarps * 32, smem, c.stream>>>(
-      c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, nullptr, nullptr, nullptr,
-      nullptr, c.cell_count, c.nc, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_inst, c.cell_inst, c.cv,
-      (const R*)c.Vr, c.nv, nullptr, c.list_cap, c.d_counters);
-  scan_counts(c, c.cell_count, c.nc, c.cell_start[nb], c.d_np + nb);
-  k_rebin<DIM, R, 1, CHECK, PROJ><<<grid, kRebinWarps * 32, smem, c.stream>>>(
+  cudaMemsetAsync(c.rebin_tiles, 0, sizeof(unsigned long long) * ((size_t)ntiles + 1), c.stream);
+  k_rebin<DIM, R, CHECK, PROJ><<<grid, kRebinWarps * 32, smem, c.stream>>>(
       c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, c.pcell[nb], (R*)c.pxi[nb],
-      (R*)c.pu[nb], c.cell_start[nb], nullptr, c.nc, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_inst,
-      c.cell_inst, c.cv, (const R*)c.Vr, c.nv, (R*)c.partial, c.list_cap, c.d_counters);
-  c.launches += 2;
+      (R*)c.pu[nb], c.cell_start[nb], c.d_np + nb, c.nc, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_inst,
+      c.cell_inst, c.cv, (const R*)c.Vr, c.nv, (R*)c.partial, c.list_cap, c.d_counters, c.rebin_tiles);
+  c.launches += 1;
   c.cur = nb;
 }
 
@@ -971,24 +931,18 @@ template <int DIM, typename R>
 static pfem2_status rebin_impl(Ctx& c, bool check, bool proj, bool from_advect) {
   const int* nc_arr = from_advect ? c.newcell : c.pcell[c.cur];
   const size_t smem = (size_t)kRebinWarps * (c.list_cap + kMaxBuckets) * sizeof(int);
-  static bool attr_set[2][2][2] = {};
-  (void)attr_set;
   auto set_attr = [&](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); };
   if (check && proj) {
-    set_attr((const void*)k_rebin<DIM, R, 0, true, false>);
-    set_attr((const void*)k_rebin<DIM, R, 1, true, true>);
+    set_attr((const void*)k_rebin<DIM, R, true, true>);
     rebin_launch<DIM, R, true, true>(c, nc_arr);
   } else if (check) {
-    set_attr((const void*)k_rebin<DIM, R, 0, true, false>);
-    set_attr((const void*)k_rebin<DIM, R, 1, true, false>);
+    set_attr((const void*)k_rebin<DIM, R, true, false>);
     rebin_launch<DIM, R, true, false>(c, nc_arr);
   } else if (proj) {
-    set_attr((const void*)k_rebin<DIM, R, 0, false, false>);
-    set_attr((const void*)k_rebin<DIM, R, 1, false, true>);
+    set_attr((const void*)k_rebin<DIM, R, false, true>);
     rebin_launch<DIM, R, false, true>(c, nc_arr);
   } else {
-    set_attr((const void*)k_rebin<DIM, R, 0, false, false>);
-    set_attr((const void*)k_rebin<DIM, R, 1, false, false>);
+    set_attr((const void*)k_rebin<DIM, R, false, false>);
     rebin_launch<DIM, R, false, false>(c, nc_arr);
   }
   return PFEM2_OK;
