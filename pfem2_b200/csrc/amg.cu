@@ -211,14 +211,16 @@ int aggregate(const Csr& A, const std::vector<int>& tile, std::vector<int>& agg)
   return na;
 }
 
-// one aggregate per tile (rows with off-diagonal entries only)
-int tile_aggregate(const Csr& A, const std::vector<int>& tile, std::vector<int>& agg) {
+// one aggregate per group of `per` consecutive tiles, counted from tile t0
+// (rows with off-diagonal entries only)
+int tile_aggregate(const Csr& A, const std::vector<int>& tile, int t0, int per, std::vector<int>& agg) {
   agg.assign(A.n, -1);
   int na = 0, last = -1;
   for (int i = 0; i < A.n; ++i) {
     if (isolated(A, i)) continue;
-    if (tile[i] != last) {
-      last = tile[i];
+    const int g = (tile[i] - t0) / per;
+    if (g != last) {
+      last = g;
       ++na;
     }
     agg[i] = na - 1;
@@ -344,7 +346,9 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
           V.J.val[e] = -V.w * V.w * V.dinv[i] * V.A.val[e] * V.dinv[j] + (i == j ? 2.0 * V.w * V.dinv[i] : 0.0);
         }
       std::vector<int> agg;
-      const int na = l < kMgLevels - 2 ? aggregate(V.A, V.tile, agg) : tile_aggregate(V.A, V.tile, agg);
+      // the coarsest level: groups of tiles, at most kMgCoarseMax unknowns per system
+      const int ntl = st0[s + 1] - st0[s], per = (ntl + kMgCoarseMax - 1) / kMgCoarseMax;
+      const int na = l < kMgLevels - 2 ? aggregate(V.A, V.tile, agg) : tile_aggregate(V.A, V.tile, st0[s], per, agg);
       if (na == 0) {
         set_error("amg: aggregation produced no coarse unknowns");
         return PFEM2_MESH_ERROR;

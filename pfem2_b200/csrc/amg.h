@@ -22,6 +22,7 @@
 namespace pfem2 {
 
 constexpr int kMgLevels = 4;
+constexpr int kMgCoarseMax = 160;  // level-3 unknowns per system at most
 
 struct MgHost {
   int n[kMgLevels] = {0, 0, 0, 0};        // dofs per level over all systems

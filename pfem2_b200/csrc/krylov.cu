@@ -237,8 +237,8 @@ __device__ __forceinline__ SV<T> maybe_stage(bool on, unsigned char*& cur, const
   return on ? stage_range(cur, src, lo, hi) : SV<T>{src, 0};
 }
 
-template <typename R, bool MG>
-__global__ void __launch_bounds__(kSolveThreads, MG ? 1 : 2) k_krylov(SolveArgs<R> a) {
+template <typename R, bool MG, int MINB>
+__global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ LocalSys ls[kMaxLocalSys];
   __shared__ Tile stile[kMaxBlockTiles];
@@ -943,6 +943,7 @@ struct KrylovWs {
   size_t items_bytes[2] = {0, 0};                  // shared memory of the item partials and offsets
   // multigrid of the pressure phase (phase 0)
   bool mg = false;
+  int mg_minb = 1;  // resident blocks per SM of the pressure solve: 2 for batches (many tiles per block)
   int nls0 = 1;
   int dmax = 1, s1max = 0, s2max = 0, s3max = 0, b2max = 0, o2max = 0, emax = 0;
   int n1 = 0, n2 = 0, n3 = 0;
@@ -1007,15 +1008,25 @@ static pfem2_status ws_upload_r(KrylovWs* w, bool mixed, void** p, const std::ve
 static size_t al16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 // shared-memory budget of the solver kernel (dynamic part)
-constexpr size_t kSmemBudget = 200 * 1024;
+// shared-memory budget of a block (dynamic part) with MINB resident blocks per SM
+constexpr size_t smem_budget(int minb) { return minb == 1 ? 200 * 1024 : 110 * 1024; }
 
-template <typename R, bool MG>
+template <typename R, bool MG, int MINB>
 static int occupancy(size_t smem) {
   int occ = 0;
   // one process-wide upper bound, so contexts with different hierarchies coexist
-  cudaFuncSetAttribute((const void*)k_krylov<R, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_krylov<R, MG>, kSolveThreads, smem) != cudaSuccess) return 0;
+  cudaFuncSetAttribute((const void*)k_krylov<R, MG, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem_budget(MINB));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_krylov<R, MG, MINB>, kSolveThreads, smem) != cudaSuccess)
+    return 0;
   return occ;
+}
+
+// the multigrid kernel with MINB resident blocks per SM
+template <bool MG>
+static int occupancy_any(bool mixed, int minb, size_t smem) {
+  if (minb == 1) return mixed ? occupancy<float, MG, 1>(smem) : occupancy<double, MG, 1>(smem);
+  return mixed ? occupancy<float, MG, 2>(smem) : occupancy<double, MG, 2>(smem);
 }
 
 void krylov_free(Ctx& c) {
@@ -1029,6 +1040,9 @@ void krylov_free(Ctx& c) {
 pfem2_status krylov_setup(Ctx& c) {
   KrylovWs* w = new KrylovWs();
   c.kws = w;
+  // one system: one block per SM (its coarse lists are replicated per block,
+  // so smaller blocks cost more than their extra warps bring); a batch: two
+  w->mg_minb = c.inst.size() > 1 ? 2 : 1;
   const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
   const int bps = std::max(1, c.solve_blocks_per_sm);
@@ -1043,7 +1057,7 @@ pfem2_status krylov_setup(Ctx& c) {
       // per system (a batch: tiles of ~8 slices, at most dcap per system,
       // so every instance gets a coarse space of its own size)
       const int dcap = ni == 1 ? 160 : 96;
-      const int nb = bps * c.num_sms;
+      const int nb = w->mg_minb * c.num_sms;
       long long tot_sl = 0;
       for (int i = 0; i < ni; ++i) tot_sl += c.inst[i].nv_pad / kSlice;
       for (int i = 0; i < ni; ++i) {
@@ -1072,15 +1086,15 @@ pfem2_status krylov_setup(Ctx& c) {
     for (const Tile& t : tiles) slot0[t.sys + 1]++;
     for (int s = 0; s < nsys; ++s) slot0[s + 1] += slot0[s];
     std::vector<int> owner(nsys, -1);
-    // the multigrid grid is sized before its shared memory is known (one
-    // block per SM); krylov_setup_precond checks residency afterwards
-    // the multigrid kernel runs one block per SM, the Jacobi kernel two
-    const int occ = ph == 0 ? 1 : std::min(2, c.mixed ? occupancy<float, false>(0) : occupancy<double, false>(0));
+    // the multigrid grid is sized before its shared memory is known
+    // (mg_minb blocks per SM); krylov_setup_precond checks residency
+    // afterwards. The Jacobi kernel runs two blocks per SM.
+    const int occ = ph == 0 ? w->mg_minb : std::min(2, occupancy_any<false>(c.mixed, 2, 0));
     if (occ < 1) {
       set_error("krylov: the solver kernel cannot be resident");
       return PFEM2_CUDA_ERROR;
     }
-    const int G = std::min(T, (ph == 0 ? std::min(occ, bps) : occ) * c.num_sms);
+    const int G = std::min(T, occ * c.num_sms);
     std::vector<int> bt0(G + 1), bsys_off(1, 0), bsys, bsl(2 * G, 0);
     // split the tile sequence where the running slice count crosses
     // b / G of the total (a tile goes to the block holding its midpoint):
@@ -1152,15 +1166,15 @@ pfem2_status krylov_setup(Ctx& c) {
     if (ph == 1) {
       w->stage[1] = 0;
       w->smem[1] = w->items_bytes[1];
-      if (w->smem[1] + meta <= kSmemBudget) {
+      if (w->smem[1] + meta <= smem_budget(2)) {
         w->stage[1] |= ST_L0META;
         w->smem[1] += meta;
       }
-      if (w->smem[1] + col <= kSmemBudget) {
+      if (w->smem[1] + col <= smem_budget(2)) {
         w->stage[1] |= ST_L0COL;
         w->smem[1] += col;
       }
-      const int occ2 = c.mixed ? occupancy<float, false>(w->smem[1]) : occupancy<double, false>(w->smem[1]);
+      const int occ2 = occupancy_any<false>(c.mixed, 2, w->smem[1]);
       if (occ2 * c.num_sms < G) {
         w->stage[1] = 0;
         w->smem[1] = w->items_bytes[1];
@@ -1210,7 +1224,7 @@ pfem2_status krylov_setup(Ctx& c) {
   // pressure phase without multigrid: level-0 staging only
   w->stage[0] = 0;
   w->smem[0] = w->items_bytes[0];
-  if (w->smem[0] + w->l0_meta[0] + w->l0_col[0] <= kSmemBudget) {
+  if (w->smem[0] + w->l0_meta[0] + w->l0_col[0] <= smem_budget(2)) {
     w->stage[0] = ST_L0META | ST_L0COL;
     w->smem[0] += w->l0_meta[0] + w->l0_col[0];
   }
@@ -1287,15 +1301,15 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   const std::pair<int, size_t> cats[] = {{ST_L0META, w->l0_meta[0]}, {ST_MGIDX, idx}, {ST_MIRROR, mirror},
                                          {ST_L0COL, w->l0_col[0]}, {ST_MGCOL, cols}, {ST_MGVAL, vals}};
   for (const auto& cs : cats)
-    if (smem + cs.second <= kSmemBudget) {
+    if (smem + cs.second <= smem_budget(w->mg_minb)) {
       stage |= cs.first;
       smem += cs.second;
     }
-  if (base > kSmemBudget) {
+  if (base > smem_budget(w->mg_minb)) {
     set_error("krylov: the pressure multigrid's per-block data exceed shared memory");
     return PFEM2_INVALID_ARG;
   }
-  const int occ = c.mixed ? occupancy<float, true>(smem) : occupancy<double, true>(smem);
+  const int occ = occupancy_any<true>(c.mixed, w->mg_minb, smem);
   if (occ * c.num_sms < w->grid[0]) {
     set_error("krylov: the multigrid solver grid cannot be resident");
     return PFEM2_CUDA_ERROR;
@@ -1481,11 +1495,12 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   k_init_solve<<<1, 32, 0, c.stream>>>(a.nsys, w->active, c.barrier, c.d_err);
   c.launches++;
   void* args[] = {&a};
+  const void* kmg = w->mg_minb == 1 ? (const void*)k_krylov<R, true, 1> : (const void*)k_krylov<R, true, 2>;
   if (mg)
-    PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, true>, dim3(w->grid[ph]), dim3(kSolveThreads),
+    PFEM2_CUDA(cudaLaunchCooperativeKernel(kmg, dim3(w->grid[ph]), dim3(kSolveThreads),
                                            args, w->smem[ph], c.stream));
   else
-    PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, false>, dim3(w->grid[ph]), dim3(kSolveThreads),
+    PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, false, 2>, dim3(w->grid[ph]), dim3(kSolveThreads),
                                            args, w->smem[ph], c.stream));
   c.launches++;
   return PFEM2_OK;
