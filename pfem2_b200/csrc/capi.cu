@@ -386,6 +386,8 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(dalloc(&c.far_keys, c.far_cap));
   PFEM2_TRY(dalloc(&c.barrier, 2));
   PFEM2_TRY(dalloc(&c.d_err, 1));
+  PFEM2_TRY(dalloc(&c.loads_dev, 7 * c.inst.size()));
+  PFEM2_CUDA(cudaMallocHost(&c.loads_host, sizeof(double) * 7 * c.inst.size()));
   c.list_cap = c.cfg.particles_per_cell_max > 0 ? c.cfg.particles_per_cell_max : (dim == 2 ? 512 : 1024);
   if (!c.cfg.particles_only) {
     PFEM2_TRY(krylov_setup(c));
@@ -624,6 +626,9 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
     cudaFree(c.pcell[b]); cudaFree(c.pxi[b]); cudaFree(c.pu[b]); cudaFree(c.cell_start[b]);
   }
   for (int k = 0; k < 8; ++k) cudaEventDestroy(c.ev[k]);
+  for (const Ctx::LoadFaces& e : c.load_faces) cudaFree(e.d);
+  cudaFree(c.loads_dev);
+  cudaFreeHost(c.loads_host);
   cudaStreamDestroy(c.stream);
   delete x;
   return PFEM2_OK;
@@ -794,68 +799,24 @@ pfem2_status pfem2_step(pfem2_ctx* x) {
   return PFEM2_OK;
 }
 
-pfem2_status pfem2_step_and_read(pfem2_ctx* x, double* loads_out, const int32_t* fields, int32_t n_fields,
-                                 double* host_fields) {
-  SEED_CHECK(x);
-  Ctx& c = x->c;
-  PFEM2_TRY(pfem2_step(x));
-  const int ni = (int)c.inst.size();
-  if (loads_out) {
-    double* d;
-    PFEM2_CUDA(cudaMallocAsync(&d, sizeof(double) * 5 * ni, c.stream));
-    for (int i = 0; i < ni; ++i) PFEM2_TRY(launch_loads(c, i, c.inst[i].cs.load_patch_id, d + 5 * i));
-    PFEM2_CUDA(cudaMemcpyAsync(loads_out, d, sizeof(double) * 5 * ni, cudaMemcpyDeviceToHost, c.stream));
-    PFEM2_CUDA(cudaFreeAsync(d, c.stream));
-  }
-  if (host_fields && fields) {
-    size_t off = 0;
-    for (int i = 0; i < ni; ++i)
-      for (int f = 0; f < n_fields; ++f) {
-        if (fields[f] < 0 || fields[f] >= PFEM2_N_FIELDS) { set_error("bad field"); return PFEM2_INVALID_ARG; }
-        PFEM2_CUDA(cudaMemcpyAsync(host_fields + off, c.F[fields[f]] + c.inst[i].v_off, sizeof(double) * c.inst[i].nv,
-                                   cudaMemcpyDeviceToHost, c.stream));
-        off += c.inst[i].nv;
-      }
-  }
-  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
-  for (int i = 0; i < ni && loads_out; ++i) {
-    const pfem2_case& cs = c.inst[i].cs;
-    double* o = loads_out + 5 * i;
-    double raw[5];
-    std::memcpy(raw, o, sizeof(raw));
-    if (c.dim == 2) {
-      const double s = cs.rho * cs.load_umean * cs.load_umean * cs.load_diam;
-      for (int k = 0; k < 4; ++k) o[k] = s != 0 ? 2.0 * raw[k] / s : 0.0;
-    } else {
-      o[3] = 0.0;
-    }
-    o[4] = 0.0;
-  }
-  if (loads_out) {
-    // probe pressure difference
-    for (int i = 0; i < ni; ++i) {
-      const pfem2_case& cs = c.inst[i].cs;
-      double pa = 0, pb = 0;
-      if (cs.probe_a >= 0) PFEM2_CUDA(cudaMemcpy(&pa, c.F[PFEM2_FIELD_P] + c.inst[i].v_off + cs.probe_a, 8, cudaMemcpyDeviceToHost));
-      if (cs.probe_b >= 0) PFEM2_CUDA(cudaMemcpy(&pb, c.F[PFEM2_FIELD_P] + c.inst[i].v_off + cs.probe_b, 8, cudaMemcpyDeviceToHost));
-      loads_out[5 * i + 4] = pa - pb;
-    }
-  }
-  return check_counters(c, false);
+// the loads of instance i (5 sums, then the two probe pressures) into
+// loads_dev[7 i ...], asynchronously on the context's stream
+static pfem2_status enqueue_loads(Ctx& c, int i, int patch) {
+  double* d = c.loads_dev + 7 * i;
+  PFEM2_TRY(launch_loads(c, i, patch, d));
+  const pfem2_case& cs = c.inst[i].cs;
+  const double* P = c.F[PFEM2_FIELD_P] + c.inst[i].v_off;
+  PFEM2_CUDA(cudaMemsetAsync(d + 5, 0, 2 * sizeof(double), c.stream));
+  if (cs.probe_a >= 0) PFEM2_CUDA(cudaMemcpyAsync(d + 5, P + cs.probe_a, 8, cudaMemcpyDeviceToDevice, c.stream));
+  if (cs.probe_b >= 0) PFEM2_CUDA(cudaMemcpyAsync(d + 6, P + cs.probe_b, 8, cudaMemcpyDeviceToDevice, c.stream));
+  return PFEM2_OK;
 }
 
-pfem2_status pfem2_loads(pfem2_ctx* x, int32_t instance, int32_t patch_id, double out[5]) {
-  SETUP_CHECK(x);
-  Ctx& c = x->c;
-  if (instance < 0 || instance >= (int)c.inst.size() || !out) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
-  double* d;
-  PFEM2_CUDA(cudaMalloc(&d, sizeof(double) * 5));
-  PFEM2_TRY(launch_loads(c, instance, patch_id, d));
-  double raw[5];
-  PFEM2_CUDA(cudaMemcpyAsync(raw, d, sizeof(raw), cudaMemcpyDeviceToHost, c.stream));
-  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
-  cudaFree(d);
-  const pfem2_case& cs = c.inst[instance].cs;
+// the 5 published load values of instance i from its 7 raw values
+// (2D: drag and lift coefficients split into viscous and pressure parts,
+// 3D: the force; the last entry is the probe pressure difference)
+static void finish_loads(const Ctx& c, int i, const double* raw, double* out) {
+  const pfem2_case& cs = c.inst[i].cs;
   if (c.dim == 2) {
     const double s = cs.rho * cs.load_umean * cs.load_umean * cs.load_diam;
     for (int k = 0; k < 4; ++k) out[k] = s != 0 ? 2.0 * raw[k] / s : 0.0;
@@ -863,11 +824,45 @@ pfem2_status pfem2_loads(pfem2_ctx* x, int32_t instance, int32_t patch_id, doubl
     for (int k = 0; k < 3; ++k) out[k] = raw[k];
     out[3] = 0.0;
   }
-  double pa = 0, pb = 0;
-  const int vo = c.inst[instance].v_off;
-  if (cs.probe_a >= 0) PFEM2_CUDA(cudaMemcpy(&pa, c.F[PFEM2_FIELD_P] + vo + cs.probe_a, 8, cudaMemcpyDeviceToHost));
-  if (cs.probe_b >= 0) PFEM2_CUDA(cudaMemcpy(&pb, c.F[PFEM2_FIELD_P] + vo + cs.probe_b, 8, cudaMemcpyDeviceToHost));
-  out[4] = (cs.probe_a >= 0 ? pa : 0.0) - (cs.probe_b >= 0 ? pb : 0.0);
+  out[4] = (cs.probe_a >= 0 ? raw[5] : 0.0) - (cs.probe_b >= 0 ? raw[6] : 0.0);
+}
+
+pfem2_status pfem2_step_and_read(pfem2_ctx* x, double* loads_out, const int32_t* fields, int32_t n_fields,
+                                 double* host_fields) {
+  SEED_CHECK(x);
+  Ctx& c = x->c;
+  const int ni = (int)c.inst.size();
+  if (host_fields && fields)
+    for (int f = 0; f < n_fields; ++f)
+      if (fields[f] < 0 || fields[f] >= PFEM2_N_FIELDS) { set_error("bad field"); return PFEM2_INVALID_ARG; }
+  PFEM2_TRY(pfem2_step(x));
+  if (loads_out) {
+    for (int i = 0; i < ni; ++i) PFEM2_TRY(enqueue_loads(c, i, c.inst[i].cs.load_patch_id));
+    PFEM2_CUDA(cudaMemcpyAsync(c.loads_host, c.loads_dev, sizeof(double) * 7 * ni, cudaMemcpyDeviceToHost, c.stream));
+  }
+  if (host_fields && fields) {
+    size_t off = 0;
+    for (int i = 0; i < ni; ++i)
+      for (int f = 0; f < n_fields; ++f) {
+        PFEM2_CUDA(cudaMemcpyAsync(host_fields + off, c.F[fields[f]] + c.inst[i].v_off, sizeof(double) * c.inst[i].nv,
+                                   cudaMemcpyDeviceToHost, c.stream));
+        off += c.inst[i].nv;
+      }
+  }
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  for (int i = 0; i < ni && loads_out; ++i) finish_loads(c, i, c.loads_host + 7 * i, loads_out + 5 * i);
+  return check_counters(c, false);
+}
+
+pfem2_status pfem2_loads(pfem2_ctx* x, int32_t instance, int32_t patch_id, double out[5]) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (instance < 0 || instance >= (int)c.inst.size() || !out) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  PFEM2_TRY(enqueue_loads(c, instance, patch_id));
+  double* h = c.loads_host + 7 * instance;
+  PFEM2_CUDA(cudaMemcpyAsync(h, c.loads_dev + 7 * instance, 7 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  finish_loads(c, instance, h, out);
   return PFEM2_OK;
 }
 

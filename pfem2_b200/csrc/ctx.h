@@ -78,6 +78,16 @@ struct Ctx {
   DevInst* d_inst = nullptr;
   std::vector<DevInst> h_inst;
 
+  // loads: boundary faces of a patch (global cell * faces-per-cell + face),
+  // built on first use per (instance, patch)
+  struct LoadFaces {
+    int inst, patch, n;
+    int* d;
+  };
+  std::vector<LoadFaces> load_faces;
+  double* loads_dev = nullptr;   // [7 * instances]: 5 load sums, then the two probe pressures
+  double* loads_host = nullptr;  // pinned copy of loads_dev
+
   // sparsity: CSR (setup, tests) and SELL-32 (solvers)
   int* rp = nullptr;
   int* ci = nullptr;

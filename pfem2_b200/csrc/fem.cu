@@ -573,43 +573,41 @@ pfem2_status launch_restore_frozen(Ctx& c) {
 }
 
 // ---------------------------------------------------------------- loads
-// One block; FP64 face integrals over the instance's cells (fixed-order
-// block reduction, so the result is deterministic).
+// One block over the patch's boundary faces; FP64 face integrals with a
+// fixed-order block reduction, so the result is deterministic.
 template <int DIM>
-__global__ void __launch_bounds__(256) k_loads(int c0, int c1, int patch, const double* __restrict__ X,
-                                               const int* __restrict__ cv, const signed char* __restrict__ fb,
+__global__ void __launch_bounds__(256) k_loads(const int* __restrict__ faces, int nfaces,
+                                               const double* __restrict__ X, const int* __restrict__ cv,
                                                const double* __restrict__ P, const double* __restrict__ Vx,
                                                const double* __restrict__ Vy, double mu, double* __restrict__ out5) {
   constexpr int NV = Dims<DIM>::NV;
   double acc[5] = {0, 0, 0, 0, 0};  // 2D: Fx_nu, Fx_p, Fy_nu, Fy_p ; 3D: Fx, Fy, Fz
-  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-    for (int f = 0; f < Dims<DIM>::NF; ++f) {
-      if (fb[(size_t)c * Dims<DIM>::NF + f] != patch) continue;
-      LocalCell<DIM, double> L;
-      double x0[DIM];
-      load_local_cell<DIM, double>(X, cv, c, L, x0);
-      for (int iq = 0; iq < (DIM == 2 ? 2 : 4); ++iq) {
-        double xi[DIM];
-        face_qp_xi<DIM, double>(f, iq, xi);
-        QP<DIM, double> q;
-        eval_qp<DIM, double>(L, xi, face_qp_w<DIM>(), f, q);
-        double pq = 0.0, dv = 0.0;
+  for (int k = threadIdx.x; k < nfaces; k += blockDim.x) {
+    const int c = faces[k] / Dims<DIM>::NF, f = faces[k] % Dims<DIM>::NF;
+    LocalCell<DIM, double> L;
+    double x0[DIM];
+    load_local_cell<DIM, double>(X, cv, c, L, x0);
+    for (int iq = 0; iq < (DIM == 2 ? 2 : 4); ++iq) {
+      double xi[DIM];
+      face_qp_xi<DIM, double>(f, iq, xi);
+      QP<DIM, double> q;
+      eval_qp<DIM, double>(L, xi, face_qp_w<DIM>(), f, q);
+      double pq = 0.0, dv = 0.0;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const int g = cv[(size_t)c * NV + v];
-          pq += P[g] * q.N[v];
-          if (DIM == 2)
-            dv += (Vx[g] * q.n[1] - Vy[g] * q.n[0]) * (q.G[v][0] * q.n[0] + q.G[v][1] * q.n[1]);
-        }
-        if (DIM == 2) {
-          acc[0] += mu * dv * q.n[1] * q.JxW;
-          acc[1] -= pq * q.n[0] * q.JxW;
-          acc[2] -= mu * dv * q.n[0] * q.JxW;
-          acc[3] -= pq * q.n[1] * q.JxW;
-        } else {
+      for (int v = 0; v < NV; ++v) {
+        const int g = cv[(size_t)c * NV + v];
+        pq += P[g] * q.N[v];
+        if (DIM == 2)
+          dv += (Vx[g] * q.n[1] - Vy[g] * q.n[0]) * (q.G[v][0] * q.n[0] + q.G[v][1] * q.n[1]);
+      }
+      if (DIM == 2) {
+        acc[0] += mu * dv * q.n[1] * q.JxW;
+        acc[1] -= pq * q.n[0] * q.JxW;
+        acc[2] -= mu * dv * q.n[0] * q.JxW;
+        acc[3] -= pq * q.n[1] * q.JxW;
+      } else {
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) acc[d] += pq * q.n[d] * q.JxW;
-        }
+        for (int d = 0; d < DIM; ++d) acc[d] += pq * q.n[d] * q.JxW;
       }
     }
   }
@@ -630,12 +628,31 @@ __global__ void __launch_bounds__(256) k_loads(int c0, int c1, int patch, const 
 
 pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev) {
   const HostInst& in = c.inst[instance];
+  const Ctx::LoadFaces* lf = nullptr;
+  for (const Ctx::LoadFaces& e : c.load_faces)
+    if (e.inst == instance && e.patch == patch) lf = &e;
+  if (!lf) {
+    // first use: the faces of the instance that carry this boundary id, in
+    // cell order (the order of the reference's loop over cells and faces)
+    const int NF = c.dim == 2 ? 4 : 6;
+    std::vector<int> h;
+    for (int k = 0; k < in.nc; ++k)
+      for (int f = 0; f < NF; ++f)
+        if (in.fb[(size_t)k * NF + f] == patch) h.push_back((in.c_off + k) * NF + f);
+    Ctx::LoadFaces e{instance, patch, (int)h.size(), nullptr};
+    if (e.n > 0) {
+      PFEM2_CUDA(cudaMalloc(&e.d, sizeof(int) * h.size()));
+      PFEM2_CUDA(cudaMemcpy(e.d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+    }
+    c.load_faces.push_back(e);
+    lf = &c.load_faces.back();
+  }
   if (c.dim == 2)
-    k_loads<2><<<1, 256, 0, c.stream>>>(in.c_off, in.c_off + in.nc, patch, c.X, c.cv, c.fb, c.F[PFEM2_FIELD_P],
-                                        c.F[PFEM2_FIELD_VX], c.F[PFEM2_FIELD_VY], in.cs.mu, out_dev);
+    k_loads<2><<<1, 256, 0, c.stream>>>(lf->d, lf->n, c.X, c.cv, c.F[PFEM2_FIELD_P], c.F[PFEM2_FIELD_VX],
+                                        c.F[PFEM2_FIELD_VY], in.cs.mu, out_dev);
   else
-    k_loads<3><<<1, 256, 0, c.stream>>>(in.c_off, in.c_off + in.nc, patch, c.X, c.cv, c.fb, c.F[PFEM2_FIELD_P],
-                                        c.F[PFEM2_FIELD_VX], c.F[PFEM2_FIELD_VY], in.cs.mu, out_dev);
+    k_loads<3><<<1, 256, 0, c.stream>>>(lf->d, lf->n, c.X, c.cv, c.F[PFEM2_FIELD_P], c.F[PFEM2_FIELD_VX],
+                                        c.F[PFEM2_FIELD_VY], in.cs.mu, out_dev);
   c.launches++;
   return PFEM2_OK;
 }
