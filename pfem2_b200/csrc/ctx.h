@@ -22,6 +22,7 @@ struct DevInst {
   double dt_sub;  // dt / PARTICLES_MOVEMENT_STEPS
   unsigned open_mask;
   int q[3];
+  double h[3];  // sub-cell widths 1.0 / q of check_cell_for_empty_parts
   int max_per_part;
   int v_off, nv_pad, c_off, nc;
 };

@@ -606,19 +606,49 @@ __device__ __forceinline__ void proj_add(ProjAcc<DIM, R>& acc, const R* x, const
   }
 }
 
+// Sums N values (N a power of two, at most 32) over a warp with N - 1
+// exchanges instead of N * 5: at each halving step a lane keeps one half of
+// its values, sends the other half to its partner and adds what it receives.
+// Afterwards the lane holds the warp total of value warp_sum_many_index<N>.
+template <int N, typename T>
+__device__ __forceinline__ T warp_sum_many(T (&v)[N], int lane) {
+#pragma unroll
+  for (int h = N / 2, o = 16; h >= 1; h >>= 1, o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const T send = up ? v[i] : v[i + h];
+      const T keep = up ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(PFEM2_FULL_MASK, send, o);
+    }
+  }
+  T r = v[0];
+#pragma unroll
+  for (int o = 16 / N; o > 0; o >>= 1) r += __shfl_xor_sync(PFEM2_FULL_MASK, r, o);
+  return r;
+}
+
+template <int N>
+__device__ __forceinline__ int warp_sum_many_index(int lane) {
+  int idx = 0;
+#pragma unroll
+  for (int h = N / 2, o = 16; h >= 1; h >>= 1, o >>= 1)
+    if (lane & o) idx += h;
+  return idx;
+}
+
 template <int DIM, typename R>
 __device__ __forceinline__ void proj_store(ProjAcc<DIM, R>& acc, R* __restrict__ partial, int c, int lane) {
   constexpr int K = Dims<DIM>::NV * (DIM + 1);
+  constexpr int N = K <= 16 ? 16 : 32;
+  static_assert(K <= N, "projection partials exceed a warp");
+  R v[N];
 #pragma unroll
-  for (int v = 0; v < Dims<DIM>::NV; ++v)
-#pragma unroll
-    for (int k = 0; k <= DIM; ++k) acc.a[v][k] = warp_sum(acc.a[v][k]);
-  if (lane == 0) {
-#pragma unroll
-    for (int v = 0; v < Dims<DIM>::NV; ++v)
-#pragma unroll
-      for (int k = 0; k <= DIM; ++k) partial[(size_t)c * K + v * (DIM + 1) + k] = acc.a[v][k];
-  }
+  for (int i = 0; i < N; ++i) v[i] = i < K ? acc.a[i / (DIM + 1)][i % (DIM + 1)] : R(0);
+  const R tot = warp_sum_many<N, R>(v, lane);
+  const int idx = warp_sum_many_index<N>(lane);
+  // every value is held by 32 / N lanes; the first of them stores it
+  if ((lane & (32 / N - 1)) == 0 && idx < K) partial[(size_t)c * K + idx] = tot;
 }
 
 // sub-cell index of check_cell_for_empty_parts: unsigned(xi / h) with
@@ -757,7 +787,7 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
     const DevInst& I = inst[__ldg(cell_inst + c)];
     const int q0 = I.q[0], q1 = I.q[1], q2 = DIM == 3 ? I.q[2] : 1;
     const int nb1 = q1 + 1, nb2 = q2 + 1;
-    const double h0 = 1.0 / q0, h1 = 1.0 / q1, h2 = 1.0 / q2;
+    const double h0 = I.h[0], h1 = I.h[1], h2 = I.h[2];
     int n_keep = n_in, n_new = 0;
     if (CHECK) {
       const int nb = (q0 + 1) * nb1 * nb2;
@@ -819,33 +849,42 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
     }
     if (lane == 0) s_cnt[warp] = ntot;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (warp == 0) {
       unsigned long long agg = 0;
       for (int w = 0; w < kRebinWarps; ++w) agg += (unsigned)s_cnt[w];
       unsigned long long excl = 0;
       if (t == 0) {
-        atomicExch(status, kTilePre | agg);
+        if (lane == 0) atomicExch(status, kTilePre | agg);
       } else {
-        atomicExch(status + t, kTileAgg | agg);
+        if (lane == 0) atomicExch(status + t, kTileAgg | agg);
+        // look back over windows of 32 predecessors (lane k reads tile
+        // j - k): the window ends at the nearest tile with a published
+        // prefix; the tiles before it must have published their aggregates
         int j = t - 1;
         unsigned spins = 0;
-        while (j >= 0) {
-          const unsigned long long wd = *(volatile const unsigned long long*)(status + j);
-          if ((wd >> 62) == 0) {
+        for (;;) {
+          const int k = j - lane;
+          const unsigned long long wd =
+              k >= 0 ? *(volatile const unsigned long long*)(status + k) : kTilePre;  // before tile 0: prefix 0
+          const unsigned pre = __ballot_sync(PFEM2_FULL_MASK, (wd >> 62) == 2);
+          const unsigned wait = __ballot_sync(PFEM2_FULL_MASK, (wd >> 62) == 0);
+          const int lp = pre ? __ffs(pre) - 1 : 31;
+          const unsigned upto = lp == 31 ? PFEM2_FULL_MASK : (2u << lp) - 1u;
+          if (wait & upto) {
             if (++spins > kLookbackSpinLimit) {
-              atomicExch(counters + CNT_SCAN_TIMEOUT, 1);
+              if (lane == 0) atomicExch(counters + CNT_SCAN_TIMEOUT, 1);
               break;
             }
             __nanosleep(32);
             continue;
           }
-          excl += wd & kTileVal;
-          if ((wd >> 62) == 2) break;
-          --j;
+          excl += warp_sum((unsigned long long)(lane <= lp ? (wd & kTileVal) : 0ull));
+          if (pre) break;
+          j -= 32;
         }
-        atomicExch(status + t, kTilePre | ((excl + agg) & kTileVal));
+        if (lane == 0) atomicExch(status + t, kTilePre | ((excl + agg) & kTileVal));
       }
-      s_base = (int)excl;
+      if (lane == 0) s_base = (int)excl;
     }
     __syncthreads();
     if (c < nc) {
@@ -860,7 +899,7 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
       }
       const DevInst& I = inst[__ldg(cell_inst + c)];
       const int q1 = I.q[1], q2 = DIM == 3 ? I.q[2] : 1;
-      const double h0 = 1.0 / I.q[0], h1 = 1.0 / q1, h2 = 1.0 / q2;
+      const double h0 = I.h[0], h1 = I.h[1], h2 = I.h[2];
       ProjAcc<DIM, R> acc;
       if (PROJ) {
 #pragma unroll
