@@ -589,9 +589,11 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
   }
   H.c3_ptr.push_back((int)H.c3_col.size());
   H.g3_ptr.assign(1, 0);
+  H.c3_pos.assign(H.c3_lk.size(), 0);
   for (int d = 0; d < H.n[3]; ++d) {
-    for (int r : g3_rows[d]) H.g3_row.push_back(r);
-    H.g3_ptr.push_back((int)H.g3_row.size());
+    int n = H.g3_ptr.back();
+    for (int r : g3_rows[d]) H.c3_pos[r] = n++;
+    H.g3_ptr.push_back(n);
   }
   for (int sl = 0; sl < c.nslices; ++sl) {
     H.p0_ptr[sl + 1] = H.p0_ptr[sl] + H.p0_len[sl] * kSlice;

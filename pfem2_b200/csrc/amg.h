@@ -36,10 +36,10 @@ struct MgHost {
   // b3 = Pt_2^T b2 in two steps: every block adds up the contributions of
   // its own level-2 rows to the level-3 dofs they touch (CSR rows c3,
   // columns = own level-2 row - first own row, grouped per block by c3_blk,
-  // c3_lk = the dof's system among the block's systems); each level-3 dof
-  // then sums its contribution rows g3_row[g3_ptr[d] .. g3_ptr[d+1]) in
-  // block order
-  std::vector<int> c3_blk, c3_ptr, c3_col, c3_lk, g3_ptr, g3_row;
+  // c3_lk = the dof's system among the block's systems) and stores row r at
+  // c3_pos[r]; the contributions of level-3 dof d are then the contiguous
+  // range [g3_ptr[d], g3_ptr[d+1]) of that array, in block order
+  std::vector<int> c3_blk, c3_ptr, c3_col, c3_lk, g3_ptr, c3_pos;
   std::vector<double> c3_val;
   // level-0 smoother J_0 on the SELL pattern of A
   std::vector<double> j0;

@@ -102,7 +102,7 @@ template <typename R> struct SolveArgs {
   const int *lk1, *lk2;                 // local system index of each level-1/2 dof (in its owner block)
   const int *r01_ptr, *r01_col, *r02_ptr, *r02_col;
   const R *r01_val, *r02_val;
-  const int *c3_blk, *c3_ptr, *c3_col, *c3_lk, *g3_ptr, *g3_row;
+  const int *c3_blk, *c3_ptr, *c3_col, *c3_lk, *g3_ptr, *c3_pos;
   const R* c3_val;
   R* contrib;                           // [c3 rows] contributions to b3
   const R* j0;                          // [nell]
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
   const SV<int> SLc = maybe_stage<int>(a.stage & ST_L0COL, cur, a.sl_col, a.sl_ptr[bs0], a.sl_ptr[bs1]);
   int s1_lo = 0, s1_hi = 0, s2_lo = 0, s2_hi = 0, s3_lo = 0, s3_hi = 0, o1lo = 0, o1hi = 0, o2lo = 0, o2hi = 0;
   SV<int> LK1{}, LK2{}, R01P{}, R01C{}, R02P{}, R02C{}, S1K{}, J1P{}, J1C{}, P1P{}, P1C{}, S2K{}, J2P{}, J2C{}, P2P{},
-      P2C{}, S3K{}, S3E{}, S3S{}, C3K{}, C3P{}, C3C{}, G3P{}, G3R{}, P0P{}, P0L{}, P0C{};
+      P2C{}, S3K{}, S3E{}, S3S{}, C3K{}, C3P{}, C3Q{}, C3C{}, G3P{}, P0P{}, P0L{}, P0C{};
   SV<R> P1V{}, J2V{}, P2V{}, C3V{}, P0V{};
   int c3lo = 0, c3hi = 0;
   if (MG) {
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     C3K = maybe_stage<int>(si, cur, a.c3_lk, c3lo, c3hi);
     C3P = maybe_stage<int>(si, cur, a.c3_ptr, c3lo, c3hi + 1);
     G3P = maybe_stage<int>(si, cur, a.g3_ptr, r3lo, r3hi + 1);
-    G3R = maybe_stage<int>(si, cur, a.g3_row, a.g3_ptr[r3lo], a.g3_ptr[r3hi]);
+    C3Q = maybe_stage<int>(si, cur, a.c3_pos, c3lo, c3hi);
     P0P = maybe_stage<int>(si, cur, a.p0_ptr, bs0, bs1 + 1);
     P0L = maybe_stage<int>(si, cur, a.p0_len, bs0, bs1);
     R01C = maybe_stage<int>(sc, cur, a.r01_col, a.r01_ptr[o1lo], a.r01_ptr[o1hi]);
@@ -637,28 +637,43 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         for (int rr = c3lo + threadIdx.x; rr < c3hi; rr += kSolveThreads) {
           const int act = ls[C3K[rr]].act;
           if (act != ACT_B && act != ACT_OUT_B) continue;
-          a.contrib[rr] = csr_dot<1, 4, R>(R(0), C3P[rr], C3P[rr + 1], 0, C3C, C3V, [&](int c) { return sb2o[c]; });
+          a.contrib[C3Q[rr]] = csr_dot<1, 4, R>(R(0), C3P[rr], C3P[rr + 1], 0, C3C, C3V, [&](int c) { return sb2o[c]; });
         }
       }
       if (any_uz) {
-        // every global read first: b2 of the local systems, J1 b1 on the
-        // level-1 list, J0 r on the own rows (into z)
+        // every global read first: b2 of the local systems, b3 (the
+        // contiguous contributions of each level-3 dof summed by a warp,
+        // four dofs per warp at a time so that their loads overlap), J1 b1
+        // on the level-1 list, J0 r on the own rows (into z)
         for (int k = 0; k < nls; ++k) {
           if (ls[k].act != ACT_UZ) continue;
           const int n = ls[k].n2, o = ls[k].off2;
           for (int d = threadIdx.x; d < n; d += kSolveThreads) sb2[ls[k].b2off + d] = __ldcg(a.b2 + o + d);
           const int D = ls[k].D3, o3 = ls[k].off3;
-          for (int d = threadIdx.x; d < D; d += kSolveThreads) {
-            const int q0 = G3P[o3 + d], q1 = G3P[o3 + d + 1];
-            R acc = R(0);
-            for (int qb = q0; qb < q1; qb += 8) {
-              R v[8];
+          for (int d0 = 4 * warp; d0 < D; d0 += 4 * kWarps) {
+            R v[4][8];
+            int q0[4], q1[4];
 #pragma unroll
-              for (int u = 0; u < 8; ++u) v[u] = qb + u < q1 ? __ldcg(a.contrib + G3R[qb + u]) : R(0);
-#pragma unroll
-              for (int u = 0; u < 8; ++u) acc += v[u];
+            for (int r = 0; r < 4; ++r) {
+              q0[r] = d0 + r < D ? G3P[o3 + d0 + r] : 0;
+              q1[r] = d0 + r < D ? G3P[o3 + d0 + r + 1] : 0;
             }
-            sb3[k * a.dmax + d] = acc;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                const int q = q0[r] + u * 32 + lane;
+                v[r][u] = q < q1[r] ? __ldcg(a.contrib + q) : R(0);
+              }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              R acc = R(0);
+#pragma unroll
+              for (int u = 0; u < 8; ++u) acc += v[r][u];
+              for (int q = q0[r] + 256 + lane; q < q1[r]; q += 32) acc += __ldcg(a.contrib + q);
+              acc = warp_sum(acc);
+              if (lane == 0 && d0 + r < D) sb3[k * a.dmax + d0 + r] = acc;
+            }
           }
         }
         {
@@ -952,7 +967,7 @@ struct KrylovWs {
   int *toff[4] = {}, *lk[3] = {};
   int *r01_ptr = nullptr, *r01_col = nullptr, *r02_ptr = nullptr, *r02_col = nullptr;
   void *r01_val = nullptr, *r02_val = nullptr, *j0 = nullptr;
-  int *c3_blk = nullptr, *c3_ptr = nullptr, *c3_col = nullptr, *c3_lk = nullptr, *g3_ptr = nullptr, *g3_row = nullptr;
+  int *c3_blk = nullptr, *c3_ptr = nullptr, *c3_col = nullptr, *c3_lk = nullptr, *g3_ptr = nullptr, *c3_pos = nullptr;
   void *c3_val = nullptr, *contrib = nullptr;
   int *p0_ptr = nullptr, *p0_len = nullptr, *p0_col = nullptr;
   void* p0_val = nullptr;
@@ -1280,7 +1295,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
                   al16(i4 * (o2hi - o2lo + 1)) + al16(i4 * (s1hi - s1lo)) + 2 * al16(i4 * (s1hi - s1lo + 1)) +
                   al16(i4 * (s2hi - s2lo)) + 2 * al16(i4 * (s2hi - s2lo + 1)) + 3 * al16(i4 * (s3hi - s3lo)) +
                   al16(i4 * (c3hi - c3lo)) + al16(i4 * (c3hi - c3lo + 1)) + al16(i4 * (r3hi - r3lo + 1)) +
-                  al16(i4 * (H.g3_ptr[r3hi] - H.g3_ptr[r3lo])) + al16(i4 * (bs1 - bs0 + 1)) + al16(i4 * (bs1 - bs0));
+                  al16(i4 * (c3hi - c3lo)) + al16(i4 * (bs1 - bs0 + 1)) + al16(i4 * (bs1 - bs0));
       const size_t n01 = H.r01_ptr[o1hi] - H.r01_ptr[o1lo], n02 = H.r02_ptr[o2hi] - H.r02_ptr[o2lo];
       const size_t nj1 = H.s_jptr[1][s1hi] - H.s_jptr[1][s1lo], np1 = H.s_pptr[1][s1hi] - H.s_pptr[1][s1lo];
       const size_t nj2 = H.s_jptr[2][s2hi] - H.s_jptr[2][s2lo], np2 = H.s_pptr[2][s2hi] - H.s_pptr[2][s2lo];
@@ -1350,7 +1365,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   PFEM2_TRY(ws_upload(w, &w->c3_lk, H.c3_lk));
   PFEM2_TRY(ws_upload_r(w, c.mixed, &w->c3_val, H.c3_val));
   PFEM2_TRY(ws_upload(w, &w->g3_ptr, H.g3_ptr));
-  PFEM2_TRY(ws_upload(w, &w->g3_row, H.g3_row));
+  PFEM2_TRY(ws_upload(w, &w->c3_pos, H.c3_pos));
   {
     std::vector<double> zero(std::max<size_t>(1, H.c3_lk.size()), 0.0);
     PFEM2_TRY(ws_upload_r(w, c.mixed, &w->contrib, zero));
@@ -1437,7 +1452,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
     a.r01_ptr = w->r01_ptr; a.r01_col = w->r01_col; a.r01_val = (const R*)w->r01_val;
     a.r02_ptr = w->r02_ptr; a.r02_col = w->r02_col; a.r02_val = (const R*)w->r02_val;
     a.c3_blk = w->c3_blk; a.c3_ptr = w->c3_ptr; a.c3_col = w->c3_col; a.c3_lk = w->c3_lk;
-    a.c3_val = (const R*)w->c3_val; a.g3_ptr = w->g3_ptr; a.g3_row = w->g3_row; a.contrib = (R*)w->contrib;
+    a.c3_val = (const R*)w->c3_val; a.g3_ptr = w->g3_ptr; a.c3_pos = w->c3_pos; a.contrib = (R*)w->contrib;
     a.j0 = (const R*)w->j0;
     a.p0_ptr = w->p0_ptr; a.p0_len = w->p0_len; a.p0_col = w->p0_col; a.p0_val = (const R*)w->p0_val;
     a.blk_s1 = w->blk_s[1]; a.s1_lk = w->s_lk[1]; a.s1_jptr = w->s_jptr[1]; a.s1_jcol = w->s_jcol[1];
