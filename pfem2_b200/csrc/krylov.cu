@@ -10,10 +10,14 @@
 // positive definite after the symmetric Dirichlet elimination, so CG reaches
 // the same solution.
 //
-// The work between two bounded grid barriers is a "phase". Every block that
-// owns tiles of a system computes that system's scalars itself, from the
-// per-tile partial sums of the previous phase, in a fixed order: no block
-// publishes scalars and no phase waits for a finalizer.
+// The work between two synchronisation points is a "phase". A phase ends
+// with every tile publishing its partial sums and a release add on its
+// system's counter; the next phase starts once the counters of the block's
+// running systems show every tile of those systems done (a per-system
+// barrier: the instances of a batch do not wait for each other). Every
+// block that owns tiles of a system computes that system's scalars itself,
+// from the per-tile partial sums of the previous phase, in a fixed order:
+// no block publishes scalars and no phase waits for a finalizer.
 //
 // Jacobi-preconditioned systems (prediction, mass) take two phases per
 // iteration:
@@ -60,7 +64,7 @@ enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, 
 constexpr int kMaxBlockTiles = 64;
 
 // categories of per-block static data copied into shared memory at kernel
-// start (every grid barrier's GPU-scope fence invalidates L1, so static
+// start (every phase start's GPU-scope acquire invalidates L1, so static
 // indices read from global memory would cost an L2 round trip per phase)
 enum {
   ST_L0META = 1,  // slice pointers / lengths of the block's slice range
@@ -127,6 +131,7 @@ template <typename R> struct SolveArgs {
   R *e, *r, *z, *p, *q;
   double* r64;
   double* part;          // [2 parities][2 sums][ntiles slots]
+  unsigned* scount;      // [nsys][32]: per-system count of tile phases published (one 128-byte line each, zeroed per launch)
   int* active;
   int* out_it;           // [nsys] iterations
   double* out_res;       // [nsys] final residual norm
@@ -181,7 +186,7 @@ __device__ __forceinline__ T sell_dot(T acc, Cols cols, int base, int len, int l
 // x[col] from the shared mirror m of the block's own rows [own0, own0 +
 // nown) when there is one, else from global memory: one generic load, no
 // branch (plain loads see the other blocks' writes of the previous phase,
-// which the grid barrier's acquire ordered before them)
+// which the phase start's acquire ordered before them)
 template <typename R>
 __device__ __forceinline__ R ldm(const R* g, const R* m, int col, int own0, int nown) {
   const unsigned o = (unsigned)(col - own0);
@@ -431,20 +436,47 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
   // the phases run, the time from the end of the last barrier to the
   // arrival at the next one (work) and the wait there
   const bool prof = a.prof != nullptr && threadIdx.x == 0;
-  unsigned long long pacc[8][3] = {}, t_phase = prof ? gtimer() : 0;
+  unsigned long long pacc[8][3] = {}, t_phase = prof ? gtimer() : 0, t_arrive = 0;
   int plabel = ACT_NONE;
   for (int iter = 0;; ++iter) {
     if (iter >= a.iter_cap) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.gb.err, 2);
+      if (threadIdx.x == 0) atomicCAS(a.gb.err, 0, 2);
       break;
     }
     const bool phaseA = (iter & 1) == 0;
     const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 2;
-    // ---- sums of the previous phase's partials (warp 0, fixed order), and
-    // the count of systems still running (0: every system is done)
+    // ---- wait for the previous phase of the block's running systems: every
+    // tile adds 1 to its system's counter with a release add once its phase
+    // is written, so iter x (tiles of the system) means that every tile of
+    // the system has finished phase iter - 1; lane k polls local system k,
+    // then an acquire fence (and the block barrier) orders everything those
+    // blocks wrote before this phase's reads. Blocks of other systems are
+    // not waited for. Then the sums of the previous phase's partials (warp
+    // 0, fixed order).
     if (warp == 0) {
-      if (lane == 0) s_stop = *(volatile const int*)a.active <= 0;
-      for (int k = 0; k < nls; ++k) {
+      bool stop = true;
+      for (int k = 0; k < nls; ++k) stop &= ls[k].state == S_DONE;
+      if (!stop && iter > 0) {
+        const bool mine = lane < nls && ls[lane].state != S_DONE;
+        const unsigned target = mine ? (unsigned)iter * (unsigned)(ls[lane].t1 - ls[lane].t0) : 0u;
+        const unsigned* cnt = a.scount + (size_t)(mine ? ls[lane].sys : 0) * 32;
+        unsigned spins = 0;
+        for (;;) {
+          const bool ok = !mine || (int)(ld_relaxed_u32(cnt) - target) >= 0;
+          if (__all_sync(PFEM2_FULL_MASK, ok)) {
+            fence_acq_rel_gpu();
+            break;
+          }
+          if (__any_sync(PFEM2_FULL_MASK, ++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)a.gb.err != 0)) {
+            if (lane == 0) atomicCAS(a.gb.err, 0, 1);
+            stop = true;
+            break;
+          }
+          __nanosleep(20);
+        }
+      }
+      if (lane == 0) s_stop = stop;
+      for (int k = 0; k < nls && !stop; ++k) {
         const int st = ls[k].state;
         if (st == S_DONE || st == S_OUT_A || (st == S_UZ && !ls[k].chk)) continue;
         const int t0 = ls[k].t0, t1 = ls[k].t1;
@@ -472,6 +504,13 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
       }
     }
     __syncthreads();
+    if (prof && iter > 0) {
+      const unsigned long long tn = gtimer();
+      pacc[plabel][0] += 1;
+      pacc[plabel][1] += t_arrive - t_phase;
+      pacc[plabel][2] += tn - t_arrive;
+      t_phase = tn;
+    }
     if (s_stop) break;
     // ---- decisions (thread 0; identical in every block owning the system)
     if (threadIdx.x == 0) {
@@ -650,7 +689,11 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           const int n = ls[k].n2, o = ls[k].off2;
           for (int d = threadIdx.x; d < n; d += kSolveThreads) sb2[ls[k].b2off + d] = __ldcg(a.b2 + o + d);
           const int D = ls[k].D3, o3 = ls[k].off3;
-          for (int d0 = 4 * warp; d0 < D; d0 += 4 * kWarps) {
+          // (blocks start at different dofs, so that they do not all read
+          // the same L2 lines at the same moment)
+          const int ng4 = (D + 3) / 4, rot = (int)((blockIdx.x * 7u) % (unsigned)max(ng4, 1));
+          for (int g4 = warp; g4 < ng4; g4 += kWarps) {
+            const int d0 = 4 * ((g4 + rot) % ng4);
             R v[4][8];
             int q0[4], q1[4];
 #pragma unroll
@@ -893,17 +936,22 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     }
     __syncthreads();
     // per tile: its items' partials in order, into this phase's parity buffer
+    // and the tile's count on its system's counter (a release add: after
+    // the block barrier above it publishes every write of the block in this
+    // phase)
     for (int tl = threadIdx.x; tl < ntl; tl += kSolveThreads) {
       const Tile T = tile_at(t_lo + tl);
-      if (ls[T.lk].act == ACT_NONE) continue;
-      double s0 = 0.0, s1 = 0.0;
-      for (int it = item0[tl]; it < item0[tl + 1]; ++it) {
-        s0 += spart[2 * it];
-        s1 += spart[2 * it + 1];
+      if (ls[T.lk].act != ACT_NONE) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int it = item0[tl]; it < item0[tl + 1]; ++it) {
+          s0 += spart[2 * it];
+          s1 += spart[2 * it + 1];
+        }
+        double* dst = a.part + (size_t)(iter & 1) * a.ntiles * 2 + T.slot;
+        dst[0] = s0;
+        dst[a.ntiles] = s1;
       }
-      double* dst = a.part + (size_t)(iter & 1) * a.ntiles * 2 + T.slot;
-      dst[0] = s0;
-      dst[a.ntiles] = s1;
+      red_release_add_u32(a.scount + (size_t)T.sys * 32, 1u);
     }
     // ---- bookkeeping
     if (threadIdx.x == 0) {
@@ -922,16 +970,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         L.act = ACT_NONE;
       }
     }
-    unsigned long long t_arrive = 0;
     if (prof) t_arrive = gtimer();
-    if (!grid_sync_ra(a.gb, bar_gen)) return;
-    if (prof) {
-      const unsigned long long tn = gtimer();
-      pacc[plabel][0] += 1;
-      pacc[plabel][1] += t_arrive - t_phase;
-      pacc[plabel][2] += tn - t_arrive;
-      t_phase = tn;
-    }
   }
   if (prof)
     for (int k = 0; k < 8; ++k)
@@ -980,6 +1019,7 @@ struct KrylovWs {
   void *e = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p = nullptr;
   double* r64 = nullptr;
   double* part = nullptr;
+  unsigned* scount = nullptr;
   int* active = nullptr;
   int* out_it[3];
   double* out_res[3];
@@ -1228,6 +1268,7 @@ pfem2_status krylov_setup(Ctx& c) {
   }
   PFEM2_TRY(ws_alloc(w, &w->r64, nv * dim));
   PFEM2_TRY(ws_alloc(w, &w->part, 4 * (size_t)maxtiles));
+  PFEM2_TRY(ws_alloc(w, &w->scount, 32 * (size_t)maxsys));
   PFEM2_TRY(ws_alloc(w, &w->active, 1));
   if (getenv("PFEM2_SOLVER_PROFILE"))
     for (int k = 0; k < 3; ++k) PFEM2_TRY(ws_alloc(w, &w->prof[k], (size_t)w->grid[k == 1 ? 0 : 1] * 8 * 3));
@@ -1411,13 +1452,15 @@ pfem2_status krylov_setup_precond(Ctx& c) {
 }
 
 __global__ void k_init_solve(int nsys, int* __restrict__ active, unsigned* __restrict__ barrier,
-                             int* __restrict__ err) {
-  if (threadIdx.x == 0) {
+                             int* __restrict__ err, unsigned* __restrict__ scount, int ncount) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
     *active = nsys;
     barrier[0] = 0;
     barrier[1] = 0;
     *err = 0;
   }
+  for (int j = i; j < ncount; j += gridDim.x * blockDim.x) scount[j] = 0u;
 }
 
 template <typename R>
@@ -1495,6 +1538,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.e = (R*)w->e; a.r = (R*)w->r; a.z = (R*)w->z; a.q = (R*)w->q; a.p = (R*)w->p;
   a.r64 = w->r64;
   a.part = w->part;
+  a.scount = w->scount;
   a.active = w->active;
   a.out_it = w->out_it[which];
   a.out_res = w->out_res[which];
@@ -1507,7 +1551,8 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
   a.prof = w->prof[which];
-  k_init_solve<<<1, 32, 0, c.stream>>>(a.nsys, w->active, c.barrier, c.d_err);
+  k_init_solve<<<std::max(1, std::min(64, (32 * a.nsys + 255) / 256)), 256, 0, c.stream>>>(
+      a.nsys, w->active, c.barrier, c.d_err, w->scount, 32 * a.nsys);
   c.launches++;
   void* args[] = {&a};
   const void* kmg = w->mg_minb == 1 ? (const void*)k_krylov<R, true, 1> : (const void*)k_krylov<R, true, 2>;
@@ -1610,7 +1655,7 @@ pfem2_status krylov_read_stats(Ctx& c) {
   int err = 0;
   PFEM2_CUDA(cudaMemcpy(&err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err == 1) {
-    set_error("krylov: a grid barrier wait timed out");
+    set_error("krylov: a wait for the other blocks timed out");
     return PFEM2_TIMEOUT;
   }
   if (err == 2) {
