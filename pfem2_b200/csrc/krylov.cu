@@ -245,6 +245,9 @@ __device__ __forceinline__ SV<T> maybe_stage(bool on, unsigned char*& cur, const
 template <typename R, bool MG, int MINB>
 __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
+  // entries of a SELL row (and of a long restriction row) whose loads are
+  // issued together: more with one block per SM, which has the registers
+  constexpr int CH = MINB == 1 ? 16 : 8;
   __shared__ LocalSys ls[kMaxLocalSys];
   __shared__ Tile stile[kMaxBlockTiles];
   __shared__ int s_nls;
@@ -659,11 +662,11 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
             const R al = R(L.alpha);
             const R* rr = a.r + (size_t)L.rpar * nv;
             const R* mrr = mr[L.rpar];
-            acc = csr_dot<32, 8, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) {
+            acc = csr_dot<32, CH, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) {
               return fma_r(-al, ldm(a.q, mq, j, own0, nown), ldm(rr, mrr, j, own0, nown));
             });
           } else {
-            acc = csr_dot<32, 8, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) { return R(__ldcg(a.r64 + j)); });
+            acc = csr_dot<32, CH, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) { return R(__ldcg(a.r64 + j)); });
           }
           acc = warp_sum(acc);
           if (lane == 0) {
@@ -742,7 +745,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           const R* mrr = mr[ls[T.lk].rpar];
           {
             const int sl = T.s0 + (it - item0[tl]);
-            const R v = sell_dot<R>(
+            const R v = sell_dot<R, CH>(
                 R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return __ldg(a.j0 + ei); },
                 [&](int col) { return ldm(r, mrr, col, own0, nown); });
             if (mz) mz[sl * 32 + lane - own0] = v;
@@ -841,7 +844,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         const double* xk = a.x[k];
         {
           const int row = sl * 32 + lane;
-          const double acc = sell_dot<double>(
+          const double acc = sell_dot<double, CH>(
               0.0, SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
               [&](int col) { return __ldcg(xk + col) + (double)ldm(e, me, col, own0, nown); });
           const double rr = a.b[k][row] - acc;
@@ -874,7 +877,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         {
           const int row = sl * 32 + lane;
           const R* mpo = mp[L.par ^ 1];
-          const R acc = sell_dot<R>(
+          const R acc = sell_dot<R, CH>(
               R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
               [&](int col) { return fma_r(beta, ldm(po, mpo, col, own0, nown), ldm(z, mz, col, own0, nown)); });
           const R pp = me ? fma_r(beta, mpo[row - own0], mz[row - own0]) : fma_r(beta, po[row], z[row]);
@@ -918,7 +921,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         // z = J0 r (first stage) + Pt0 x1
         {
           const int row = sl * 32 + lane;
-          const R acc = sell_dot<R>(
+          const R acc = sell_dot<R, CH>(
               mz ? mz[row - own0] : z[row], P0C, P0P[sl], P0L[sl], lane, [&](int ei) { return P0V[ei]; },
               [&](int col) { return sx1[col]; });
           z[row] = acc;
