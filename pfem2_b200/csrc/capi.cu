@@ -587,6 +587,7 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   PFEM2_CUDA(cudaGetDeviceProperties(&prop, c.device));
   c.num_sms = prop.multiProcessorCount;
   if (const char* v = getenv("PFEM2_ADVECT_SPLIT_MIN")) c.adv_split_min = atoll(v);
+  if (const char* v = getenv("PFEM2_MG_WIDE_MIN")) c.mg_wide_min = atoll(v);
   PFEM2_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   for (int k = 0; k < 8; ++k) PFEM2_CUDA(cudaEventCreate(&c.ev[k]));
   *out = x;

@@ -161,6 +161,7 @@ struct Ctx {
   int coop_blocks = 0;
   int solve_threads = 256;
   int solve_blocks_per_sm = 1;  // persistent Krylov grid: blocks per SM
+  long long mg_wide_min = 262144;  // rows from which one pressure system runs two blocks per SM
   bool two_level = true;        // pressure: multigrid preconditioner (else Jacobi)
   double refine_eta = 1e-3;     // mixed: inner residual reduction per FP64 refinement
 

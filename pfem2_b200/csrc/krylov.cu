@@ -1098,9 +1098,11 @@ void krylov_free(Ctx& c) {
 pfem2_status krylov_setup(Ctx& c) {
   KrylovWs* w = new KrylovWs();
   c.kws = w;
-  // one system: one block per SM (its coarse lists are replicated per block,
-  // so smaller blocks cost more than their extra warps bring); a batch: two
-  w->mg_minb = c.inst.size() > 1 ? 2 : 1;
+  // one system of moderate size: one block per SM (its coarse lists are
+  // replicated per block, so smaller blocks cost more than their extra
+  // warps bring); a batch, or one system from mg_wide_min rows on (where the
+  // solve is bound by memory parallelism, not by latency): two
+  w->mg_minb = (c.inst.size() > 1 || (long long)c.nv >= c.mg_wide_min) ? 2 : 1;
   const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
   const int bps = std::max(1, c.solve_blocks_per_sm);
@@ -1114,7 +1116,7 @@ pfem2_status krylov_setup(Ctx& c) {
       // one per block of the persistent grid (balanced work), at most dcap
       // per system (a batch: tiles of ~8 slices, at most dcap per system,
       // so every instance gets a coarse space of its own size)
-      const int dcap = ni == 1 ? 160 : 96;
+      const int dcap = ni == 1 ? (w->mg_minb == 2 ? 2 * c.num_sms : 160) : 96;
       const int nb = w->mg_minb * c.num_sms;
       long long tot_sl = 0;
       for (int i = 0; i < ni; ++i) tot_sl += c.inst[i].nv_pad / kSlice;

@@ -44,6 +44,19 @@ def test_oracle_reproduces_golden(name):
 @pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
 @pytest.mark.parametrize("name", CASES)
 def test_library_matches_golden(name, prec):
+    _check_library(name, prec)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_library_matches_golden_wide_multigrid(name, monkeypatch):
+    """the pressure multigrid at two blocks per SM (a tile per block, used for
+    one large system from PFEM2_MG_WIDE_MIN rows on), forced on the small cases"""
+    monkeypatch.setenv("PFEM2_MG_WIDE_MIN", "0")
+    _check_library(name, A.PREC_MIXED)
+
+
+def _check_library(name, prec):
     from pfem2_b200.solver import Solver
 
     sp, steps = golden_cases()[name]
