@@ -272,8 +272,9 @@ bool spd_inverse(std::vector<double>& M, int n) {
 
 pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vector<int>& col,
                       const std::vector<int>& len, const std::vector<Tile>& tiles, const std::vector<int>& st0,
-                      const std::vector<int>& bt0, MgHost& H) {
+                      const std::vector<int>& bt0, bool split, MgHost& H) {
   const int ni = (int)c.inst.size(), T = (int)tiles.size(), G = (int)bt0.size() - 1;
+  H.split = split;
   const std::vector<int>& sp = c.h_sl_ptr;
   std::vector<std::vector<Level>> sysL(ni);
   std::vector<std::vector<double>> Einv(ni);
@@ -415,15 +416,22 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
   };
   for (int s = 0; s < ni; ++s) {
     std::vector<Level>& L = sysL[s];
-    const Csr P01 = spgemm(L[0].Pt2, L[1].Pt2);
     append_rows(transpose(L[0].Pt2), c.inst[s].v_off, H.r01_ptr, H.r01_col, H.r01_val);
-    append_rows(transpose(P01), c.inst[s].v_off, H.r02_ptr, H.r02_col, H.r02_val);
+    if (split) {
+      append_rows(transpose(L[1].Pt2), goff[1][s], H.q2_ptr, H.q2_col, H.q2_val);
+    } else {
+      const Csr P01 = spgemm(L[0].Pt2, L[1].Pt2);
+      append_rows(transpose(P01), c.inst[s].v_off, H.r02_ptr, H.r02_col, H.r02_val);
+    }
     H.sys_D3.push_back(L[3].A.n);
     H.sys_off3.push_back(goff[3][s]);
     H.sys_n2.push_back(L[2].A.n);
     H.sys_off2.push_back(goff[2][s]);
     H.dmax = std::max(H.dmax, L[3].A.n);
   }
+  // the restriction not in use: empty rows
+  if (split) H.r02_ptr.assign(H.n[2] + 1, 0);
+  else H.q2_ptr.assign(H.n[2] + 1, 0);
   // ---- per-block lists
   std::vector<int> sys_of_tile(T);
   for (int s = 0; s < ni; ++s)

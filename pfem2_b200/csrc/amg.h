@@ -30,9 +30,15 @@ struct MgHost {
   std::vector<int> lsys[kMgLevels];       // [l][n_l] system of each level-l dof (l >= 1)
   std::vector<int> lk[3];                 // [1..2][n_l] index of that system among its block's systems
   // restrictions from level 0 (CSR over the rows of level l, global
-  // level-0 columns): R0l = (Pt_0 ... Pt_{l-1})^T, l = 1, 2
+  // level-0 columns): R0l = (Pt_0 ... Pt_{l-1})^T, l = 1, 2; R02 only
+  // without the split restriction
   std::vector<int> r01_ptr, r01_col, r02_ptr, r02_col;
   std::vector<double> r01_val, r02_val;
+  // split restriction (large systems): b2 = Pt_1^T b1 in a phase of its
+  // own, CSR over the level-2 rows with global level-1 columns
+  bool split = false;
+  std::vector<int> q2_ptr, q2_col;
+  std::vector<double> q2_val;
   // b3 = Pt_2^T b2 in two steps: every block adds up the contributions of
   // its own level-2 rows to the level-3 dofs they touch (CSR rows c3,
   // columns = own level-2 row - first own row, grouped per block by c3_blk,
@@ -70,10 +76,11 @@ struct MgHost {
 // Builds the hierarchy of every pressure system. A, col, len: host copy of
 // the eliminated FP64 pressure matrix in the context's SELL layout; tiles,
 // st0: the pressure solve's tiles and first tile per system; bt0: first
-// tile per block of the persistent grid.
+// tile per block of the persistent grid; split: restrict to level 2 in a
+// phase of its own (b2 = Pt_1^T b1) instead of through the composite R02.
 pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vector<int>& col,
                       const std::vector<int>& len, const std::vector<Tile>& tiles, const std::vector<int>& st0,
-                      const std::vector<int>& bt0, MgHost& out);
+                      const std::vector<int>& bt0, bool split, MgHost& out);
 
 // In-place inverse of an SPD matrix (Cholesky, then L^-T L^-1); false if
 // the matrix is not SPD.

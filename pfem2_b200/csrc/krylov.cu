@@ -58,8 +58,8 @@ constexpr int kSolveThreads = 384;  // 12 warps
 constexpr int kWarps = kSolveThreads / 32;
 constexpr int kMaxLocalSys = 16;
 
-enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_UZ = 5 };
-enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_UZ = 6 };
+enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_UZ = 5, S_B2 = 6 };
+enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_UZ = 6, ACT_B2 = 7 };
 
 constexpr int kMaxBlockTiles = 64;
 
@@ -106,6 +106,9 @@ template <typename R> struct SolveArgs {
   const int *lk1, *lk2;                 // local system index of each level-1/2 dof (in its owner block)
   const int *r01_ptr, *r01_col, *r02_ptr, *r02_col;
   const R *r01_val, *r02_val;
+  int split;                            // restriction to level 2 in a phase of its own (B2)
+  const int *q2_ptr, *q2_col;           // split: Pt1^T per level-2 row, global level-1 columns
+  const R* q2_val;
   const int *c3_blk, *c3_ptr, *c3_col, *c3_lk, *g3_ptr, *c3_pos;
   const R* c3_val;
   R* contrib;                           // [c3 rows] contributions to b3
@@ -222,6 +225,7 @@ struct LocalSys {
   int t0, t1;                       // partial slots of the system
   int D3, off3, n2, off2, b2off;    // multigrid: coarse sizes and offsets
   double tol, intol, res, rz_prev, alpha, beta;
+  double rr_b;                      // split restriction: r'.r' of the B phase, for the UZ decision
   double sum[2];
 };
 
@@ -342,9 +346,9 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
   const SV<int> SLl = maybe_stage<int>(a.stage & ST_L0META, cur, a.sl_len, bs0, bs1);
   const SV<int> SLc = maybe_stage<int>(a.stage & ST_L0COL, cur, a.sl_col, a.sl_ptr[bs0], a.sl_ptr[bs1]);
   int s1_lo = 0, s1_hi = 0, s2_lo = 0, s2_hi = 0, s3_lo = 0, s3_hi = 0, o1lo = 0, o1hi = 0, o2lo = 0, o2hi = 0;
-  SV<int> LK1{}, LK2{}, R01P{}, R01C{}, R02P{}, R02C{}, S1K{}, J1P{}, J1C{}, P1P{}, P1C{}, S2K{}, J2P{}, J2C{}, P2P{},
+  SV<int> LK1{}, LK2{}, R01P{}, R01C{}, R02P{}, R02C{}, Q2P{}, Q2C{}, S1K{}, J1P{}, J1C{}, P1P{}, P1C{}, S2K{}, J2P{}, J2C{}, P2P{},
       P2C{}, S3K{}, S3E{}, S3S{}, C3K{}, C3P{}, C3Q{}, C3C{}, G3P{}, P0P{}, P0L{}, P0C{};
-  SV<R> P1V{}, J2V{}, P2V{}, C3V{}, P0V{};
+  SV<R> P1V{}, J2V{}, P2V{}, C3V{}, P0V{}, Q2V{};
   int c3lo = 0, c3hi = 0;
   if (MG) {
     s1_lo = a.blk_s1[blockIdx.x];
@@ -368,6 +372,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     R01P = maybe_stage<int>(si, cur, a.r01_ptr, o1lo, o1hi + 1);
     LK2 = maybe_stage<int>(si, cur, a.lk2, o2lo, o2hi);
     R02P = maybe_stage<int>(si, cur, a.r02_ptr, o2lo, o2hi + 1);
+    Q2P = maybe_stage<int>(si, cur, a.q2_ptr, o2lo, o2hi + 1);
     S1K = maybe_stage<int>(si, cur, a.s1_lk, s1_lo, s1_hi);
     J1P = maybe_stage<int>(si, cur, a.s1_jptr, s1_lo, s1_hi + 1);
     P1P = maybe_stage<int>(si, cur, a.s1_pptr, s1_lo, s1_hi + 1);
@@ -385,6 +390,8 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     P0L = maybe_stage<int>(si, cur, a.p0_len, bs0, bs1);
     R01C = maybe_stage<int>(sc, cur, a.r01_col, a.r01_ptr[o1lo], a.r01_ptr[o1hi]);
     R02C = maybe_stage<int>(sc, cur, a.r02_col, a.r02_ptr[o2lo], a.r02_ptr[o2hi]);
+    Q2C = maybe_stage<int>(sc, cur, a.q2_col, a.q2_ptr[o2lo], a.q2_ptr[o2hi]);
+    Q2V = maybe_stage<R>(sc, cur, a.q2_val, a.q2_ptr[o2lo], a.q2_ptr[o2hi]);
     J1C = maybe_stage<int>(sc, cur, a.s1_jcol, a.s1_jptr[s1_lo], a.s1_jptr[s1_hi]);
     P1C = maybe_stage<int>(sc, cur, a.s1_pcol, a.s1_pptr[s1_lo], a.s1_pptr[s1_hi]);
     J2C = maybe_stage<int>(sc, cur, a.s2_jcol, a.s2_jptr[s2_lo], a.s2_jptr[s2_hi]);
@@ -481,7 +488,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
       if (lane == 0) s_stop = stop;
       for (int k = 0; k < nls && !stop; ++k) {
         const int st = ls[k].state;
-        if (st == S_DONE || st == S_OUT_A || (st == S_UZ && !ls[k].chk)) continue;
+        if (st == S_DONE || st == S_OUT_A || (st == S_UZ && (!ls[k].chk || a.split))) continue;
         const int t0 = ls[k].t0, t1 = ls[k].t1;
         double s0 = 0.0, s1 = 0.0;
         for (int tb = t0; tb < t1; tb += 256) {
@@ -575,11 +582,16 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
                 L.first = 1;  // CG restarts from the true residual
                 L.chk = 0;
                 act = ACT_OUT_B;
-                L.state = S_UZ;
+                L.state = a.split ? S_B2 : S_UZ;
               }
               break;
+            case S_B2:
+              L.rr_b = L.sum[0];
+              act = ACT_B2;
+              L.state = S_UZ;
+              break;
             case S_UZ: {
-              const double rr = sqrt(L.sum[0]);
+              const double rr = sqrt(a.split ? L.rr_b : L.sum[0]);
               if (L.chk && (rr <= L.intol || L.it >= L.maxit || !(rr == rr))) {
                 act = ACT_OUT_A;  // reliable update in FP64
                 L.state = S_OUT_B;
@@ -603,7 +615,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
               L.it += 1;
               L.chk = 1;
               act = ACT_B;
-              L.state = S_UZ;
+              L.state = a.split ? S_B2 : S_UZ;
               break;
             default:
               break;
@@ -616,12 +628,15 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     __syncthreads();
     // ---- coarse-level work of the block (multigrid; pressure = component 0)
     if (MG) {
-      bool any_b = false, any_uz = false;
+      bool any_b = false, any_uz = false, any_b2 = false;
       for (int k = 0; k < nls; ++k) {
         const int act = ls[k].act;
         any_b |= act == ACT_B || act == ACT_OUT_B;
         any_uz |= act == ACT_UZ;
+        any_b2 |= act == ACT_B2;
       }
+      // the phase that computes b2 and the contributions to b3
+      const auto b2_act = [&](int act) { return a.split ? act == ACT_B2 : (act == ACT_B || act == ACT_OUT_B); };
       if (any_b) {
         // b_l = R0l r' on the own level-l rows; after a reliable update
         // r' = r64, else r' = r - alpha q formed on the fly. Level 1: 8 lanes
@@ -652,22 +667,39 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
             if (sub == 0 && (act == ACT_B || act == ACT_OUT_B)) a.b1[i] = acc;
           }
         }
+        if (!a.split) {
+          for (int i = o2lo + warp; i < o2hi; i += kWarps) {
+            const LocalSys& L = ls[LK2[i]];
+            const int act = L.act;
+            if (act != ACT_B && act != ACT_OUT_B) continue;
+            const int k0 = R02P[i], k1 = R02P[i + 1];
+            R acc = R(0);
+            if (act == ACT_B) {
+              const R al = R(L.alpha);
+              const R* rr = a.r + (size_t)L.rpar * nv;
+              const R* mrr = mr[L.rpar];
+              acc = csr_dot<32, CH, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) {
+                return fma_r(-al, ldm(a.q, mq, j, own0, nown), ldm(rr, mrr, j, own0, nown));
+              });
+            } else {
+              acc = csr_dot<32, CH, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) { return R(__ldcg(a.r64 + j)); });
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) {
+              a.b2[i] = acc;
+              sb2o[i - o2lo] = acc;
+            }
+          }
+          __syncthreads();
+        }
+      }
+      if (any_b2) {
+        // split restriction: b2 = Pt1^T b1 on the own level-2 rows (a warp
+        // per row, b1 of the whole system from the previous phase)
         for (int i = o2lo + warp; i < o2hi; i += kWarps) {
           const LocalSys& L = ls[LK2[i]];
-          const int act = L.act;
-          if (act != ACT_B && act != ACT_OUT_B) continue;
-          const int k0 = R02P[i], k1 = R02P[i + 1];
-          R acc = R(0);
-          if (act == ACT_B) {
-            const R al = R(L.alpha);
-            const R* rr = a.r + (size_t)L.rpar * nv;
-            const R* mrr = mr[L.rpar];
-            acc = csr_dot<32, CH, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) {
-              return fma_r(-al, ldm(a.q, mq, j, own0, nown), ldm(rr, mrr, j, own0, nown));
-            });
-          } else {
-            acc = csr_dot<32, CH, R>(acc, k0, k1, lane, R02C, R02V, [&](int j) { return R(__ldcg(a.r64 + j)); });
-          }
+          if (L.act != ACT_B2) continue;
+          R acc = csr_dot<32, CH, R>(R(0), Q2P[i], Q2P[i + 1], lane, Q2C, Q2V, [&](int c) { return __ldcg(a.b1 + c); });
           acc = warp_sum(acc);
           if (lane == 0) {
             a.b2[i] = acc;
@@ -675,10 +707,11 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           }
         }
         __syncthreads();
+      }
+      if (any_b2 || (any_b && !a.split)) {
         // contributions of the own level-2 rows to b3 (thread per row)
         for (int rr = c3lo + threadIdx.x; rr < c3hi; rr += kSolveThreads) {
-          const int act = ls[C3K[rr]].act;
-          if (act != ACT_B && act != ACT_OUT_B) continue;
+          if (!b2_act(ls[C3K[rr]].act)) continue;
           a.contrib[C3Q[rr]] = csr_dot<1, 4, R>(R(0), C3P[rr], C3P[rr + 1], 0, C3C, C3V, [&](int c) { return sb2o[c]; });
         }
       }
@@ -1008,6 +1041,9 @@ struct KrylovWs {
   long long mg_sizes[12] = {};           // see pfem2_solver_sizes
   int *toff[4] = {}, *lk[3] = {};
   int *r01_ptr = nullptr, *r01_col = nullptr, *r02_ptr = nullptr, *r02_col = nullptr;
+  int *q2_ptr = nullptr, *q2_col = nullptr;
+  void* q2_val = nullptr;
+  bool split = false;
   void *r01_val = nullptr, *r02_val = nullptr, *j0 = nullptr;
   int *c3_blk = nullptr, *c3_ptr = nullptr, *c3_col = nullptr, *c3_lk = nullptr, *g3_ptr = nullptr, *c3_pos = nullptr;
   void *c3_val = nullptr, *contrib = nullptr;
@@ -1303,7 +1339,13 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   PFEM2_CUDA(cudaMemcpy(col.data(), c.sl_col, sizeof(int) * c.nell, cudaMemcpyDeviceToHost));
   PFEM2_CUDA(cudaMemcpy(len.data(), c.sl_len, sizeof(int) * c.nslices, cudaMemcpyDeviceToHost));
   MgHost H;
-  PFEM2_TRY(mg_build(c, A, col, len, w->h_tiles0, w->h_sys_t0_0, w->h_blk_t0_0, H));
+  // large systems restrict to level 2 in a phase of their own: the composite
+  // R02 of the twice-smoothed prolongators grows faster than the extra
+  // synchronisation costs (3D pipe: 52M entries against Pt1's few million)
+  long long nvmax = 0;
+  for (const HostInst& in : c.inst) nvmax = std::max<long long>(nvmax, in.nv);
+  w->split = nvmax >= c.mg_wide_min;
+  PFEM2_TRY(mg_build(c, A, col, len, w->h_tiles0, w->h_sys_t0_0, w->h_blk_t0_0, w->split, H));
   const size_t rs = c.mixed ? sizeof(float) : sizeof(double);
   w->dmax = H.dmax;
   w->s1max = H.s1max;
@@ -1341,12 +1383,14 @@ pfem2_status krylov_setup_precond(Ctx& c) {
                   al16(i4 * (o2hi - o2lo + 1)) + al16(i4 * (s1hi - s1lo)) + 2 * al16(i4 * (s1hi - s1lo + 1)) +
                   al16(i4 * (s2hi - s2lo)) + 2 * al16(i4 * (s2hi - s2lo + 1)) + 3 * al16(i4 * (s3hi - s3lo)) +
                   al16(i4 * (c3hi - c3lo)) + al16(i4 * (c3hi - c3lo + 1)) + al16(i4 * (r3hi - r3lo + 1)) +
-                  al16(i4 * (c3hi - c3lo)) + al16(i4 * (bs1 - bs0 + 1)) + al16(i4 * (bs1 - bs0));
+                  al16(i4 * (c3hi - c3lo)) + al16(i4 * (bs1 - bs0 + 1)) + al16(i4 * (bs1 - bs0)) +
+                  al16(i4 * (o2hi - o2lo + 1));
       const size_t n01 = H.r01_ptr[o1hi] - H.r01_ptr[o1lo], n02 = H.r02_ptr[o2hi] - H.r02_ptr[o2lo];
+      const size_t nq2 = H.q2_ptr[o2hi] - H.q2_ptr[o2lo];
       const size_t nj1 = H.s_jptr[1][s1hi] - H.s_jptr[1][s1lo], np1 = H.s_pptr[1][s1hi] - H.s_pptr[1][s1lo];
       const size_t nj2 = H.s_jptr[2][s2hi] - H.s_jptr[2][s2lo], np2 = H.s_pptr[2][s2hi] - H.s_pptr[2][s2lo];
       const size_t n23 = H.c3_ptr[c3hi] - H.c3_ptr[c3lo], np0 = H.p0_ptr[bs1] - H.p0_ptr[bs0];
-      const size_t bc = al16(i4 * n01) + al16(i4 * n02) + al16(i4 * nj1) + al16(i4 * np1) + al16(i4 * nj2) +
+      const size_t bc = al16(i4 * n01) + al16(i4 * n02) + al16(i4 * nq2) + al16(rs * nq2) + al16(i4 * nj1) + al16(i4 * np1) + al16(i4 * nj2) +
                         al16(i4 * np2) + al16(i4 * n23) + al16(i4 * np0);
       const size_t bv = al16(rs * np1) + al16(rs * nj2) + al16(rs * np2) + al16(rs * n23) + al16(rs * np0);
       idx = std::max(idx, bi);
@@ -1380,13 +1424,15 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   {
     char buf[512];
     snprintf(buf, sizeof(buf),
-             "multigrid: dofs %d %d %d %d; per block max lists S1 %d S2 %d S3 %d; nnz R01 %zu R02 %zu C3 %zu "
+             "multigrid: dofs %d %d %d %d; per block max lists S1 %d S2 %d S3 %d; nnz R01 %zu R02/Pt1^T %zu C3 %zu "
              "J1 %zu P1 %zu J2 %zu P2 %zu P0 %zu; staged 0x%x, %zu bytes of shared memory\n",
-             c.nv, H.n[1], H.n[2], H.n[3], H.s1max, H.s2max, H.s3max, H.r01_col.size(), H.r02_col.size(),
+             c.nv, H.n[1], H.n[2], H.n[3], H.s1max, H.s2max, H.s3max, H.r01_col.size(),
+             w->split ? H.q2_col.size() : H.r02_col.size(),
              H.c3_col.size(), H.s_jcol[1].size(), H.s_pcol[1].size(), H.s_jcol[2].size(), H.s_pcol[2].size(),
              H.p0_col.size(), stage, smem);
     w->mg_info = buf;
-    const long long sz[12] = {c.nv, H.n[1], H.n[2], H.n[3], (long long)H.r01_col.size(), (long long)H.r02_col.size(),
+    const long long sz[12] = {c.nv, H.n[1], H.n[2], H.n[3], (long long)H.r01_col.size(),
+                              (long long)(w->split ? H.q2_col.size() : H.r02_col.size()),
                               (long long)H.c3_col.size(), (long long)H.p0_col.size(), (long long)H.s_jcol[1].size(),
                               (long long)H.s_pcol[1].size(), (long long)H.s_jcol[2].size(),
                               (long long)H.s_pcol[2].size()};
@@ -1404,6 +1450,9 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r01_val, H.r01_val));
   PFEM2_TRY(ws_upload(w, &w->r02_ptr, H.r02_ptr));
   PFEM2_TRY(ws_upload(w, &w->r02_col, H.r02_col));
+  PFEM2_TRY(ws_upload(w, &w->q2_ptr, H.q2_ptr));
+  PFEM2_TRY(ws_upload(w, &w->q2_col, H.q2_col));
+  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->q2_val, H.q2_val));
   PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r02_val, H.r02_val));
   PFEM2_TRY(ws_upload(w, &w->c3_blk, H.c3_blk));
   PFEM2_TRY(ws_upload(w, &w->c3_ptr, H.c3_ptr));
@@ -1499,6 +1548,8 @@ static pfem2_status solve_impl(Ctx& c, int which) {
     a.lk1 = w->lk[1]; a.lk2 = w->lk[2];
     a.r01_ptr = w->r01_ptr; a.r01_col = w->r01_col; a.r01_val = (const R*)w->r01_val;
     a.r02_ptr = w->r02_ptr; a.r02_col = w->r02_col; a.r02_val = (const R*)w->r02_val;
+    a.split = w->split ? 1 : 0;
+    a.q2_ptr = w->q2_ptr; a.q2_col = w->q2_col; a.q2_val = (const R*)w->q2_val;
     a.c3_blk = w->c3_blk; a.c3_ptr = w->c3_ptr; a.c3_col = w->c3_col; a.c3_lk = w->c3_lk;
     a.c3_val = (const R*)w->c3_val; a.g3_ptr = w->g3_ptr; a.c3_pos = w->c3_pos; a.contrib = (R*)w->contrib;
     a.j0 = (const R*)w->j0;
@@ -1551,7 +1602,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.eta = c.mixed ? c.refine_eta : 0.0;
   int mx = 0;
   for (auto& in : c.inst) mx = std::max(mx, in.cs.max_iter > 0 ? in.cs.max_iter : 10000);
-  a.iter_cap = (mg ? 3 : 2) * mx + 256;
+  a.iter_cap = (mg ? (w->split ? 4 : 3) : 2) * mx + 256;
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
@@ -1622,7 +1673,7 @@ std::string krylov_profile(Ctx& c) {
   std::string out;
   if (!w) return out;
   static const char* kind[3] = {"prediction", "pressure", "correction"};
-  static const char* act[8] = {"-", "out_a", "out_b", "out_done", "a", "b", "uz", "-"};
+  static const char* act[8] = {"-", "out_a", "out_b", "out_done", "a", "b", "uz", "b2"};
   out += w->mg_info;
   for (int k = 0; k < 3; ++k) {
     if (!w->prof[k]) continue;
