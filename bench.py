@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--stress-n", type=int, default=2048, help="particle-stress mesh: n x n cells (0 = skip)")
     ap.add_argument("--ensemble-n", type=int, default=64, help="instances of the batched leg (0 = skip)")
+    ap.add_argument("--pipe-n", type=int, default=64,
+                    help="3D pipe leg: n x n x 4n hex cells, mixed and FP64 (0 = skip)")
     ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of the stress and ensemble legs")
     return ap.parse_args()
 
@@ -125,6 +127,14 @@ def peaks():
         d = json.load(open(p))
         return d["hbm_gbs"], "measured"
     return 6650.0, "fallback"
+
+
+# DRAM bytes (read + write) of one pressure-solve launch of the channel
+# workload per CG iteration, from the ncu capture summarised in
+# profiles/krylov_channel_disk.md (49 iterations, 32.97 MB read + 0.42 MB
+# written); the solve's working set stays in L2, so DRAM traffic is far
+# below the algorithmic bytes
+KRYLOV_DRAM_BYTES_PER_ITER = (32.973824e6 + 0.421120e6) / 49
 
 
 def pressure_solve_bytes(s, iters, outer):
@@ -264,6 +274,7 @@ def run_ours(args, rank, world, local):
         m2.close()
 
     stress = stress_leg(args, local, flush) if args.stress_n > 0 else None
+    pipe = pipe_leg(args, local, flush) if args.pipe_n > 0 else None
     ensemble = None
     if args.ensemble_n > 0:
         ensemble = ensemble_leg(args, rank, world, local, flush, fp64["timesteps_per_s"] if fp64 else None)
@@ -294,12 +305,16 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "kernel": "k_krylov<float> (pressure solve)",
                      "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None,
-                     "traffic": None, "algorithmic_bytes_per_step": ps_bytes / args.steps},
+                     "traffic": KRYLOV_DRAM_BYTES_PER_ITER * it_p / args.steps,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one channel pressure-solve "
+                                       "launch, per CG iteration, times the timed iterations per step",
+                     "algorithmic_bytes_per_step": ps_bytes / args.steps},
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clk,
         "fp64": fp64,
         "particle_stress": stress,
+        "pipe_3d": pipe,
         "ensemble": ensemble,
         "cpu_baseline": cpu,
     }
@@ -326,6 +341,49 @@ def timed_steps(solver, stream, flush, steps):
         e1.synchronize()
         tot += e0.elapsed_time(e1)
     return tot
+
+
+def pipe_leg(args, local, flush):
+    """3D pipe Poiseuille (hex mesh n x n x 4n, 3x3x3 particles per cell,
+    dp/dn driven): the mixed path (FP32 inner solves, FP64 refinement) and
+    the plain FP64 path on the same steps, one context after the other"""
+    import torch
+
+    from pfem2_b200 import _abi as A
+    from pfem2_b200 import cases
+    from pfem2_b200.solver import STAGE_NAMES, Solver
+
+    n = args.pipe_n
+    sp = cases.pipe_3d(ny=n, nz=n, nx=4 * n)
+    k, warm = args.extra_steps, 2
+    out = {"workload": f"3D pipe Poiseuille, circular section mapped from a square, {n}x{n}x{4 * n} Q1 hex cells, "
+                       f"nu=0.01, dt=0.001, dp/dn=1, 3x3x3 particles/cell",
+           "cells": sp.mesh.n_cells, "vertices": sp.mesh.n_vertices, "steps": k, "warmup": warm}
+    fields = {}
+    for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        s = Solver(sp, precision=prec, device=local, use_graph=True)
+        s.seed_particles(sp.q, sp.seed, sp.jitter)
+        stream = torch.cuda.ExternalStream(s.stream(), device=local)
+        for _ in range(warm):
+            s.step()
+        s.synchronize()
+        s.enable_stage_timing(True)
+        s.stage_times(reset=True)
+        ms = timed_steps(s, stream, flush, k)
+        stages = s.stage_times()
+        st = s.stats()
+        out[name] = {"timesteps_per_s": k / (ms / 1e3), "ms_per_step": ms / k,
+                     "stage_ms_per_step": {nm: stages[i] / k for i, nm in enumerate(STAGE_NAMES)},
+                     "pressure_cg_iters_last_step": st["iters"][3], "particles": st["n_particles"]}
+        if name == "mixed":
+            out["particle_updates_per_s"] = st["n_particles"] / (ms / k / 1e3)
+        fields[name] = [s.field(f) for f in (A.FIELD_VX, A.FIELD_P)]
+        s.close()
+    out["mixed_vs_fp64_rel_l2"] = {
+        nm: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        for nm, a, b in zip(("vx", "p"), fields["mixed"], fields["fp64"])}
+    out["mixed_over_fp64"] = out["mixed"]["timesteps_per_s"] / out["fp64"]["timesteps_per_s"]
+    return out
 
 
 def stress_leg(args, local, flush):
@@ -359,12 +417,12 @@ def stress_leg(args, local, flush):
     nc, nv = sp.mesh.n_cells, sp.mesh.n_vertices
     hbm, kind = peaks()
     # algorithmic bytes (FP32 SoA): advect reads cell+xi+u (20 B) and writes
-    # xi+u+newcell (20 B) per particle; the rebin passes read newcell (4 B),
-    # then newcell+xi+u (20 B) and write cell+xi+u (20 B) per particle plus
-    # 2 offsets and 48 B of projection partials per cell; the node gather
-    # reads the partials and writes 12 B per node.
+    # xi+u+newcell (20 B) per particle; the rebin reads newcell+xi+u (20 B)
+    # and writes cell+xi+u (20 B) per particle plus 2 offsets and 48 B of
+    # projection partials per cell; the node gather reads the partials and
+    # writes 12 B per node.
     b_adv = 40.0 * npart
-    b_reb = 44.0 * npart + (8 + 48) * nc
+    b_reb = 40.0 * npart + (8 + 48) * nc
     b_nod = 48.0 * nc + 28.0 * nv
     adv_ms = stages[STAGE_NAMES.index("advect")] / k
     reb_ms = stages[STAGE_NAMES.index("rebin")] / k

@@ -272,7 +272,7 @@ bool spd_inverse(std::vector<double>& M, int n) {
 
 pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vector<int>& col,
                       const std::vector<int>& len, const std::vector<Tile>& tiles, const std::vector<int>& st0,
-                      const std::vector<int>& bt0, bool split, MgHost& H) {
+                      const std::vector<int>& bt0, bool split, int coarse_max, MgHost& H) {
   const int ni = (int)c.inst.size(), T = (int)tiles.size(), G = (int)bt0.size() - 1;
   H.split = split;
   const std::vector<int>& sp = c.h_sl_ptr;
@@ -347,8 +347,8 @@ pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vec
           V.J.val[e] = -V.w * V.w * V.dinv[i] * V.A.val[e] * V.dinv[j] + (i == j ? 2.0 * V.w * V.dinv[i] : 0.0);
         }
       std::vector<int> agg;
-      // the coarsest level: groups of tiles, at most kMgCoarseMax unknowns per system
-      const int ntl = st0[s + 1] - st0[s], per = (ntl + kMgCoarseMax - 1) / kMgCoarseMax;
+      // the coarsest level: groups of tiles, at most coarse_max unknowns per system
+      const int ntl = st0[s + 1] - st0[s], per = (ntl + coarse_max - 1) / coarse_max;
       const int na = l < kMgLevels - 2 ? aggregate(V.A, V.tile, agg) : tile_aggregate(V.A, V.tile, st0[s], per, agg);
       if (na == 0) {
         set_error("amg: aggregation produced no coarse unknowns");

@@ -22,7 +22,6 @@
 namespace pfem2 {
 
 constexpr int kMgLevels = 4;
-constexpr int kMgCoarseMax = 160;  // level-3 unknowns per system at most
 
 struct MgHost {
   int n[kMgLevels] = {0, 0, 0, 0};        // dofs per level over all systems
@@ -77,10 +76,12 @@ struct MgHost {
 // the eliminated FP64 pressure matrix in the context's SELL layout; tiles,
 // st0: the pressure solve's tiles and first tile per system; bt0: first
 // tile per block of the persistent grid; split: restrict to level 2 in a
-// phase of its own (b2 = Pt_1^T b1) instead of through the composite R02.
+// phase of its own (b2 = Pt_1^T b1) instead of through the composite R02;
+// coarse_max: level-3 unknowns per system at most (groups of tiles share
+// one), which bounds the dense inverse rows a block holds in shared memory.
 pfem2_status mg_build(const Ctx& c, const std::vector<double>& A, const std::vector<int>& col,
                       const std::vector<int>& len, const std::vector<Tile>& tiles, const std::vector<int>& st0,
-                      const std::vector<int>& bt0, bool split, MgHost& out);
+                      const std::vector<int>& bt0, bool split, int coarse_max, MgHost& out);
 
 // In-place inverse of an SPD matrix (Cholesky, then L^-T L^-1); false if
 // the matrix is not SPD.

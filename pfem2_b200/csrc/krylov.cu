@@ -1345,7 +1345,10 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   long long nvmax = 0;
   for (const HostInst& in : c.inst) nvmax = std::max<long long>(nvmax, in.nv);
   w->split = nvmax >= c.mg_wide_min;
-  PFEM2_TRY(mg_build(c, A, col, len, w->h_tiles0, w->h_sys_t0_0, w->h_blk_t0_0, w->split, H));
+  // the dense level-3 inverse rows of a block (up to coarse_max^2 floats)
+  // must leave room in the two-blocks-per-SM shared-memory budget
+  const int coarse_max = w->mg_minb == 1 ? 160 : 128;
+  PFEM2_TRY(mg_build(c, A, col, len, w->h_tiles0, w->h_sys_t0_0, w->h_blk_t0_0, w->split, coarse_max, H));
   const size_t rs = c.mixed ? sizeof(float) : sizeof(double);
   w->dmax = H.dmax;
   w->s1max = H.s1max;

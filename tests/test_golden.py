@@ -48,12 +48,14 @@ def test_library_matches_golden(name, prec):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
 @pytest.mark.parametrize("name", CASES)
-def test_library_matches_golden_wide_multigrid(name, monkeypatch):
-    """the pressure multigrid at two blocks per SM (a tile per block, used for
-    one large system from PFEM2_MG_WIDE_MIN rows on), forced on the small cases"""
+def test_library_matches_golden_wide_multigrid(name, prec, monkeypatch):
+    """the pressure multigrid of one large system (from PFEM2_MG_WIDE_MIN rows
+    on: two blocks per SM, a tile per block, the restriction to level 2 in a
+    phase of its own), forced on the small cases"""
     monkeypatch.setenv("PFEM2_MG_WIDE_MIN", "0")
-    _check_library(name, A.PREC_MIXED)
+    _check_library(name, prec)
 
 
 def _check_library(name, prec):
