@@ -310,6 +310,7 @@ static pfem2_status do_setup(Ctx& c) {
     d.open_mask = in.cs.open_boundary_mask;
     d.q[0] = d.q[1] = d.q[2] = 1;
     d.h[0] = d.h[1] = d.h[2] = 1.0;
+    d.qm[0] = d.qm[1] = d.qm[2] = 1ull << 32;
     d.max_per_part = c.cfg.max_particles_per_cell_part;
     d.dt_sub = in.cs.dt / c.cfg.movement_steps;
     d.v_off = in.v_off; d.nv_pad = in.nv_pad; d.c_off = in.c_off; d.nc = in.nc;
@@ -684,6 +685,7 @@ pfem2_status pfem2_seed(pfem2_ctx* x, int32_t instance, const uint32_t q[3], uin
       for (int d = 0; d < 3; ++d) {
         c.h_inst[i].q[d] = (int)c.inst[i].q[d];
         c.h_inst[i].h[d] = 1.0 / c.h_inst[i].q[d];
+        c.h_inst[i].qm[d] = ((1ull << 32) + c.h_inst[i].q[d] - 1) / c.h_inst[i].q[d];
       }
     }
   for (auto& in : c.inst)

@@ -23,6 +23,7 @@ struct DevInst {
   unsigned open_mask;
   int q[3];
   double h[3];  // sub-cell widths 1.0 / q of check_cell_for_empty_parts
+  unsigned long long qm[3];  // ceil(2^32 / q): t / q = (t * qm) >> 32 exactly for t, q < 2^16
   int max_per_part;
   int v_off, nv_pad, c_off, nc;
 };

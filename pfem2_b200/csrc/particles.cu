@@ -655,12 +655,33 @@ __device__ __forceinline__ void proj_store(ProjAcc<DIM, R>& acc, R* __restrict__
 // h = 1.0 / q, which is q for xi == 1 (a bucket of its own, as in the
 // reference); clamped to [0, q]. xi * q has the same integer part unless it
 // lies within rounding of an integer, and only there the quotient is formed.
-__device__ __forceinline__ int sub_bucket(double xi, double h, int q) {
+// For FP32 coordinates xi * q is exact in FP64, so that happens only when
+// it is an integer; for FP64 coordinates a relative 1e-12 decides.
+template <typename R>
+__device__ __forceinline__ int sub_bucket(R xr, double h, int q) {
+  const double xi = (double)xr;
   double t = xi * (double)q;
-  if (fabs(t - rint(t)) <= 1e-12 * fmax(1.0, fabs(t))) t = xi / h;
+  if (sizeof(R) == 4) {
+    if (t == rint(t)) t = xi / h;
+  } else if (fabs(t - rint(t)) <= 1e-12 * fmax(1.0, fabs(t))) {
+    t = xi / h;
+  }
   if (!(t >= 0.0)) t = 0.0;
   if (t > (double)q) t = (double)q;
   return (int)(unsigned)t;
+}
+
+// t / q for t, q < 2^16 with qm = ceil(2^32 / q)
+__device__ __forceinline__ int div_small(int t, unsigned long long qm) {
+  return (int)(((unsigned long long)(unsigned)t * qm) >> 32);
+}
+
+// (i, j, k) of sub-cell t in (i, j, k) order with extents (q0, q1, q2)
+__device__ __forceinline__ void sub_cell_ijk(int t, int q1, int q2, const unsigned long long* qm, int id[3]) {
+  const int u = div_small(t, qm[2]);  // t / q2
+  id[2] = t - u * q2;
+  id[0] = div_small(u, qm[1]);        // t / (q1 q2)
+  id[1] = u - id[0] * q1;
 }
 
 __device__ __forceinline__ int far_lower_bound(const unsigned long long* keys, int n, unsigned long long k) {
@@ -800,9 +821,9 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
         const int p = active ? list[i] : -1;
         int bi = -1;
         if (active) {
-          const int b0 = sub_bucket((double)oxi[p], h0, q0);
-          const int b1 = sub_bucket((double)oxi[cap + p], h1, q1);
-          const int b2 = DIM == 3 ? sub_bucket((double)oxi[2 * cap + p], h2, q2) : 0;
+          const int b0 = sub_bucket<R>(oxi[p], h0, q0);
+          const int b1 = sub_bucket<R>(oxi[cap + p], h1, q1);
+          const int b2 = DIM == 3 ? sub_bucket<R>(oxi[2 * cap + p], h2, q2) : 0;
           bi = (b0 * nb1 + b1) * nb2 + b2;
         }
         const unsigned peers = __match_any_sync(PFEM2_FULL_MASK, bi);
@@ -827,7 +848,9 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
         const int t = base + lane;
         bool e = false;
         if (t < Q) {
-          const int i0 = t / (q1 * q2), i1 = (t / q2) % q1, i2 = t % q2;
+          int ijk[3];
+          sub_cell_ijk(t, q1, q2, I.qm, ijk);
+          const int i0 = ijk[0], i1 = ijk[1], i2 = ijk[2];
           e = bcnt[(i0 * nb1 + i1) * nb2 + i2] == 0;
         }
         const unsigned em = __ballot_sync(PFEM2_FULL_MASK, e);
@@ -918,7 +941,8 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
           }
         } else {
           const int t = -1 - code;
-          const int id[3] = {t / (q1 * q2), (t / q2) % q1, t % q2};
+          int id[3];
+          sub_cell_ijk(t, q1, q2, I.qm, id);
           const double hh[3] = {h0, h1, h2};
 #pragma unroll
           for (int d = 0; d < DIM; ++d) x[d] = R((id[d] + 1.0 / 2) * hh[d]);
