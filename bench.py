@@ -275,6 +275,7 @@ def run_ours(args, rank, world, local):
 
     stress = stress_leg(args, local, flush) if args.stress_n > 0 else None
     pipe = pipe_leg(args, local, flush) if args.pipe_n > 0 else None
+    extras = extras_leg(args, local, flush)
     ensemble = None
     if args.ensemble_n > 0:
         ensemble = ensemble_leg(args, rank, world, local, flush, fp64["timesteps_per_s"] if fp64 else None)
@@ -315,6 +316,7 @@ def run_ours(args, rank, world, local):
         "fp64": fp64,
         "particle_stress": stress,
         "pipe_3d": pipe,
+        "vorticity_and_wall_pushback": extras,
         "ensemble": ensemble,
         "cpu_baseline": cpu,
     }
@@ -341,6 +343,57 @@ def timed_steps(solver, stream, flush, steps):
         e1.synchronize()
         tot += e0.elapsed_time(e1)
     return tot
+
+
+def extras_leg(args, local, flush):
+    """the kernels beyond the time step on the channel workload: the nodal
+    vorticity (calculate_vorticity) and the wall push-back after the
+    projection (its cost read from the projection stage, flag on vs off)"""
+    import torch
+
+    from pfem2_b200 import _abi as A
+    from pfem2_b200 import cases
+    from pfem2_b200.solver import STAGE_NAMES, Solver
+
+    out = {}
+    proj = {}
+    for push in (0, 1):
+        sp = cases.channel_disk(h=args.h, zero_ids=(3, 4), wall_pushback=push)
+        s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True)
+        s.seed_particles(sp.q, sp.seed, sp.jitter)
+        stream = torch.cuda.ExternalStream(s.stream(), device=local)
+        for _ in range(3):
+            s.step()
+        s.synchronize()
+        s.enable_stage_timing(True)
+        s.stage_times(reset=True)
+        timed_steps(s, stream, flush, args.extra_steps)
+        proj[push] = s.stage_times()[STAGE_NAMES.index("project_nodes")] / args.extra_steps
+        if push == 1:
+            # vorticity: K calls, CUDA events on the library stream
+            s.enable_stage_timing(False)
+            s.calculate_vorticity()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k = 20
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0.record(stream)
+            for _ in range(k):
+                s.L.pfem2_calculate_vorticity(s.h)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / k
+            nv, nc = sp.mesh.n_vertices, sp.mesh.n_cells
+            # algorithmic bytes: Vx, Vy and coordinates of every vertex (32 B),
+            # the result (8 B), connectivity (16 B per cell)
+            b = 40.0 * nv + 16.0 * nc
+            hbm, kind = peaks()
+            out["vorticity"] = {"ms": ms, "GB/s": b / (ms / 1e3) / 1e9, "frac": b / (ms / 1e3) / 1e9 / hbm,
+                                "peak_kind": kind, "vertices": nv}
+        s.close()
+    out["wall_pushback"] = {"project_stage_ms_off": proj[0], "project_stage_ms_on": proj[1],
+                            "walls": "disk and channel walls (boundary ids 3, 4)"}
+    return out
 
 
 def pipe_leg(args, local, flush):

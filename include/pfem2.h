@@ -38,7 +38,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define PFEM2_ABI_VERSION 1
+#define PFEM2_ABI_VERSION 2
 
 typedef enum {
   PFEM2_OK = 0,
@@ -62,7 +62,8 @@ typedef enum {
   PFEM2_FIELD_OLD_VX = 4, PFEM2_FIELD_OLD_VY = 5, PFEM2_FIELD_OLD_VZ = 6, PFEM2_FIELD_OLD_P = 7,
   PFEM2_FIELD_PRED_VX = 8, PFEM2_FIELD_PRED_VY = 9, PFEM2_FIELD_PRED_VZ = 10,
   PFEM2_FIELD_NODE_WEIGHT = 11,  /* sum of shape values from the last projection */
-  PFEM2_N_FIELDS = 12
+  PFEM2_FIELD_VORTICITY = 12,    /* nodal vorticity from the last pfem2_calculate_vorticity (2D) */
+  PFEM2_N_FIELDS = 13
 } pfem2_field;
 
 typedef enum {
@@ -120,6 +121,12 @@ typedef struct {
   int32_t vel_solver;             /* pfem2_solver_kind */
   int32_t p_solver;               /* pfem2_solver_kind */
   int32_t reassemble_every_step;  /* 1: rebuild matrices each step like the reference */
+  /* 1: wall push-back after the projection (nacaAirfoil/pfem2particle.cpp:
+   * 919-952): for every zero_after_projection vertex whose projected
+   * velocity has a component above 1e-5 in magnitude, every particle of the
+   * cells around it loses N_vertex(xi_p) times that velocity, before the
+   * vertex is set to zero. 0: the vertex is only set to zero. */
+  int32_t wall_pushback;
 } pfem2_case;
 
 /* A mesh of one instance (host arrays, copied by pfem2_add_instance). */
@@ -198,6 +205,12 @@ pfem2_status pfem2_fem_step(pfem2_ctx* ctx);
  * {Cx_nu, Cx_p, Cy_nu, Cy_p, p(probe_a) - p(probe_b)} (2D). In 3D out =
  * {Fx_p, Fy_p, Fz_p, 0, p(probe_a) - p(probe_b)} (tubePoiseuille3D/pfem2particle.cpp:693-737). */
 pfem2_status pfem2_loads(pfem2_ctx* ctx, int32_t instance, int32_t patch_id, double out[5]);
+/* calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050), 2D: at the
+ * QGauss(2) points of every cell w = sum_i (dN_i/dx Vy_i - dN_i/dy Vx_i),
+ * and at every vertex the sum over its cells and their points of N_vertex w
+ * divided by the sum of N_vertex; into PFEM2_FIELD_VORTICITY of every
+ * instance (read it with pfem2_get_field). INVALID_ARG in 3D. */
+pfem2_status pfem2_calculate_vorticity(pfem2_ctx* ctx);
 /* One whole time step: correct -> move -> project -> fem_step, with fused
  * kernels (and a CUDA graph if cfg.use_graph); advances time by dt. */
 pfem2_status pfem2_step(pfem2_ctx* ctx);

@@ -44,6 +44,8 @@ def _load():
     lib.or_step.argtypes = [vp, C.c_int]
     lib.or_step.restype = C.c_int
     lib.or_loads.argtypes = [vp, C.c_int, _dp]
+    lib.or_vorticity.argtypes = [vp]
+    lib.or_vorticity.restype = C.c_int
     lib.or_n_particles.argtypes = [vp]
     lib.or_n_particles.restype = C.c_int
     lib.or_nnz.argtypes = [vp]
@@ -131,6 +133,12 @@ class Oracle:
         out = np.zeros(5)
         self.L.or_loads(self.h, patch_id, out)
         return out
+
+    def calculate_vorticity(self):
+        """nodal vorticity (2D), cylinderDyM/pfem2particle.cpp:1000-1050"""
+        if self.L.or_vorticity(self.h) != 0:
+            raise ValueError("the vorticity is computed for 2D meshes only")
+        return self.field(A.FIELD_VORTICITY)
 
     def step(self, precond_p=1):
         return self.L.or_step(self.h, precond_p)

@@ -22,6 +22,8 @@
  *              absolute residual tolerance), textbook CG
  *   loads      TurekBenchmark/pfem2particle.cpp:920-970,
  *              tubePoiseuille3D/pfem2particle.cpp:693-737
+ *   wall push-back  nacaAirfoil/pfem2particle.cpp:919-952
+ *   vorticity  cylinderDyM/pfem2particle.cpp:1000-1050
  *   deal.II pieces restated from their mathematics: FE_Q(1) shape functions,
  *   MappingQ1 (bi/trilinear map and its Newton inverse), QGauss(2),
  *   GeometryInfo::is_inside_unit_cell, GridTools::vertex_to_cell_map and
@@ -763,6 +765,36 @@ void or_project(omodel* m) {
   for (int v = 0; v < m->nv; ++v)
     for (int d = 0; d < dim; ++d) m->f[PFEM2_FIELD_VX + d][v] = w[v] != 0.0 ? acc[d][v] / w[v] : 0.0;
   for (int d = 0; d < dim; ++d) free(acc[d]);
+  if (m->cs.zero_after_projection_mask && m->cs.wall_pushback) {
+    /* wall push-back (nacaAirfoil/pfem2particle.cpp:919-952): for every wall
+     * vertex whose projected velocity has a component above 1e-5, every
+     * particle of the cells around it loses N_vertex(xi_p) times that
+     * velocity; here per particle, over its cell's wall vertices in
+     * ascending local order */
+    unsigned char* wall = (unsigned char*)xcalloc(m->nv, 1);
+    for (int c = 0; c < m->nc; ++c)
+      for (int f = 0; f < m->nfc; ++f) {
+        int b = m->fb[(size_t)c * m->nfc + f];
+        if (b < 0 || b > 31 || !((m->cs.zero_after_projection_mask >> b) & 1u)) continue;
+        int ax = f / 2, side = f % 2;
+        for (int v = 0; v < nvc; ++v)
+          if (((v >> ax) & 1) == side) wall[m->cv[(size_t)c * nvc + v]] = 1;
+      }
+    for (int p = 0; p < m->np; ++p) {
+      int c = m->pc[p];
+      double N[MAXV];
+      shape_values(dim, m->pxi + (size_t)p * dim, N);
+      for (int v = 0; v < nvc; ++v) {
+        int g = m->cv[(size_t)c * nvc + v];
+        if (!wall[g]) continue;
+        int big = 0;
+        for (int d = 0; d < dim; ++d) big |= fabs(m->f[PFEM2_FIELD_VX + d][g]) > 1e-5;
+        if (!big) continue;
+        for (int d = 0; d < dim; ++d) m->pu[(size_t)p * dim + d] -= N[v] * m->f[PFEM2_FIELD_VX + d][g];
+      }
+    }
+    free(wall);
+  }
   if (m->cs.zero_after_projection_mask) {
     for (int c = 0; c < m->nc; ++c)
       for (int f = 0; f < m->nfc; ++f) {
@@ -774,6 +806,44 @@ void or_project(omodel* m) {
             for (int d = 0; d < dim; ++d) m->f[PFEM2_FIELD_VX + d][m->cv[(size_t)c * nvc + v]] = 0.0;
       }
   }
+}
+
+/* calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050), 2D: per
+ * cell, at the QGauss(2) points, w = sum_i (dN_i/dx Vy_i - dN_i/dy Vx_i);
+ * the cell's sums of N_v w and N_v over its points are added to its vertices
+ * in ascending cell order; node value = quotient (0 where the weight is 0).
+ * Returns -1 in 3D. */
+int or_vorticity(omodel* m) {
+  if (m->dim != 2) return -1;
+  double* acc = (double*)xcalloc(m->nv, sizeof(double));
+  double* wsum = (double*)xcalloc(m->nv, sizeof(double));
+  const double* Vx = m->f[PFEM2_FIELD_VX];
+  const double* Vy = m->f[PFEM2_FIELD_VY];
+  for (int c = 0; c < m->nc; ++c) {
+    qpoint qs[8];
+    int nq = cell_qpoints(m, c, qs);
+    double lv[MAXV] = {0}, lw[MAXV] = {0};
+    for (int k = 0; k < nq; ++k) {
+      double w = 0.0;
+      for (int i = 0; i < 4; ++i) {
+        int g = m->cv[(size_t)c * 4 + i];
+        w += qs[k].G[i * 2] * Vy[g] - qs[k].G[i * 2 + 1] * Vx[g];
+      }
+      for (int v = 0; v < 4; ++v) {
+        lv[v] += qs[k].N[v] * w;
+        lw[v] += qs[k].N[v];
+      }
+    }
+    for (int v = 0; v < 4; ++v) {
+      int g = m->cv[(size_t)c * 4 + v];
+      acc[g] += lv[v];
+      wsum[g] += lw[v];
+    }
+  }
+  for (int v = 0; v < m->nv; ++v) m->f[PFEM2_FIELD_VORTICITY][v] = wsum[v] != 0.0 ? acc[v] / wsum[v] : 0.0;
+  free(acc);
+  free(wsum);
+  return 0;
 }
 
 /* ------------------------------------------------------------------ */

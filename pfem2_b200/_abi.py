@@ -17,8 +17,8 @@ STATUS_NAMES = {
 PREC_FP64, PREC_MIXED = 0, 1
 
 (FIELD_VX, FIELD_VY, FIELD_VZ, FIELD_P, FIELD_OLD_VX, FIELD_OLD_VY, FIELD_OLD_VZ, FIELD_OLD_P,
- FIELD_PRED_VX, FIELD_PRED_VY, FIELD_PRED_VZ, FIELD_NODE_WEIGHT) = range(12)
-N_FIELDS = 12
+ FIELD_PRED_VX, FIELD_PRED_VY, FIELD_PRED_VZ, FIELD_NODE_WEIGHT, FIELD_VORTICITY) = range(13)
+N_FIELDS = 13
 
 BC_CONSTANT, BC_PARABOLA = 0, 1
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
@@ -45,6 +45,7 @@ class Case(C.Structure):
         ("vel_tol", C.c_double), ("p_tol", C.c_double),
         ("max_iter", C.c_int32), ("vel_solver", C.c_int32), ("p_solver", C.c_int32),
         ("reassemble_every_step", C.c_int32),
+        ("wall_pushback", C.c_int32),
     ]
 
 

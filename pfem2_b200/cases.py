@@ -41,7 +41,8 @@ class CaseSpec:
 
 def make_case(mu, rho, dt, vel_bcs, p_bcs, open_ids, open_flux=0.0, zero_ids=(), load_patch=-1,
               load_diam=1.0, load_umean=1.0, probes=(-1, -1), outer=1, vel_tol=1e-7, p_tol=1e-7,
-              max_iter=10000, vel_solver=A.SOLVER_BICGSTAB, p_solver=A.SOLVER_CG, reassemble=0):
+              max_iter=10000, vel_solver=A.SOLVER_BICGSTAB, p_solver=A.SOLVER_CG, reassemble=0,
+              wall_pushback=0):
     """vel_bcs: list (per velocity component) of lists of (bid, kind, value, axis, a, b);
     p_bcs: list of the same tuples for the pressure."""
     cs = A.Case()
@@ -70,6 +71,7 @@ def make_case(mu, rho, dt, vel_bcs, p_bcs, open_ids, open_flux=0.0, zero_ids=(),
     cs.max_iter = max_iter
     cs.vel_solver, cs.p_solver = vel_solver, p_solver
     cs.reassemble_every_step = reassemble
+    cs.wall_pushback = wall_pushback
     return cs
 
 
@@ -96,7 +98,7 @@ def poiseuille_2d(nx=64, ny=16, steps=200, jitter=0.1, seed=0, q=(4, 4), **kw):
 
 
 def channel_disk(h=0.0088, radius=0.1, reynolds=100.0, umax=1.5, dt=0.002, steps=500, q=(5, 5),
-                 seed=0, jitter=0.0, **kw):
+                 seed=0, jitter=0.0, zero_ids=(), **kw):
     mesh = M.channel_disk_mesh(h=h, radius=radius)
     umean = 2.0 / 3.0 * umax
     diam = 2.0 * radius
@@ -105,7 +107,7 @@ def channel_disk(h=0.0088, radius=0.1, reynolds=100.0, umax=1.5, dt=0.002, steps
         mu=nu, rho=1.0, dt=dt,
         vel_bcs=[[parabola(1, umax, 1, 0.0, 1.0), const(3), const(4)],
                  [const(1), const(3), const(4)]],
-        p_bcs=[const(2)], open_ids=(1, 2), zero_ids=(), load_patch=3,
+        p_bcs=[const(2)], open_ids=(1, 2), zero_ids=zero_ids, load_patch=3,
         load_diam=diam, load_umean=umean,
         probes=(M.nearest_vertex(mesh, (0.5 - radius, 0.5)), M.nearest_vertex(mesh, (0.5 + radius, 0.5))),
         **kw)

@@ -349,6 +349,22 @@ static pfem2_status do_setup(Ctx& c) {
     PFEM2_TRY(dalloc(&c.shift[f], nv));
   }
   PFEM2_TRY(upload(&c.zero_flag, zflag));
+  {
+    // cells that the wall push-back visits
+    std::vector<int> wc;
+    for (auto& in : c.inst)
+      if (in.cs.wall_pushback)
+        for (int ce = in.c_off; ce < in.c_off + in.nc; ++ce) {
+          bool touch = false;
+          for (int b = 0; b < NV; ++b) touch |= zflag[cv[(size_t)ce * NV + b]] != 0;
+          if (touch) wc.push_back(ce);
+        }
+    c.n_wall_cells = (int)wc.size();
+    if (!wc.empty()) {
+      PFEM2_TRY(upload(&c.wall_cells, wc));
+      PFEM2_TRY(dalloc(&c.wall_dv, (size_t)dim * nv));
+    }
+  }
   PFEM2_TRY(upload(&c.d_inst, c.h_inst));
   {
     double* t = nullptr;
@@ -613,7 +629,8 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   krylov_free(c);
   // device memory is released with the context's allocations; free the big ones
   void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
-                  c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.d_inst,
+                  c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.wall_dv,
+                  c.wall_cells, c.d_inst,
                   c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.rebin_tiles, c.d_np, c.d_counters,
                   c.far_keys, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
   for (void* p : ptrs)
@@ -859,6 +876,18 @@ pfem2_status pfem2_step_and_read(pfem2_ctx* x, double* loads_out, const int32_t*
   PFEM2_CUDA(cudaStreamSynchronize(c.stream));
   for (int i = 0; i < ni && loads_out; ++i) finish_loads(c, i, c.loads_host + 7 * i, loads_out + 5 * i);
   return check_counters(c, false);
+}
+
+pfem2_status pfem2_calculate_vorticity(pfem2_ctx* x) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (c.dim != 2) {
+    set_error("calculate_vorticity: the vorticity is computed for 2D meshes only");
+    return PFEM2_INVALID_ARG;
+  }
+  PFEM2_TRY(launch_vorticity(c));
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
 }
 
 pfem2_status pfem2_loads(pfem2_ctx* x, int32_t instance, int32_t patch_id, double out[5]) {

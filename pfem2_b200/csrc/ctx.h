@@ -110,6 +110,12 @@ struct Ctx {
   double* dirval[4] = {};
   double* shift[4] = {};
   unsigned char* zero_flag = nullptr;
+  // wall push-back: projected values of the zero-flag vertices before they
+  // are zeroed ([dim][nv]) and the cells touching such vertices in
+  // instances with wall_pushback (ascending)
+  double* wall_dv = nullptr;
+  int* wall_cells = nullptr;
+  int n_wall_cells = 0;
 
   // nodal fields (FP64 masters) and Real mirrors for particle kernels
   double* F[PFEM2_N_FIELDS] = {};
@@ -231,6 +237,7 @@ pfem2_status launch_rhs_correction(Ctx& c);
 pfem2_status launch_finish_fem(Ctx& c);
 pfem2_status launch_restore_frozen(Ctx& c);
 pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev);
+pfem2_status launch_vorticity(Ctx& c);
 
 // krylov.cu
 pfem2_status krylov_setup(Ctx& c);

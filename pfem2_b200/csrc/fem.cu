@@ -657,4 +657,60 @@ pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev) {
   return PFEM2_OK;
 }
 
+// ---------------------------------------------------------------- vorticity
+// calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050), 2D, FP64.
+// Node-centric: a thread per vertex walks the cells around it in ascending
+// order; per cell it sums N_loc(q) w(q) and N_loc(q) over the QGauss(2)
+// points (x fastest), w = sum_i (dN_i/dx Vy_i - dN_i/dy Vx_i), and adds the
+// cell sums, as the reference's distribute_local_to_global does; the node
+// value is the quotient (0 where the weight is 0).
+__global__ void __launch_bounds__(256) k_vorticity(int nv, const int* __restrict__ v2c_ptr,
+                                                   const int* __restrict__ v2c_cell,
+                                                   const unsigned char* __restrict__ v2c_loc,
+                                                   const double* __restrict__ X, const int* __restrict__ cv,
+                                                   const double* __restrict__ Vx, const double* __restrict__ Vy,
+                                                   double* __restrict__ out) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    double acc = 0.0, wsum = 0.0;
+    const int k1 = v2c_ptr[v + 1];
+    for (int k = v2c_ptr[v]; k < k1; ++k) {
+      const int c = v2c_cell[k], loc = v2c_loc[k];
+      LocalCell<2, double> L;
+      double x0[2];
+      load_local_cell<2, double>(X, cv, c, L, x0);
+      double vx[4], vy[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int g = __ldg(cv + (size_t)c * 4 + i);
+        vx[i] = Vx[g];
+        vy[i] = Vy[g];
+      }
+      double lv = 0.0, lw = 0.0;
+#pragma unroll
+      for (int iq = 0; iq < 4; ++iq) {
+        double xi[2];
+        cell_qp_xi<2, double>(iq, xi);
+        QP<2, double> q;
+        eval_qp<2, double>(L, xi, cell_qp_w<2>(), -1, q);
+        double w = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w += q.G[i][0] * vy[i] - q.G[i][1] * vx[i];
+        lv += q.N[loc] * w;
+        lw += q.N[loc];
+      }
+      acc += lv;
+      wsum += lw;
+    }
+    out[v] = wsum != 0.0 ? acc / wsum : 0.0;
+  }
+}
+
+pfem2_status launch_vorticity(Ctx& c) {
+  k_vorticity<<<grid_for(c, c.nv, 256, 8), 256, 0, c.stream>>>(c.nv, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.X, c.cv,
+                                                              c.F[PFEM2_FIELD_VX], c.F[PFEM2_FIELD_VY],
+                                                              c.F[PFEM2_FIELD_VORTICITY]);
+  c.launches++;
+  return PFEM2_OK;
+}
+
 }  // namespace pfem2

@@ -1057,7 +1057,8 @@ __global__ void __launch_bounds__(256) k_project_nodes(int nv, const int* __rest
                                                        const unsigned char* __restrict__ zero_flag,
                                                        double* __restrict__ V0, double* __restrict__ V1,
                                                        double* __restrict__ V2, double* __restrict__ W,
-                                                       R* __restrict__ Vr, int* __restrict__ counters) {
+                                                       R* __restrict__ Vr, int* __restrict__ counters,
+                                                       double* __restrict__ wall_dv) {
   constexpr int K = Dims<DIM>::NV * (DIM + 1);
   double* V[3] = {V0, V1, V2};
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
@@ -1076,11 +1077,66 @@ __global__ void __launch_bounds__(256) k_project_nodes(int nv, const int* __rest
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       R val = (w != R(0)) ? s[d] / w : R(0);
-      if (z) val = R(0);
+      if (z) {
+        if (wall_dv) wall_dv[(size_t)d * nv + v] = (double)val;  // for the wall push-back
+        val = R(0);
+      }
       V[d][v] = (double)val;
       Vr[(size_t)d * nv + v] = val;
     }
     W[v] = (double)w;
+  }
+}
+
+// Wall push-back after the projection (nacaAirfoil/pfem2particle.cpp:
+// 919-952): a warp per cell touching a zero-flag vertex; every particle of
+// the cell loses N_v(xi_p) times the projected velocity of each such vertex v
+// whose velocity has a component above 1e-5 in magnitude (vertices in
+// ascending local order, FP64 products).
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_wall_pushback(int ncells, const int* __restrict__ cells,
+                                                       const int* __restrict__ cell_start, const int* __restrict__ cv,
+                                                       const unsigned char* __restrict__ zero_flag,
+                                                       const double* __restrict__ dv, int nv,
+                                                       const R* __restrict__ xi, R* __restrict__ u, size_t cap) {
+  constexpr int NV = Dims<DIM>::NV;
+  const int lane = threadIdx.x & 31;
+  for (int wc = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5); wc < ncells;
+       wc += (int)((gridDim.x * (size_t)blockDim.x) >> 5)) {
+    const int c = cells[wc];
+    double d[NV][DIM];
+    bool on[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const int g = __ldg(cv + (size_t)c * NV + v);
+      on[v] = false;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) d[v][a] = 0.0;
+      if (zero_flag[g]) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          d[v][a] = dv[(size_t)a * nv + g];
+          on[v] |= fabs(d[v][a]) > 1e-5;
+        }
+      }
+    }
+    const int p1 = cell_start[c + 1];
+    for (int p = cell_start[c] + lane; p < p1; p += 32) {
+      double x[DIM], N[NV];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) x[a] = (double)xi[(size_t)a * cap + p];
+      shape_values<DIM, double>(x, N);
+      double uu[DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) uu[a] = (double)u[(size_t)a * cap + p];
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        if (on[v])
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) uu[a] -= N[v] * d[v][a];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) u[(size_t)a * cap + p] = R(uu[a]);
+    }
   }
 }
 
@@ -1095,8 +1151,14 @@ static pfem2_status project_impl(Ctx& c, bool partials_ready) {
   k_project_nodes<DIM, R><<<grid_for(c, c.nv, 256, 8), 256, 0, c.stream>>>(
       c.nv, c.v2c_ptr, c.v2c_cell, c.v2c_loc, (const R*)c.partial, c.zero_flag, c.F[PFEM2_FIELD_VX],
       c.F[PFEM2_FIELD_VY], c.dim == 3 ? c.F[PFEM2_FIELD_VZ] : c.F[PFEM2_FIELD_VZ], c.F[PFEM2_FIELD_NODE_WEIGHT],
-      (R*)c.Vr, c.d_counters);
+      (R*)c.Vr, c.d_counters, c.wall_dv);
   c.launches++;
+  if (c.n_wall_cells > 0) {
+    k_wall_pushback<DIM, R><<<grid_for(c, (long long)c.n_wall_cells * 32, 256, 8), 256, 0, c.stream>>>(
+        c.n_wall_cells, c.wall_cells, c.cell_start[b], c.cv, c.zero_flag, c.wall_dv, c.nv, (const R*)c.pxi[b],
+        (R*)c.pu[b], (size_t)c.pcap);
+    c.launches++;
+  }
   return PFEM2_OK;
 }
 

@@ -37,6 +37,7 @@ EXPORTS = [
     "pfem2_get_particles", "pfem2_set_particles", "pfem2_get_stats", "pfem2_get_time", "pfem2_synchronize",
     "pfem2_launch_count", "pfem2_stage_times", "pfem2_enable_stage_timing", "pfem2_get_stream",
     "pfem2_last_error", "pfem2_abi_version", "pfem2_project_noalloc", "pfem2_solver_sizes",
+    "pfem2_calculate_vorticity",
 ]
 
 
@@ -73,6 +74,7 @@ def load_library(path=LIB_PATH):
         "pfem2_launch_count": [vp, C.POINTER(C.c_int64)],
         "pfem2_stage_times": [vp, dp, C.c_int32],
         "pfem2_solver_sizes": [vp, C.POINTER(C.c_int64)],
+        "pfem2_calculate_vorticity": [vp],
         "pfem2_enable_stage_timing": [vp, C.c_int32],
         "pfem2_get_stream": [vp, C.POINTER(vp)],
     }
@@ -176,6 +178,12 @@ class Solver:
         out = np.zeros(5)
         self._check(self.L.pfem2_loads(self.h, instance, patch_id, _dptr(out)))
         return out
+
+    def calculate_vorticity(self, instance=0):
+        """calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050), 2D:
+        the nodal vorticity of every instance; returns the given instance's."""
+        self._check(self.L.pfem2_calculate_vorticity(self.h))
+        return self.field(A.FIELD_VORTICITY, instance)
 
     def step(self):
         self._check(self.L.pfem2_step(self.h))

@@ -70,7 +70,7 @@ def test_exports_cover_header():
     for n in names:
         assert hasattr(lib, n), n
     lib.pfem2_abi_version.restype = C.c_int32
-    assert lib.pfem2_abi_version() == 1
+    assert lib.pfem2_abi_version() == 2
 
 
 def test_status_codes_match_header():
@@ -110,7 +110,7 @@ def test_cpp_shim_compiles_and_links():
         "    pfem2b::Solver s(c, m, k); s.seed_particles({4, 4}); s.correct_particles_velocities();\n"
         "    s.move_particles(); s.distribute_particle_velocities_to_grid(); s.fem_step();\n"
         "    std::ofstream f(\"forces.csv\"); s.calculate_loads(3, &f); s.step(); }\n"
-        "  return pfem2_abi_version() == 1 ? 0 : 1; }\n")
+        "  return pfem2_abi_version() == 2 ? 0 : 1; }\n")
     with tempfile.TemporaryDirectory() as d:
         cpp = os.path.join(d, "drv.cpp")
         exe = os.path.join(d, "drv")

@@ -313,3 +313,59 @@ def test_advect_split_equals_one_kernel(monkeypatch):
     for x, y in zip(fa, fb):
         assert np.array_equal(x, y)
     assert da == db
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_vorticity(prec):
+    """calculate_vorticity on the library's own fields after two steps
+    against the oracle's restatement on the same fields (FP64 in both)"""
+    sp = cases.channel_disk(h=0.05, dt=0.01)
+    g = Solver(sp, precision=prec)
+    g.seed_particles(sp.q, seed=0, jitter=0.1)
+    for _ in range(2):
+        g.step()
+    w = g.calculate_vorticity()
+    o = O.Oracle(sp.mesh, sp.case)
+    o.set_field(A.FIELD_VX, g.field(A.FIELD_VX))
+    o.set_field(A.FIELD_VY, g.field(A.FIELD_VY))
+    assert rel_l2(w, o.calculate_vorticity()) <= 1e-12
+    assert np.abs(w).max() > 1.0  # the disk sheds vorticity
+    g.close()
+
+
+def test_vorticity_rejects_3d():
+    sp = spec_3d()
+    g = Solver(sp, precision=A.PREC_FP64)
+    with pytest.raises(Exception):
+        g.calculate_vorticity()
+    g.close()
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_wall_pushback_steps(prec):
+    """three whole steps of the disk channel with the wall push-back on the
+    disk and the channel walls (zero_after_projection), against the oracle"""
+    sp = cases.channel_disk(h=0.05, dt=0.01, zero_ids=(3, 4), wall_pushback=1)
+    sp.case.vel_tol = 1e-13
+    sp.case.p_tol = 1e-12
+    g, o = make_pair(sp, prec)
+    g.seed_particles(sp.q, seed=0, jitter=0.1)
+    o.seed_particles(sp.q, seed=0, jitter=0.1)
+    for _ in range(3):
+        g.step()
+        o.step(1)
+    tol = {A.PREC_FP64: 1e-8, A.PREC_MIXED: 1e-4}[prec]
+    for fld in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P):
+        e = rel_l2(g.field(fld), o.field(fld))
+        assert e <= tol, (fld, e)
+    # the push-back changed the particles next to the walls: without it
+    # the run differs by more than the tolerance
+    sp0 = cases.channel_disk(h=0.05, dt=0.01, zero_ids=(3, 4), wall_pushback=0)
+    sp0.case.vel_tol, sp0.case.p_tol = 1e-13, 1e-12
+    g0 = Solver(sp0, precision=prec)
+    g0.seed_particles(sp0.q, seed=0, jitter=0.1)
+    for _ in range(3):
+        g0.step()
+    assert rel_l2(g0.field(A.FIELD_VX), g.field(A.FIELD_VX)) > 10 * tol
+    g.close()
+    g0.close()

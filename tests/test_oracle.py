@@ -222,3 +222,50 @@ def test_loads_pressure_only():
     s = 2.0 / (1.0 * 1.0 ** 2 * 0.2)
     assert abs(out[1] - s * area) < 2e-3 * s
     assert abs(out[3]) < 1e-10 and abs(out[0]) < 1e-14
+
+
+def test_vorticity_of_linear_fields():
+    """calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050): Q1 cells
+    reproduce a linear velocity field exactly, so every node recovers its
+    vorticity dVy/dx - dVx/dy, also on the curved O-grid cells"""
+    sp = cases.channel_disk(h=0.05)
+    o = O.Oracle(sp.mesh, sp.case)
+    X = sp.mesh.vertices
+    o.set_field(A.FIELD_VX, 2.0 - 0.5 * X[:, 1] + 0.3 * X[:, 0])
+    o.set_field(A.FIELD_VY, 1.5 * X[:, 0] - 0.3 * X[:, 1])
+    w = o.calculate_vorticity()
+    assert np.allclose(w, 2.0, rtol=0, atol=1e-10)
+
+
+def test_vorticity_rejects_3d():
+    sp = cases.pipe_3d(ny=4, nz=4, nx=8)
+    o = O.Oracle(sp.mesh, sp.case)
+    with pytest.raises(ValueError):
+        o.calculate_vorticity()
+
+
+def test_wall_pushback_known_answer():
+    """wall push-back (nacaAirfoil/pfem2particle.cpp:919-952): a uniform
+    particle velocity U projects to U at every node; then every particle of a
+    wall cell keeps U (1 - sum of N_v over the cell's wall vertices) and the
+    wall nodes are zero. Without the flag the particles keep U."""
+    U = np.array([1.0, 0.5])
+    for push in (0, 1):
+        sp = cases.poiseuille_2d(nx=4, ny=2, zero_ids=(2, 3), wall_pushback=push)
+        o = O.Oracle(sp.mesh, sp.case)
+        o.seed_particles((2, 2), seed=0, jitter=0.0)
+        cell, xi, u = o.particles()
+        o.set_particles(cell, xi, np.tile(U, (len(cell), 1)), q=(2, 2))
+        o.distribute_particle_velocities_to_grid()
+        cell2, xi2, u2 = o.particles()
+        X = sp.mesh.vertices
+        wall = (np.abs(X[:, 1]) < 1e-12) | (np.abs(X[:, 1] - 1.0) < 1e-12)
+        vx, vy = o.field(A.FIELD_VX), o.field(A.FIELD_VY)
+        assert np.all(vx[wall] == 0.0) and np.all(vy[wall] == 0.0)
+        assert np.allclose(vx[~wall], U[0]) and np.allclose(vy[~wall], U[1])
+        cv = sp.mesh.cells
+        for p in range(len(cell2)):
+            x, y = xi2[p]
+            N = np.array([(1 - x) * (1 - y), x * (1 - y), (1 - x) * y, x * y])
+            f = 1.0 - push * N[wall[cv[cell2[p]]]].sum()
+            assert np.allclose(u2[p], f * U, atol=1e-14)
