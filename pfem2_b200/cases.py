@@ -127,6 +127,33 @@ def pipe_3d(ny=64, nz=64, nx=256, steps=100, q=(3, 3, 3), dpdx=-1.0, seed=0, jit
     return CaseSpec("pipe_3d", mesh, cs, q, seed, jitter, steps, meta={"nu": nu, "dpdx": dpdx})
 
 
+def cylinder2d_unv(path, mu=0.003333333, dt=0.02, u_in=1.0, steps=100, q=(2, 2), seed=0, jitter=0.0, **kw):
+    """The reference's cylinder2D case on a mesh read from a UNV file
+    (cylinder2D/cylinder2D.cc:266-277, 455-470, 530-545, 605-610 and
+    input_data.prm): boundary group 1 = inlet (Vx = u_in, Vy = 0), 2 = outlet
+    (p = 0), 3 = cylinder (no slip, the load patch), 4 = walls (Vy = 0);
+    inlet and outlet are the open sections."""
+    from pfem2_b200 import unv
+
+    mesh = unv.read_unv(path)
+    cyl = np.unique(mesh.cells[np.nonzero(mesh.face_bid == 3)[0]].ravel())
+    on3 = set()
+    for c, f in zip(*np.nonzero(mesh.face_bid == 3)):
+        ax, side = f // 2, f % 2
+        on3.update(int(mesh.cells[c][v]) for v in range(4) if ((v >> ax) & 1) == side)
+    pts = mesh.vertices[sorted(on3)] if on3 else mesh.vertices[cyl]
+    centre = pts.mean(axis=0)
+    diam = 2.0 * float(np.mean(np.linalg.norm(pts - centre, axis=1)))
+    cs = make_case(
+        mu=mu, rho=1.0, dt=dt,
+        vel_bcs=[[const(1, u_in), const(3)], [const(1), const(3), const(4)]],
+        p_bcs=[const(2)], open_ids=(1, 2), load_patch=3, load_diam=diam, load_umean=u_in,
+        probes=(M.nearest_vertex(mesh, (float(centre[0]) - diam, float(centre[1]))),
+                M.nearest_vertex(mesh, (float(centre[0]) + diam, float(centre[1])))),
+        **kw)
+    return CaseSpec("cylinder2d_unv", mesh, cs, q, seed, jitter, steps, meta={"diam": diam, "centre": centre.tolist()})
+
+
 def ensemble(n=64, seed=2, cells_lo=5000, cells_hi=60000, re_lo=20.0, re_hi=200.0, r_lo=0.05, r_hi=0.15,
              q=(5, 5), steps=500, **kw):
     """Instances of channel_disk with log-uniform cells / Re and uniform radius."""
