@@ -153,6 +153,60 @@ def _lexicographic(X, v, dim):
     return lex
 
 
+def repair_unv(src, dst):
+    """What the reference's repairMesh tool does (repairMesh/repairMesh.cc)
+    for deal.II import: drop every dataset before the nodes, keep the nodes,
+    the cells and only those line (2D) / face (3D) elements that a group
+    lists (internal boundaries and leftovers go), keep the groups. Returns
+    (elements kept, elements dropped). read_unv gives the same mesh for the
+    original and the repaired file."""
+    with open(src) as f:
+        lines = f.read().splitlines()
+    out = []
+    listed = set()
+    blocks = list(_datasets(lines))
+    for did, blk in blocks:
+        if did in (2467, 2477, 2452, 2435):
+            k = 0
+            while k < len(blk):
+                count = int(blk[k].split()[-1])
+                k += 2
+                n = 0
+                while n < count:
+                    v = [int(t) for t in blk[k].split()]
+                    for a in range(0, len(v), 4):
+                        if v[a] == 8:
+                            listed.add(v[a + 1])
+                    n += len(v) // 4
+                    k += 1
+    kept = dropped = 0
+    bricks = any(did == 2412 and any(len(l.split()) == 6 and l.split()[1] == "115" for l in blk)
+                 for did, blk in blocks)
+    cell_fe = 115 if bricks else 44
+    for did, blk in blocks:
+        if did == 2411:
+            out += ["    -1", "  2411"] + blk + ["    -1"]
+        elif did == 2412:
+            body = []
+            k = 0
+            while k < len(blk):
+                rec = [int(t) for t in blk[k].split()]
+                label, fe, nn = rec[0], rec[1], rec[5]
+                n_lines = 1 + (1 if fe in _BEAMS else 0) + (nn + 7) // 8
+                if fe == cell_fe or label in listed:
+                    body += blk[k:k + n_lines]
+                    kept += 1
+                else:
+                    dropped += 1
+                k += n_lines
+            out += ["    -1", "  2412"] + body + ["    -1"]
+        elif did in (2467, 2477, 2452, 2435):
+            out += ["    -1", f"  {did}"] + blk + ["    -1"]
+    with open(dst, "w") as f:
+        f.write("\n".join(out) + "\n")
+    return kept, dropped
+
+
 def write_unv(mesh, path, groups=None):
     """Writes a mesh as UNV (nodes, cells, boundary elements, groups): the
     inverse of read_unv for round-trip tests. groups: {boundary id: [(cell,

@@ -96,3 +96,36 @@ def test_reference_cylinder_case_runs_in_the_oracle():
     assert np.isclose(np.median(vx[inlet]), 1.0)
     loads = o.calculate_loads(3)
     assert np.all(np.isfinite(loads)) and loads[0] + loads[1] != 0.0
+
+
+def test_repair_drops_preamble_and_unlisted_elements(tmp_path):
+    """repairMesh: the datasets before the nodes and the line elements no
+    group lists (an internal boundary here) go; the mesh read back is the same"""
+    m = M.rect_mesh(4, 2, 0.0, 4.0, 0.0, 1.0)
+    p = tmp_path / "m.unv"
+    unv.write_unv(m, p)
+    lines = p.read_text().splitlines()
+    # a header dataset in front, and an unlisted internal line element
+    head = ["    -1", "   164", "METER", "    -1", "    -1", "  2420", "         1", "SMESH_Auxiliary_Cartesian_System",
+            "    -1"]
+    i = lines.index("  2412") + 1
+    extra = [f"{99999:10d}{11:10d}{2:10d}{1:10d}{7:10d}{2:10d}", f"{0:10d}{1:10d}{1:10d}",
+             f"{int(m.cells[0, 1]) + 1:10d}{int(m.cells[0, 3]) + 1:10d}"]
+    lines = head + lines[:i] + extra + lines[i:]
+    p.write_text("\n".join(lines) + "\n")
+    q = tmp_path / "repaired.unv"
+    kept, dropped = unv.repair_unv(p, q)
+    assert dropped == 1 and kept == m.n_cells + int((m.face_bid >= 0).sum())
+    assert "2420" not in q.read_text() and "164" not in q.read_text().split("2411")[0]
+    a, b = unv.read_unv(p), unv.read_unv(q)
+    assert np.array_equal(a.cells, b.cells) and np.array_equal(a.face_bid, b.face_bid)
+    assert np.array_equal(a.face_bid, m.face_bid)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_MESH), reason="the reference tree is not present")
+def test_repair_reference_mesh(tmp_path):
+    q = tmp_path / "repaired.unv"
+    kept, dropped = unv.repair_unv(REF_MESH, q)
+    assert (kept, dropped) == (7050 + 380, 0)  # every line element of that file is in a group
+    a, b = unv.read_unv(REF_MESH), unv.read_unv(q)
+    assert np.array_equal(a.cells, b.cells) and np.array_equal(a.face_bid, b.face_bid)
