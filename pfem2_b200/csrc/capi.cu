@@ -339,6 +339,22 @@ static pfem2_status do_setup(Ctx& c) {
   else PFEM2_TRY((c.mixed ? upload_cell_geo<3, float>(c, X, cv) : upload_cell_geo<3, double>(c, X, cv)));
   PFEM2_TRY(upload(&c.ring_ptr, ring_ptr));
   PFEM2_TRY(upload(&c.ring_cell, ring_cell));
+  {
+    // position of each cell in the rings of its ring cells (rings are
+    // symmetric: s is in ring(c) iff c is in ring(s)); 32 and beyond share
+    // the mask's all-ones code
+    std::vector<int> rev(ring_cell.size(), 0);
+    for (int ce = 0; ce < nc; ++ce)
+      for (int k = ring_ptr[ce]; k < ring_ptr[ce + 1]; ++k) {
+        const int s = ring_cell[k];
+        const int* b = ring_cell.data() + ring_ptr[s];
+        const int* e = ring_cell.data() + ring_ptr[s + 1];
+        const int* it = std::lower_bound(b, e, ce);
+        rev[k] = (it != e && *it == ce) ? (int)(it - b) : 32;
+      }
+    PFEM2_TRY(upload(&c.ring_rev, rev));
+    PFEM2_TRY(dalloc(&c.dest_mask, (size_t)nc));
+  }
   PFEM2_TRY(upload(&c.sl_ptr, sl_ptr));
   PFEM2_TRY(upload(&c.sl_len, sl_len));
   PFEM2_TRY(upload(&c.sl_col, sl_col));
@@ -630,7 +646,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   // device memory is released with the context's allocations; free the big ones
   void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.wall_dv,
-                  c.wall_cells, c.d_inst,
+                  c.wall_cells, c.ring_rev, c.dest_mask, c.d_inst,
                   c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.rebin_tiles, c.d_np, c.d_counters,
                   c.far_keys, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
   for (void* p : ptrs)

@@ -77,6 +77,8 @@ struct Ctx {
   void* cell_geo = nullptr;   // [nc] CellGeo<dim, Real>: local frame, inverse Jacobian, affine flag
   int* ring_ptr = nullptr;
   int* ring_cell = nullptr;
+  int* ring_rev = nullptr;       // [ring entry (c, k)] position of c in the ring of ring_cell[k]
+  unsigned* dest_mask = nullptr; // [nc] per old cell: ring positions that received movers (reset per advection)
   DevInst* d_inst = nullptr;
   std::vector<DevInst> h_inst;
 

@@ -407,14 +407,22 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect(
 __device__ __forceinline__ void advect_record(int p, int c0, int c, const int* __restrict__ ring_ptr,
                                               const int* __restrict__ ring_cell,
                                               unsigned long long* __restrict__ far_keys, int far_cap,
-                                              int* __restrict__ counters) {
+                                              int* __restrict__ counters, unsigned* __restrict__ dest_mask) {
   if (c < 0) {
     atomicAdd(counters + CNT_DELETED, 1);
   } else if (c != c0) {
-    // a particle that left the 1-ring of its old cell goes to the far list
+    // a particle that left the 1-ring of its old cell goes to the far list;
+    // one that stays in it marks its destination (bit = ring position) in
+    // the old cell's mask, so that the re-sort scans only segments that send
+    // particles to a cell
     bool near = false;
-    for (int rr = __ldg(ring_ptr + c0); rr < __ldg(ring_ptr + c0 + 1); ++rr)
-      if (__ldg(ring_cell + rr) == c) { near = true; break; }
+    const int r0 = __ldg(ring_ptr + c0);
+    for (int rr = r0; rr < __ldg(ring_ptr + c0 + 1); ++rr)
+      if (__ldg(ring_cell + rr) == c) {
+        near = true;
+        atomicOr(dest_mask + c0, rr - r0 < 32 ? 1u << (rr - r0) : 0xffffffffu);
+        break;
+      }
     if (!near) {
       int slot = atomicAdd(counters + CNT_FAR, 1);
       if (slot < far_cap) far_keys[slot] = ((unsigned long long)(unsigned)c << 32) | (unsigned)p;
@@ -433,7 +441,7 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_
     const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
     const int* __restrict__ cell_inst, const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
     const R* __restrict__ v2c_dir, const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell,
-    unsigned long long* __restrict__ far_keys, int far_cap, int* __restrict__ counters) {
+    unsigned long long* __restrict__ far_keys, int far_cap, int* __restrict__ counters, unsigned* __restrict__ dest_mask) {
   constexpr int NV = Dims<DIM>::NV;
   const int n = min(*d_np, (int)cap);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -459,7 +467,7 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_
     int s_left = 0;
     int c = advect_steps<DIM, R, true>(c0, x, dts, 0, s_left, S, geo, cv, Vr, nv, v2c_ptr, v2c_cell, v2c_dir);
     if (c < 0) c = -1;
-    advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters);
+    advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters, dest_mask);
     newcell[p] = c;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
@@ -478,7 +486,7 @@ __global__ void __launch_bounds__(256) k_advect_left(
     const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell, const int* __restrict__ queue,
     const unsigned char* __restrict__ qstep, const int* __restrict__ wcount,
     unsigned long long* __restrict__ far_keys, int far_cap,
-    int* __restrict__ counters) {
+    int* __restrict__ counters, unsigned* __restrict__ dest_mask) {
   const int n = min(*d_np, (int)cap);
   const int chunk = (n + fast_grid - 1) / fast_grid;
   const int wcap = ((chunk + 255) / 256) * 32;
@@ -499,7 +507,7 @@ __global__ void __launch_bounds__(256) k_advect_left(
       int s_left = 0;
       int c = advect_steps<DIM, R, true>(c0, x, dts, s0, s_left, S, geo, cv, Vr, nv, v2c_ptr, v2c_cell, v2c_dir);
       if (c < 0) c = -1;
-      advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters);
+      advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters, dest_mask);
       newcell[p] = c;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
@@ -543,12 +551,14 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
       k_advect_one<DIM, R, true><<<grid, 256, 0, c.stream>>>(
           c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
           (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
-          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters,
+          c.dest_mask);
     else
       k_advect_one<DIM, R, false><<<grid, 256, 0, c.stream>>>(
           c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
           (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
-          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters);
+          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters,
+          c.dest_mask);
     c.launches++;
   } else {
   if (fuse)
@@ -565,7 +575,7 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
   k_advect_left<DIM, R><<<G, 256, 0, c.stream>>>(
       c.pcell[b], (R*)c.pxi[b], c.newcell, (size_t)c.pcap, c.d_np + b, G, (const CellGeo<DIM, R>*)c.cell_geo, c.cv,
       (const R*)c.Vr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
-      c.ring_cell, c.adv_queue, c.adv_qstep, c.adv_wcount, c.far_keys, c.far_cap, c.d_counters);
+      c.ring_cell, c.adv_queue, c.adv_qstep, c.adv_wcount, c.far_keys, c.far_cap, c.d_counters, c.dest_mask);
   c.launches++;
   }
   k_far_sort<<<1, 1024, sizeof(unsigned long long) * c.far_cap, c.stream>>>(c.far_keys, c.d_counters, c.far_cap);
@@ -575,6 +585,7 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
 
 pfem2_status launch_advect(Ctx& c, bool fuse) {
   PFEM2_CUDA(cudaMemsetAsync(c.d_counters, 0, sizeof(int) * CNT_N, c.stream));
+  PFEM2_CUDA(cudaMemsetAsync(c.dest_mask, 0, sizeof(unsigned) * c.nc, c.stream));
   if (c.dim == 2) return c.mixed ? advect_impl<2, float>(c, fuse) : advect_impl<2, double>(c, fuse);
   return c.mixed ? advect_impl<3, float>(c, fuse) : advect_impl<3, double>(c, fuse);
 }
@@ -712,7 +723,8 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
     const int* __restrict__ old_start, const int* __restrict__ newcell, const R* __restrict__ oxi,
     const R* __restrict__ ou, size_t cap, int* __restrict__ ncell, R* __restrict__ nxi, R* __restrict__ nu,
     int* __restrict__ new_start, int* __restrict__ np_out, int nc, const int* __restrict__ ring_ptr,
-    const int* __restrict__ ring_cell, const unsigned long long* __restrict__ far_keys, int far_cap,
+    const int* __restrict__ ring_cell, const int* __restrict__ ring_rev,
+    const unsigned* __restrict__ dest_mask, const unsigned long long* __restrict__ far_keys, int far_cap,
     const DevInst* __restrict__ inst, const int* __restrict__ cell_inst, const int* __restrict__ cv,
     const R* __restrict__ Vr, int nv, R* __restrict__ partial, int list_cap, int* __restrict__ counters,
     unsigned long long* __restrict__ tiles) {
@@ -737,8 +749,10 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
     int ntot = 0;
     if (c < nc) {
     // gather the incoming particles of c in (ring cell, segment) order: the
-    // ring's segment bounds are loaded across lanes, then the first 32
-    // new-cell ids of 8 segments at a time, so the loads overlap
+    // ring's segment bounds are loaded across lanes, segments of neighbours
+    // that sent no particle to c (their destination masks) are dropped, then
+    // the first 32 new-cell ids of 8 remaining segments at a time, so the
+    // loads overlap
     int n_in = 0;
     const int r0 = __ldg(ring_ptr + c), nr = __ldg(ring_ptr + c + 1) - r0;
     for (int kb = 0; kb < nr; kb += 32) {
@@ -747,20 +761,32 @@ __global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
         const int s = __ldg(ring_cell + r0 + kb + lane);
         sb = min(old_start[s], (int)cap);
         se = min(old_start[s + 1], (int)cap);
+        if (s != c) {
+          const int rv = __ldg(ring_rev + r0 + kb + lane);
+          const unsigned m = dest_mask[s];
+          const bool sends = rv < 32 ? ((m >> rv) & 1u) != 0u : m != 0u;
+          if (!sends) se = sb;
+        }
       }
-      const int ng = min(32, nr - kb);
-      for (int k0 = 0; k0 < ng; k0 += 8) {
-        int v[8], bs[8], es[8];
+      unsigned act = __ballot_sync(PFEM2_FULL_MASK, se > sb);
+      while (act) {
+        int idx[8], v[8], bs[8], es[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          bs[j] = __shfl_sync(PFEM2_FULL_MASK, sb, (k0 + j) & 31);
-          es[j] = __shfl_sync(PFEM2_FULL_MASK, se, (k0 + j) & 31);
-          const int p = bs[j] + lane;
-          v[j] = (k0 + j < ng && p < es[j]) ? newcell[p] : -1;
+          idx[j] = act ? __ffs(act) - 1 : -1;
+          act &= act ? act - 1u : 0u;
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          if (k0 + j >= ng) break;
+          const int src = idx[j] < 0 ? 0 : idx[j];
+          bs[j] = __shfl_sync(PFEM2_FULL_MASK, sb, src);
+          es[j] = __shfl_sync(PFEM2_FULL_MASK, se, src);
+          const int p = bs[j] + lane;
+          v[j] = (idx[j] >= 0 && p < es[j]) ? newcell[p] : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (idx[j] < 0) break;
           {
             const int p = bs[j] + lane;
             const bool pred = v[j] == c;
@@ -984,7 +1010,8 @@ static void rebin_launch(Ctx& c, const int* newcell) {
   cudaMemsetAsync(c.rebin_tiles, 0, sizeof(unsigned long long) * ((size_t)ntiles + 1), c.stream);
   k_rebin<DIM, R, CHECK, PROJ><<<grid, kRebinWarps * 32, smem, c.stream>>>(
       c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, c.pcell[nb], (R*)c.pxi[nb],
-      (R*)c.pu[nb], c.cell_start[nb], c.d_np + nb, c.nc, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_inst,
+      (R*)c.pu[nb], c.cell_start[nb], c.d_np + nb, c.nc, c.ring_ptr, c.ring_cell, c.ring_rev, c.dest_mask, c.far_keys,
+      c.far_cap, c.d_inst,
       c.cell_inst, c.cv, (const R*)c.Vr, c.nv, (R*)c.partial, c.list_cap, c.d_counters, c.rebin_tiles);
   c.launches += 1;
   c.cur = nb;
