@@ -25,6 +25,10 @@ namespace pfem2 {
 
 constexpr int kRebinWarps = 8;
 constexpr int kMaxBuckets = 256;
+// resident rebin blocks per SM the registers are capped for: the kernel is
+// bound by dependent loads, and six blocks (48 warps) measured 17% faster
+// than the four that 64 registers allowed, at a few spilled bytes
+constexpr int kRebinMinBlocks = 6;
 
 // ------------------------------------------------------------------ seed
 template <int DIM, typename R>
@@ -477,8 +481,10 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_
 // Advection, second kernel: the queued particles (a warp per queue region),
 // sub-steps redone from their start with the full point location; deletion
 // count and far movers (left the 1-ring of the old cell) recorded here.
+// Registers capped for four resident blocks (its point location is bound by
+// dependent loads: 5% faster than the three blocks 78 registers allowed).
 template <int DIM, typename R>
-__global__ void __launch_bounds__(256) k_advect_left(
+__global__ void __launch_bounds__(256, 4) k_advect_left(
     const int* __restrict__ cell, R* __restrict__ xi, int* __restrict__ newcell, size_t cap,
     const int* __restrict__ d_np, int fast_grid, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
     const R* __restrict__ Vr, int nv, int S, const DevInst* __restrict__ inst, const int* __restrict__ cell_inst,
@@ -719,7 +725,7 @@ constexpr unsigned kLookbackSpinLimit = 1u << 24;
 // flagged in CNT_SCAN_TIMEOUT), then every warp writes its cell's particles,
 // its new_start entry and its projection partials.
 template <int DIM, typename R, bool CHECK, bool PROJ>
-__global__ void __launch_bounds__(kRebinWarps * 32) k_rebin(
+__global__ void __launch_bounds__(kRebinWarps * 32, kRebinMinBlocks) k_rebin(
     const int* __restrict__ old_start, const int* __restrict__ newcell, const R* __restrict__ oxi,
     const R* __restrict__ ou, size_t cap, int* __restrict__ ncell, R* __restrict__ nxi, R* __restrict__ nu,
     int* __restrict__ new_start, int* __restrict__ np_out, int nc, const int* __restrict__ ring_ptr,
