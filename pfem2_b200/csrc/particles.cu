@@ -26,9 +26,13 @@ namespace pfem2 {
 constexpr int kRebinWarps = 8;
 constexpr int kMaxBuckets = 256;
 // resident rebin blocks per SM the registers are capped for: the kernel is
-// bound by dependent loads, and six blocks (48 warps) measured 17% faster
-// than the four that 64 registers allowed, at a few spilled bytes
-constexpr int kRebinMinBlocks = 6;
+// bound by dependent loads, and in 2D FP32 six blocks (48 warps) measured
+// 17% faster than the four that 64 registers allowed, at a few spilled
+// bytes; the 3D and FP64 forms need their registers (no cap)
+template <int DIM, typename R>
+struct RebinMinBlocks {
+  static constexpr int value = (DIM == 2 && sizeof(R) == 4) ? 6 : 1;
+};
 
 // ------------------------------------------------------------------ seed
 template <int DIM, typename R>
@@ -725,7 +729,7 @@ constexpr unsigned kLookbackSpinLimit = 1u << 24;
 // flagged in CNT_SCAN_TIMEOUT), then every warp writes its cell's particles,
 // its new_start entry and its projection partials.
 template <int DIM, typename R, bool CHECK, bool PROJ>
-__global__ void __launch_bounds__(kRebinWarps * 32, kRebinMinBlocks) k_rebin(
+__global__ void __launch_bounds__(kRebinWarps * 32, RebinMinBlocks<DIM, R>::value) k_rebin(
     const int* __restrict__ old_start, const int* __restrict__ newcell, const R* __restrict__ oxi,
     const R* __restrict__ ou, size_t cap, int* __restrict__ ncell, R* __restrict__ nxi, R* __restrict__ nu,
     int* __restrict__ new_start, int* __restrict__ np_out, int nc, const int* __restrict__ ring_ptr,
