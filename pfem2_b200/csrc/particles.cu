@@ -485,10 +485,11 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_
 // Advection, second kernel: the queued particles (a warp per queue region),
 // sub-steps redone from their start with the full point location; deletion
 // count and far movers (left the 1-ring of the old cell) recorded here.
-// Registers capped for four resident blocks (its point location is bound by
-// dependent loads: 5% faster than the three blocks 78 registers allowed).
+// In 2D FP32 the registers are capped for four resident blocks (its point
+// location is bound by dependent loads: 5% faster than the three blocks 78
+// registers allowed); the 3D and FP64 forms keep their registers.
 template <int DIM, typename R>
-__global__ void __launch_bounds__(256, 4) k_advect_left(
+__global__ void __launch_bounds__(256, (DIM == 2 && sizeof(R) == 4) ? 4 : 1) k_advect_left(
     const int* __restrict__ cell, R* __restrict__ xi, int* __restrict__ newcell, size_t cap,
     const int* __restrict__ d_np, int fast_grid, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
     const R* __restrict__ Vr, int nv, int S, const DevInst* __restrict__ inst, const int* __restrict__ cell_inst,
