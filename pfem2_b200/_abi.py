@@ -19,6 +19,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 (FIELD_VX, FIELD_VY, FIELD_VZ, FIELD_P, FIELD_OLD_VX, FIELD_OLD_VY, FIELD_OLD_VZ, FIELD_OLD_P,
  FIELD_PRED_VX, FIELD_PRED_VY, FIELD_PRED_VZ, FIELD_NODE_WEIGHT, FIELD_VORTICITY) = range(13)
 N_FIELDS = 13
+ABI_VERSION = 2  # PFEM2_ABI_VERSION of include/pfem2.h
 
 BC_CONSTANT, BC_PARABOLA = 0, 1
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1

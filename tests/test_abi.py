@@ -70,7 +70,7 @@ def test_exports_cover_header():
     for n in names:
         assert hasattr(lib, n), n
     lib.pfem2_abi_version.restype = C.c_int32
-    assert lib.pfem2_abi_version() == 2
+    assert lib.pfem2_abi_version() == A.ABI_VERSION
 
 
 def test_status_codes_match_header():
@@ -110,7 +110,7 @@ def test_cpp_shim_compiles_and_links():
         "    pfem2b::Solver s(c, m, k); s.seed_particles({4, 4}); s.correct_particles_velocities();\n"
         "    s.move_particles(); s.distribute_particle_velocities_to_grid(); s.fem_step();\n"
         "    std::ofstream f(\"forces.csv\"); s.calculate_loads(3, &f); s.step(); }\n"
-        "  return pfem2_abi_version() == 2 ? 0 : 1; }\n")
+        "  return pfem2_abi_version() == PFEM2_ABI_VERSION ? 0 : 1; }\n")
     with tempfile.TemporaryDirectory() as d:
         cpp = os.path.join(d, "drv.cpp")
         exe = os.path.join(d, "drv")
@@ -119,3 +119,8 @@ def test_cpp_shim_compiles_and_links():
         subprocess.check_call(["g++", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), cpp, "-o", exe,
                                "-L", libdir, "-lpfem2b", f"-Wl,-rpath,{libdir}"])
         assert subprocess.call([exe]) == 0
+
+
+def test_abi_version_mirror_matches_header():
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pfem2.h")).read()
+    assert int(re.search(r"#define PFEM2_ABI_VERSION (\d+)", hdr).group(1)) == A.ABI_VERSION
