@@ -26,12 +26,12 @@ namespace pfem2 {
 constexpr int kRebinWarps = 8;
 constexpr int kMaxBuckets = 256;
 // resident rebin blocks per SM the registers are capped for: the kernel is
-// bound by dependent loads, and in 2D FP32 six blocks (48 warps) measured
-// 17% faster than the four that 64 registers allowed, at a few spilled
-// bytes; the 3D and FP64 forms need their registers (no cap)
+// bound by dependent loads; in 2D FP32 six blocks (48 warps) measured 17%
+// faster than the four that 64 registers allowed, in 3D FP32 four blocks 36%
+// faster than uncapped, each at a few spilled bytes; FP64 is not capped
 template <int DIM, typename R>
 struct RebinMinBlocks {
-  static constexpr int value = (DIM == 2 && sizeof(R) == 4) ? 6 : 1;
+  static constexpr int value = sizeof(R) == 4 ? (DIM == 2 ? 6 : 4) : 1;
 };
 
 // ------------------------------------------------------------------ seed
