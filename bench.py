@@ -138,7 +138,7 @@ KRYLOV_DRAM_BYTES_PER_ITER = (32.973824e6 + 0.421120e6) / 49
 
 
 def pressure_solve_bytes(s, iters, outer):
-    """Algorithmic bytes of the pressure solves, per the model in DESIGN.md.
+    """Algorithmic bytes of the pressure solves.
     One inner CG iteration (inner type R: FP32 for the mixed path) reads
     every operator once with its column indices and streams the vectors:
         A   q = A (z + beta p)         nnz*(R+4) + n*(z, p in; p, q out)
