@@ -72,6 +72,12 @@ class Solver {
       *out << time << "," << c[0] + c[1] << "," << c[2] + c[3] << "," << c[4] << "," << c[0] << "," << c[1] << ","
            << c[2] << "," << c[3] << std::endl;
   }
+  // calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050), 2D: the
+  // nodal vorticity, also kept in PFEM2_FIELD_VORTICITY
+  std::vector<double> calculate_vorticity() {
+    check(pfem2_calculate_vorticity(ctx_));
+    return get_field(PFEM2_FIELD_VORTICITY);
+  }
   // one run() iteration with fused kernels (and a CUDA graph)
   void step() {
     check(pfem2_step(ctx_));

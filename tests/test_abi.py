@@ -109,7 +109,7 @@ def test_cpp_shim_compiles_and_links():
         "  if (argc > 5) { pfem2_config c{}; pfem2_mesh_view m{}; pfem2_case k{};\n"
         "    pfem2b::Solver s(c, m, k); s.seed_particles({4, 4}); s.correct_particles_velocities();\n"
         "    s.move_particles(); s.distribute_particle_velocities_to_grid(); s.fem_step();\n"
-        "    std::ofstream f(\"forces.csv\"); s.calculate_loads(3, &f); s.step(); }\n"
+        "    std::ofstream f(\"forces.csv\"); s.calculate_loads(3, &f); s.step(); s.calculate_vorticity(); }\n"
         "  return pfem2_abi_version() == PFEM2_ABI_VERSION ? 0 : 1; }\n")
     with tempfile.TemporaryDirectory() as d:
         cpp = os.path.join(d, "drv.cpp")
