@@ -4,10 +4,14 @@ Workload (default): the 2D channel with a disk obstacle, ~52k Q1 cells,
 25 particles per cell (~1.3M particles), Re=100, dt=0.002: one `step` is one
 whole PFEM2 time step (correct -> move/locate/reseed -> project -> fractional
 -step FEM with the three Krylov solves) of the mixed-precision path, inputs
-resident in HBM. The FP64 path runs the same steps for the mixed-vs-FP64
-comparison and its field error.
+resident in HBM, every solve to |r| <= rtol |b|. The mixed path runs the
+inner Krylov iterations in FP32 and refines them in FP64; the bench checks
+that its fields stay within 1e-6 relative L2 of the FP64 path after the same
+steps (`fixed_error`), and reports the FP64 path, the all-FP32 path and the
+per-stage error of each FP32 stage beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --only stress|pipe|ensemble|budget|channel   (one leg, its own JSON)
 
 Multi-GPU: a single mesh does not shard, so N ranks run N independent
 replicas of the instance (weak scaling, no data-path collective); value is
@@ -38,13 +42,18 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--h", type=float, default=0.0088, help="cell size of the channel mesh (~52k cells)")
+    ap.add_argument("--rtol", type=float, default=1e-10,
+                    help="relative tolerance |r| <= rtol |b| of every solve, both paths")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--stress-n", type=int, default=2048, help="particle-stress mesh: n x n cells (0 = skip)")
     ap.add_argument("--ensemble-n", type=int, default=64, help="instances of the batched leg (0 = skip)")
     ap.add_argument("--pipe-n", type=int, default=64,
                     help="3D pipe leg: n x n x 4n hex cells, mixed and FP64 (0 = skip)")
+    ap.add_argument("--pipe-rtol", type=float, default=1e-13, help="relative tolerance of the pipe leg's solves")
     ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of the stress and ensemble legs")
+    ap.add_argument("--only", default="all", choices=["all", "channel", "stress", "pipe", "ensemble", "budget"],
+                    help="run one leg alone and print its JSON (for profilers); 'all' prints the bench line")
     return ap.parse_args()
 
 
@@ -55,11 +64,25 @@ def dist_info():
     return rank, world, local
 
 
+METRIC = "timesteps/s (mixed-precision PFEM2 step at fixed error vs FP64; particle updates/s alongside)"
+
+# the bar the mixed path is measured at: relative L2 of velocity and
+# pressure against the FP64 path on the same workload, seed and steps
+FIXED_ERROR = 1e-6
+
+
+def tight(sp, rtol):
+    """both paths solve to |r| <= rtol |b| (no absolute floor), so that
+    their difference is the arithmetic, not the stopping rule"""
+    sp.case.vel_tol = sp.case.p_tol = 0.0
+    sp.case.vel_rtol = sp.case.p_rtol = rtol
+    return sp
+
+
 def workload(args):
     from pfem2_b200 import cases
 
-    sp = cases.channel_disk(h=args.h)
-    return sp
+    return tight(cases.channel_disk(h=args.h), args.rtol)
 
 
 WORKLOAD_DESC = {
@@ -129,16 +152,24 @@ def peaks():
     return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) of one pressure-solve launch of the channel
-# workload per CG iteration, from the ncu capture summarised in
-# profiles/krylov_channel_disk.md (49 iterations, 32.97 MB read + 0.42 MB
-# written); the solve's working set stays in L2, so DRAM traffic is far
-# below the algorithmic bytes
-KRYLOV_DRAM_BYTES_PER_ITER = (32.973824e6 + 0.421120e6) / 49
+def cg_bytes(s, iters, outer):
+    """Algorithmic bytes of the pressure solves by the per-row figures of a
+    CG iteration on a Q1 SpMV: (FP32 values, int32 columns) SpMV 9 nnz x 8 B
+    + row pointer, x, y = 84 B/row in 2D (27 nnz: 228 B/row in 3D), two dot
+    products 16 B/row, three axpy 36 B/row, a Jacobi step 8 B/row: 144 B/row
+    in 2D, 288 B/row in 3D (twice the value bytes in FP64); an FP64 residual
+    refinement reads the FP64 matrix once: 9 x 12 + 4 + 24 = 136 B/row in 2D,
+    27 x 12 + 4 + 24 = 352 B/row in 3D."""
+    info = s.sizes()
+    n, rb = info["rows"], info["real_bytes"]
+    nnz_row = 9 if s.dim == 2 else 27
+    inner = nnz_row * (rb + 4) + 4 + 2 * rb + 2 * 2 * rb + 3 * 3 * rb + 2 * rb
+    outerb = nnz_row * 12 + 4 + 24
+    return n * (iters * inner + outer * outerb)
 
 
 def pressure_solve_bytes(s, iters, outer):
-    """Algorithmic bytes of the pressure solves.
+    """Algorithmic bytes of the pressure solves with the multigrid operators.
     One inner CG iteration (inner type R: FP32 for the mixed path) reads
     every operator once with its column indices and streams the vectors:
         A   q = A (z + beta p)         nnz*(R+4) + n*(z, p in; p, q out)
@@ -154,6 +185,10 @@ def pressure_solve_bytes(s, iters, outer):
     return iters * inner + outer * outerb
 
 
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -167,11 +202,19 @@ def run_ours(args, rank, world, local):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    if args.only != "all":
+        out = {"stress": lambda: stress_leg(args, local, flush), "pipe": lambda: pipe_leg(args, local, flush),
+               "ensemble": lambda: ensemble_leg(args, rank, world, local, flush, None),
+               "budget": lambda: budget_leg(args, local),
+               "channel": lambda: channel_leg(args, local, flush, A.PREC_MIXED, 0)}[args.only]()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
     sp = workload(args)
     s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True)
     s.seed_particles(sp.q, sp.seed, sp.jitter)
     stream = torch.cuda.ExternalStream(s.stream(), device=local)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     for _ in range(args.warmup):
         s.step()
     s.synchronize()
@@ -210,17 +253,20 @@ def run_ours(args, rank, world, local):
     value = steps_per_s * world
     pupd = np_sum / (ms / 1e3) * world
 
-    # roofline: the pressure solve (dominant kernel), bytes from the live iteration counts
+    # roofline of the dominant kernel, the pressure solve, from its live
+    # iteration counts: the CG bytes per row of the scope table (primary) and
+    # the byte model that also counts the multigrid operators (secondary)
     hbm, peak_kind = peaks()
     ps_ms = stages[STAGE_NAMES.index("pressure_solve")]
-    ps_bytes = pressure_solve_bytes(s, it_p, outer_p)
-    achieved = ps_bytes / (ps_ms / 1e3) / 1e9 if ps_ms > 0 else None
+    cgb = cg_bytes(s, it_p, outer_p)
+    mgb = pressure_solve_bytes(s, it_p, outer_p)
+    gbs = (lambda b: b / (ps_ms / 1e3) / 1e9 if ps_ms > 0 else None)
     s.enable_stage_timing(False)
 
     # e2e: the same steps through the C ABI with a host read of the loads and
-    # of the Vx, Vy, P fields every step (pfem2_step_and_read)
-    # (pinned host buffers; the median of three runs of K steps, so that one
-    # host-side stall does not stand for the whole measurement)
+    # of the Vx, Vy, P fields every step (pfem2_step_and_read) into pinned
+    # host buffers; the median of three runs of K steps, so that one
+    # host-side stall does not stand for the whole measurement
     fields = (A.FIELD_VX, A.FIELD_VY, A.FIELD_P)
     loads = torch.zeros(5, dtype=torch.float64, pin_memory=True).numpy()
     out = torch.zeros(sp.mesh.n_vertices * len(fields), dtype=torch.float64, pin_memory=True).numpy()
@@ -238,54 +284,35 @@ def run_ours(args, rank, world, local):
 
         e2e_s = max_over_ranks(e2e_s)
     e2e = {"value": args.steps / e2e_s * world, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
-           "d2h_bytes_per_step": int(out.nbytes + loads.nbytes)}
+           "d2h_bytes_per_step": int(out.nbytes + loads.nbytes),
+           "note": "the time stepper's state stays resident on the device: a step has no host inputs; "
+                   "every step reads Vx, Vy, P and the loads back through pfem2_step_and_read"}
+    s.close()
 
-    # FP64 leg on the same workload: its speed and the mixed-vs-FP64 field error
-    fp64 = None
+    # the FP64 path and the all-FP32 path on the same workload: speed, and
+    # the field error of each path against FP64 after the same steps
+    fp64 = cmp = None
     if not args.no_fp64:
-        s64 = Solver(sp, precision=A.PREC_FP64, device=local, use_graph=True)
-        m2 = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True)
-        s64.seed_particles(sp.q, sp.seed, sp.jitter)
-        m2.seed_particles(sp.q, sp.seed, sp.jitter)
-        nst = args.warmup + args.steps
-        for _ in range(args.warmup):
-            s64.step()
-            m2.step()
-        st64 = torch.cuda.ExternalStream(s64.stream(), device=local)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ms64 = 0.0
-        for _ in range(args.steps):
-            with torch.cuda.stream(st64):
-                flush.zero_()
-            e0.record(st64)
-            s64.step()
-            e1.record(st64)
-            e1.synchronize()
-            ms64 += e0.elapsed_time(e1)
-            m2.step()
-            m2.synchronize()  # both contexts run persistent kernels: no overlap with the next timed step
-        errs = {}
-        for name, f in (("vx", A.FIELD_VX), ("vy", A.FIELD_VY), ("p", A.FIELD_P)):
-            a, b = m2.field(f), s64.field(f)
-            errs[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-        fp64 = {"timesteps_per_s": args.steps / (ms64 / 1e3), "steps_compared": nst,
-                "mixed_vs_fp64_rel_l2": errs}
-        s64.close()
-        m2.close()
+        fp64 = channel_leg(args, local, flush, A.PREC_FP64, 0)
+        fast = channel_leg(args, local, flush, A.PREC_MIXED, A.FP32_ALL)
+        cmp = fixed_error(args, local)
+        fast["rel_l2_vs_fp64"] = cmp.pop("fp32_all")
 
     stress = stress_leg(args, local, flush) if args.stress_n > 0 else None
     pipe = pipe_leg(args, local, flush) if args.pipe_n > 0 else None
     extras = extras_leg(args, local, flush)
     ensemble = None
     if args.ensemble_n > 0:
-        ensemble = ensemble_leg(args, rank, world, local, flush, fp64["timesteps_per_s"] if fp64 else None)
+        ensemble = ensemble_leg(args, rank, world, local, flush, fp64)
+    budget = budget_leg(args, local) if not args.no_fp64 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sp, threads=1, budget_s=20.0)
 
+    cells = sp.mesh.n_cells
     res = {
-        "metric": "timesteps/s (mixed-precision PFEM2 step; particle updates/s and FP64 leg alongside)",
+        "metric": METRIC,
         "value": value,
         "unit": "timesteps/s",
         "n_gpus": world,
@@ -295,37 +322,137 @@ def run_ours(args, rank, world, local):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 particles/assembly/inner Krylov + f64 refinement",
+        "dtype": "f64 fields, particles and assembly; f32 inner Krylov iterations refined in f64",
         "data": "synthetic (programmatic mesh, seeded particles)",
-        "config": dict(WORKLOAD_DESC, cells=sp.mesh.n_cells, vertices=sp.mesh.n_vertices,
+        "config": dict(WORKLOAD_DESC, cells=cells, vertices=sp.mesh.n_vertices,
                        particles=int(np_sum / args.steps), l2="flushed between timed steps (256 MB write)",
+                       solver_stop=f"|r| <= {args.rtol:g} |b| in every solve (both paths)",
                        parallelism=f"replicas x{world}" if world > 1 else "single instance"),
+        "fixed_error": cmp,
         "particle_updates_per_s": pupd,
+        "cell_updates_per_s": cells * value,
         "stage_ms_per_step": {n: stages[i] / args.steps for i, n in enumerate(STAGE_NAMES)},
         "pressure_cg_iters_per_step": it_p / args.steps,
-        "roofline": {"bound": "hbm", "kernel": "k_krylov<float> (pressure solve)",
-                     "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": (achieved / hbm) if achieved else None,
-                     "traffic": KRYLOV_DRAM_BYTES_PER_ITER * it_p / args.steps,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one channel pressure-solve "
-                                       "launch, per CG iteration, times the timed iterations per step",
-                     "algorithmic_bytes_per_step": ps_bytes / args.steps},
+        "roofline": {"bound": "hbm", "kernel": "k_krylov<float, MG> (pressure solve: CG, multigrid preconditioner)",
+                     "achieved": gbs(cgb), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": (gbs(cgb) / hbm) if gbs(cgb) else None,
+                     "algorithmic_bytes_per_step": cgb / args.steps,
+                     "bytes_model": "CG per row: SpMV 9 nnz x (4+4) + 12, 2 dots 16, 3 axpy 36, Jacobi 8 = 144 B "
+                                    "x rows x live iterations, + FP64 refinements 136 B/row",
+                     "traffic": KRYLOV_TRAFFIC_PER_ITER * it_p / args.steps if KRYLOV_TRAFFIC_PER_ITER else None,
+                     "traffic_source": KRYLOV_TRAFFIC_SOURCE,
+                     "with_multigrid_operators": {"achieved": gbs(mgb), "frac": (gbs(mgb) / hbm) if gbs(mgb) else None,
+                                                  "bytes_per_step": mgb / args.steps}},
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clk,
         "fp64": fp64,
+        "fp32_all": fast if not args.no_fp64 else None,
+        "speedups": speedups(value, cells, fp64, ensemble),
         "particle_stress": stress,
         "pipe_3d": pipe,
         "vorticity_and_wall_pushback": extras,
         "ensemble": ensemble,
+        "error_budget": budget,
         "cpu_baseline": cpu,
     }
-    s.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(res), flush=True)
+
+
+# DRAM bytes (read + write) per CG iteration of the channel pressure solve,
+# from an ncu capture of one solve launch in the timed window of this bench
+# (None until captured)
+KRYLOV_TRAFFIC_PER_ITER = None
+KRYLOV_TRAFFIC_SOURCE = None
+
+
+def speedups(value, cells, fp64, ensemble):
+    """like-for-like ratios in cell updates per second"""
+    if not fp64:
+        return None
+    f = fp64["timesteps_per_s"] * cells
+    out = {"mixed_over_fp64_single": value * cells / f}
+    if ensemble:
+        out["ensemble_mixed_over_fp64_single"] = ensemble["cell_updates_per_s"] / f
+    return out
+
+
+def channel_leg(args, local, flush, prec, stages):
+    """the channel workload in one precision: K timed steps after W warm-up"""
+    import torch
+
+    from pfem2_b200.solver import STAGE_NAMES, Solver
+
+    sp = workload(args)
+    s = Solver(sp, precision=prec, fp32_stages=stages, device=local, use_graph=True)
+    s.seed_particles(sp.q, sp.seed, sp.jitter)
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+    for _ in range(args.warmup):
+        s.step()
+    s.synchronize()
+    s.enable_stage_timing(True)
+    s.stage_times(reset=True)
+    ms, iters = 0.0, []
+    for _ in range(args.steps):
+        ms += timed_steps(s, stream, flush, 1)
+        iters.append(s.stats()["iters"][3])
+    stages_ms = s.stage_times()
+    out = {"timesteps_per_s": args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+           "fp32_stages": s.fp32_stages(),
+           "stage_ms_per_step": {n: stages_ms[i] / args.steps for i, n in enumerate(STAGE_NAMES)},
+           "pressure_cg_iters_per_step": iters}
+    s.close()
+    return out
+
+
+def fixed_error(args, local, steps=None):
+    """relative L2 of Vx, Vy, P of the mixed path (and of the all-FP32 path)
+    against the FP64 path after the bench's warm-up + timed steps"""
+    from pfem2_b200 import _abi as A
+    from pfem2_b200.solver import Solver
+
+    n = steps or (args.warmup + args.steps)
+    sp = workload(args)
+    runs = {}
+    for name, prec, stages in (("fp64", A.PREC_FP64, 0), ("mixed", A.PREC_MIXED, 0),
+                               ("fp32_all", A.PREC_MIXED, A.FP32_ALL)):
+        s = Solver(sp, precision=prec, fp32_stages=stages, device=local, use_graph=True)
+        s.seed_particles(sp.q, sp.seed, sp.jitter)
+        for _ in range(n):
+            s.step()
+        runs[name] = [s.field(f) for f in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P)]
+        s.close()
+    err = {k: {f: rel_l2(a, b) for f, a, b in zip(("vx", "vy", "p"), runs[k], runs["fp64"])}
+           for k in ("mixed", "fp32_all")}
+    return {"bar": FIXED_ERROR, "steps_compared": n, "rel_l2_vs_fp64": err["mixed"],
+            "met": max(err["mixed"].values()) <= FIXED_ERROR, "fp32_all": err["fp32_all"]}
+
+
+def budget_leg(args, local, steps=25):
+    """per-stage error budget: one FP32 stage at a time against FP64 on the
+    channel (relative L2 of Vx, Vy, P after `steps` steps)"""
+    from pfem2_b200 import _abi as A
+    from pfem2_b200.solver import Solver
+
+    sp = workload(args)
+    sets = (("fp64", A.PREC_FP64, 0), ("krylov", A.PREC_MIXED, A.FP32_KRYLOV),
+            ("particles", A.PREC_MIXED, A.FP32_PARTICLES), ("assembly", A.PREC_MIXED, A.FP32_ASSEMBLY),
+            ("pressure_rhs", A.PREC_MIXED, A.FP32_PRESSURE_RHS), ("all", A.PREC_MIXED, A.FP32_ALL))
+    runs = {}
+    for name, prec, stages in sets:
+        s = Solver(sp, precision=prec, fp32_stages=stages, device=local, use_graph=True)
+        s.seed_particles(sp.q, sp.seed, sp.jitter)
+        for _ in range(steps):
+            s.step()
+        runs[name] = [s.field(f) for f in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P)]
+        s.close()
+    return {"workload": "the bench channel", "steps": steps,
+            "fp32_stage_rel_l2_vs_fp64": {k: {f: rel_l2(a, b) for f, a, b in zip(("vx", "vy", "p"), v, runs["fp64"])}
+                                          for k, v in runs.items() if k != "fp64"}}
 
 
 def timed_steps(solver, stream, flush, steps):
@@ -398,8 +525,9 @@ def extras_leg(args, local, flush):
 
 def pipe_leg(args, local, flush):
     """3D pipe Poiseuille (hex mesh n x n x 4n, 3x3x3 particles per cell,
-    dp/dn driven): the mixed path (FP32 inner solves, FP64 refinement) and
-    the plain FP64 path on the same steps, one context after the other"""
+    dp/dn driven): the mixed path (FP32 inner solves refined in FP64) and the
+    FP64 path on the same steps, one context after the other; the pressure
+    solve's bytes by the CG per-row figure of the scope table (288 B/row in 3D)"""
     import torch
 
     from pfem2_b200 import _abi as A
@@ -407,11 +535,13 @@ def pipe_leg(args, local, flush):
     from pfem2_b200.solver import STAGE_NAMES, Solver
 
     n = args.pipe_n
-    sp = cases.pipe_3d(ny=n, nz=n, nx=4 * n)
+    sp = tight(cases.pipe_3d(ny=n, nz=n, nx=4 * n), args.pipe_rtol)
     k, warm = args.extra_steps, 2
     out = {"workload": f"3D pipe Poiseuille, circular section mapped from a square, {n}x{n}x{4 * n} Q1 hex cells, "
                        f"nu=0.01, dt=0.001, dp/dn=1, 3x3x3 particles/cell",
-           "cells": sp.mesh.n_cells, "vertices": sp.mesh.n_vertices, "steps": k, "warmup": warm}
+           "cells": sp.mesh.n_cells, "vertices": sp.mesh.n_vertices, "steps": k, "warmup": warm,
+           "solver_stop": f"|r| <= {args.pipe_rtol:g} |b|"}
+    hbm, kind = peaks()
     fields = {}
     for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
         s = Solver(sp, precision=prec, device=local, use_graph=True)
@@ -422,26 +552,44 @@ def pipe_leg(args, local, flush):
         s.synchronize()
         s.enable_stage_timing(True)
         s.stage_times(reset=True)
-        ms = timed_steps(s, stream, flush, k)
+        tot, e0, e1 = 0.0, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        it_p = outer_p = 0
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0.record(stream)
+            s.step()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+            st = s.stats(check=False)
+            it_p += st["iters"][3]
+            outer_p += st["refinements_p"]
+        ms = tot
         stages = s.stage_times()
-        st = s.stats()
+        ps_ms = stages[STAGE_NAMES.index("pressure_solve")]
+        cgb = cg_bytes(s, it_p, outer_p)
         out[name] = {"timesteps_per_s": k / (ms / 1e3), "ms_per_step": ms / k,
                      "stage_ms_per_step": {nm: stages[i] / k for i, nm in enumerate(STAGE_NAMES)},
-                     "pressure_cg_iters_last_step": st["iters"][3], "particles": st["n_particles"]}
+                     "pressure_cg_iters_per_step": it_p / k, "particles": st["n_particles"],
+                     "status": st["status"],
+                     "pressure_solve_roofline": {"GB/s": cgb / (ps_ms / 1e3) / 1e9, "frac": cgb / (ps_ms / 1e3) / 1e9 / hbm,
+                                                 "peak": hbm, "peak_kind": kind,
+                                                 "bytes_per_step": cgb / k}}
         if name == "mixed":
             out["particle_updates_per_s"] = st["n_particles"] / (ms / k / 1e3)
         fields[name] = [s.field(f) for f in (A.FIELD_VX, A.FIELD_P)]
         s.close()
-    out["mixed_vs_fp64_rel_l2"] = {
-        nm: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-        for nm, a, b in zip(("vx", "p"), fields["mixed"], fields["fp64"])}
+    out["mixed_vs_fp64_rel_l2"] = {nm: rel_l2(a, b) for nm, a, b in zip(("vx", "p"), fields["mixed"], fields["fp64"])}
+    out["fixed_error_met"] = max(out["mixed_vs_fp64_rel_l2"].values()) <= FIXED_ERROR
     out["mixed_over_fp64"] = out["mixed"]["timesteps_per_s"] / out["fp64"]["timesteps_per_s"]
     return out
 
 
 def stress_leg(args, local, flush):
     """particle kernels alone (advect + project + correct) on a frozen field:
-    unit square n x n, 4x4 particles per cell uniform in their sub-cells"""
+    unit square n x n, 4x4 particles per cell uniform in their sub-cells,
+    FP32 particle coordinates and velocities (PFEM2_FP32_PARTICLES)"""
     import torch
 
     from pfem2_b200 import _abi as A
@@ -450,7 +598,8 @@ def stress_leg(args, local, flush):
 
     n = args.stress_n
     sp = cases.stress_2d(n=n)
-    s = Solver(sp, precision=A.PREC_MIXED, device=local, use_graph=True, particles_only=True, capacity_factor=3.0)
+    s = Solver(sp, precision=A.PREC_MIXED, fp32_stages=A.FP32_ALL, device=local, use_graph=True,
+               particles_only=True, capacity_factor=3.0)
     ux, uy = sp.meta["ux"], sp.meta["uy"]
     for f, v in ((A.FIELD_VX, ux), (A.FIELD_VY, uy), (A.FIELD_PRED_VX, ux), (A.FIELD_PRED_VY, uy)):
         s.set_field(f, v)
@@ -469,14 +618,16 @@ def stress_leg(args, local, flush):
     npart = 0.5 * (st0["n_particles"] + st["n_particles"])
     nc, nv = sp.mesh.n_cells, sp.mesh.n_vertices
     hbm, kind = peaks()
-    # algorithmic bytes (FP32 SoA): advect reads cell+xi+u (20 B) and writes
-    # xi+u+newcell (20 B) per particle; the rebin reads newcell+xi+u (20 B)
-    # and writes cell+xi+u (20 B) per particle plus 2 offsets and 48 B of
-    # projection partials per cell; the node gather reads the partials and
-    # writes 12 B per node.
-    b_adv = 40.0 * npart
-    b_reb = 40.0 * npart + (8 + 48) * nc
-    b_nod = 48.0 * nc + 28.0 * nv
+    # algorithmic bytes (FP32 SoA, the per-unit figures of the scope table):
+    # advect with the correction fused: read cell + xi + u (20 B), write
+    # xi + u + new cell (20 B) per particle, the nodal velocity and its
+    # increment once (16 B per node); re-sort with check and projection
+    # partials fused: read + write the particle state (2 x 20 B) plus keys
+    # and offsets (8 B) per particle, 48 B of partials and a 4 B offset per
+    # cell; node gather: the partials (48 B per cell) in, 12 B per node out
+    b_adv = 40.0 * npart + 16.0 * nv
+    b_reb = 48.0 * npart + 52.0 * nc
+    b_nod = 48.0 * nc + 12.0 * nv
     adv_ms = stages[STAGE_NAMES.index("advect")] / k
     reb_ms = stages[STAGE_NAMES.index("rebin")] / k
     nod_ms = stages[STAGE_NAMES.index("project_nodes")] / k
@@ -488,7 +639,8 @@ def stress_leg(args, local, flush):
         "particle_updates_per_s": npart * k / (ms / 1e3),
         "advect": {"ms": adv_ms, "GB/s": gbs(b_adv, adv_ms), "frac": gbs(b_adv, adv_ms) / hbm if adv_ms else None},
         "rebin": {"ms": reb_ms, "GB/s": gbs(b_reb, reb_ms), "frac": gbs(b_reb, reb_ms) / hbm if reb_ms else None},
-        "project_nodes": {"ms": nod_ms, "GB/s": gbs(b_nod, nod_ms)},
+        "project_nodes": {"ms": nod_ms, "GB/s": gbs(b_nod, nod_ms), "frac": gbs(b_nod, nod_ms) / hbm if nod_ms else None},
+        "bytes_per_step": {"advect": b_adv, "rebin": b_reb, "project_nodes": b_nod},
         "step_GB/s": gbs(b_adv + b_reb + b_nod, ms / k), "peak": hbm, "peak_kind": kind,
         "deleted_per_step": st["deleted"], "far_movers": st["far"],
     }
@@ -498,16 +650,16 @@ def stress_leg(args, local, flush):
 
 def ensemble_leg(args, rank, world, local, flush, fp64_single):
     """many independent channel instances of uneven size in one batch:
-    every stage is one launch for all of them; with N ranks every rank runs
-    its longest-processing-time share of the instances (no collective but
-    the max-over-ranks time)"""
+    every stage is one launch for all of them (mixed path, the bench's
+    relative tolerance); with N ranks every rank runs its longest-processing-
+    time share of the instances (no collective but the max-over-ranks time)"""
     import torch
 
     from pfem2_b200 import _abi as A
     from pfem2_b200 import cases, sharding
     from pfem2_b200.solver import Solver
 
-    all_specs = cases.ensemble(n=args.ensemble_n)
+    all_specs = [tight(sp, args.rtol) for sp in cases.ensemble(n=args.ensemble_n)]
     specs = all_specs
     if world > 1:
         _, specs = sharding.shard(all_specs, rank, world)
@@ -531,7 +683,6 @@ def ensemble_leg(args, rank, world, local, flush, fp64_single):
         "ms_per_batch_step": ms / args.extra_steps, "instance_timesteps_per_s": inst_steps,
         "cell_updates_per_s": cells * args.extra_steps / (ms / 1e3),
         "max_pressure_cg_iters": st["iters"][3],
-        "vs_fp64_single_instance_timesteps_per_s": (inst_steps / fp64_single) if fp64_single else None,
     }
     s.close()
     return out
@@ -569,7 +720,8 @@ def run_reference(args, rank, world):
     o = O.Oracle(sp.mesh, sp.case, movement_steps=sp.movement_steps, max_per_part=sp.max_per_part,
                  threads=threads)
     o.seed_particles(sp.q, sp.seed, sp.jitter)
-    for _ in range(max(1, min(args.warmup, 2))):
+    warm = max(1, min(args.warmup, 2))
+    for _ in range(warm):
         o.step(1)
     budget = 120.0
     n = 0
@@ -583,14 +735,14 @@ def run_reference(args, rank, world):
     v = n / el
     res = {
         "impl": "reference",
-        "metric": "timesteps/s (mixed-precision PFEM2 step; particle updates/s and FP64 leg alongside)",
-        "value": v, "unit": "timesteps/s", "n_gpus": world, "steps": n, "warmup": args.warmup,
+        "metric": METRIC,
+        "value": v, "unit": "timesteps/s", "n_gpus": world, "steps": n, "warmup": warm,
         "ms_per_step": el / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (programmatic mesh, seeded particles)",
         "config": dict(WORKLOAD_DESC, cells=sp.mesh.n_cells, parallelism="host cores"),
         "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": threads, "kind": "port",
                          "sample": f"{n} whole time steps (of {args.steps} requested, 120 s cap) after "
-                                   f"{max(1, min(args.warmup, 2))} warm-up steps; deal.II, which the "
+                                   f"{warm} warm-up steps (of {args.warmup} requested); deal.II, which the "
                                    f"reference needs, is not installed, so its FP64 CPU restatement runs"},
         "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -38,7 +38,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define PFEM2_ABI_VERSION 2
+#define PFEM2_ABI_VERSION 3
 
 typedef enum {
   PFEM2_OK = 0,
@@ -54,8 +54,24 @@ typedef enum {
 
 typedef enum {
   PFEM2_PREC_FP64 = 0,   /* everything FP64 ("plain" path) */
-  PFEM2_PREC_MIXED = 1   /* FP32 particles/assembly/inner Krylov, FP64 refinement, dots, loads */
+  PFEM2_PREC_MIXED = 1   /* the stages of pfem2_config.fp32_stages in FP32; FP64 refinement, dots, loads */
 } pfem2_precision;
+
+/* Stages that a PFEM2_PREC_MIXED context runs in FP32 (pfem2_config.fp32_stages,
+ * a bit mask; 0 selects PFEM2_FP32_DEFAULT). Everything not listed stays FP64:
+ * the nodal fields, the Krylov residual refinement, dot products and norms,
+ * the load integrals. The default keeps the fields within 1e-6 relative L2
+ * of the FP64 path: only the inner Krylov iterations run in FP32, their
+ * result refined in FP64 to the FP64 tolerance. Each further stage in FP32
+ * moves the fields by 1e-5 to 4e-4 relative L2 after 25 steps of the 52k-cell
+ * disk channel (particles: 8e-6 vx, 4e-5 p; prediction/correction right-hand
+ * sides: 2e-5 vx, 2e-4 p; pressure right-hand side: 7e-6 vx, 4e-4 p). */
+#define PFEM2_FP32_PARTICLES 1  /* particle state (reference coordinates, velocities) and the particle kernels */
+#define PFEM2_FP32_ASSEMBLY 2   /* right-hand sides of the prediction and correction systems */
+#define PFEM2_FP32_KRYLOV 4     /* inner Krylov iterations (FP64 reliable updates to the FP64 tolerance) */
+#define PFEM2_FP32_PRESSURE_RHS 8 /* right-hand side of the pressure Poisson system */
+#define PFEM2_FP32_ALL 15       /* every stage above */
+#define PFEM2_FP32_DEFAULT PFEM2_FP32_KRYLOV
 
 typedef enum {
   PFEM2_FIELD_VX = 0, PFEM2_FIELD_VY = 1, PFEM2_FIELD_VZ = 2, PFEM2_FIELD_P = 3,
@@ -118,8 +134,17 @@ typedef struct {
    * unpreconditioned residual norm as in deal.II (cylinder2D/cylinder2D.cc:736-779). */
   double vel_tol, p_tol;
   int32_t max_iter;
-  int32_t vel_solver;             /* pfem2_solver_kind */
-  int32_t p_solver;               /* pfem2_solver_kind */
+  /* pfem2_solver_kind of the velocity systems (prediction and correction):
+   * CG or BiCGStab, both with the Jacobi preconditioner of the reference's
+   * velocity solves (cylinder2D/cylinder2D.cc:736-758). */
+  int32_t vel_solver;
+  /* pfem2_solver_kind of the pressure system: CG with the algebraic multigrid
+   * preconditioner (the reference's Trilinos cases use AMG,
+   * TurekBenchmarkCuda/TurekBenchmark.cc:731-797), or BiCGStab with the
+   * Jacobi preconditioner (the reference's serial cases use BiCGStab with
+   * SSOR, cylinder2D/cylinder2D.cc:760-779). Every instance of a context
+   * must name the same kinds (PFEM2_INVALID_ARG otherwise). */
+  int32_t p_solver;
   int32_t reassemble_every_step;  /* 1: rebuild matrices each step like the reference */
   /* 1: wall push-back after the projection (nacaAirfoil/pfem2particle.cpp:
    * 919-952): for every zero_after_projection vertex whose projected
@@ -127,6 +152,12 @@ typedef struct {
    * cells around it loses N_vertex(xi_p) times that velocity, before the
    * vertex is set to zero. 0: the vertex is only set to zero. */
   int32_t wall_pushback;
+  int32_t pad_;
+  /* Relative tolerances (0 = off): a solve stops once its residual norm is
+   * <= max(tol, rtol * |b|), |b| the norm of its right-hand side (deal.II's
+   * SolverControl with the tolerance scaled by the right-hand side). Tight
+   * values make two runs that differ only in arithmetic comparable. */
+  double vel_rtol, p_rtol;
 } pfem2_case;
 
 /* A mesh of one instance (host arrays, copied by pfem2_add_instance). */
@@ -153,6 +184,9 @@ typedef struct {
    * PFEM2_FIELD_PRED_V*: after each step V is reset to the frozen field and
    * V_old to the new projection (the particle-kernel stress workload). */
   int32_t particles_only;
+  /* PFEM2_PREC_MIXED only: the PFEM2_FP32_* stages that run in FP32
+   * (0 = PFEM2_FP32_DEFAULT). Ignored by PFEM2_PREC_FP64. */
+  int32_t fp32_stages;
 } pfem2_config;
 
 typedef struct pfem2_ctx pfem2_ctx;
@@ -203,7 +237,8 @@ pfem2_status pfem2_project(pfem2_ctx* ctx);
 pfem2_status pfem2_fem_step(pfem2_ctx* ctx);
 /* calculate_loads (TurekBenchmark/pfem2particle.cpp:920-970): out[5] =
  * {Cx_nu, Cx_p, Cy_nu, Cy_p, p(probe_a) - p(probe_b)} (2D). In 3D out =
- * {Fx_p, Fy_p, Fz_p, 0, p(probe_a) - p(probe_b)} (tubePoiseuille3D/pfem2particle.cpp:693-737). */
+ * {Fx_p, Fy_p, Fz_p, 0, p_probe} with p_probe the mean pressure over the
+ * probe vertices that are set (tubePoiseuille3D/pfem2particle.cpp:693-737). */
 pfem2_status pfem2_loads(pfem2_ctx* ctx, int32_t instance, int32_t patch_id, double out[5]);
 /* calculate_vorticity (cylinderDyM/pfem2particle.cpp:1000-1050), 2D: at the
  * QGauss(2) points of every cell w = sum_i (dN_i/dx Vy_i - dN_i/dy Vx_i),
@@ -268,20 +303,28 @@ int32_t pfem2_abi_version(void);
  * projection of distribute_particle_velocities_to_grid on caller-owned
  * device buffers, FP64, allocating nothing. Its per-cell scratch is a fixed
  * device array of PFEM2_NOALLOC_MAX_CELLS cells held by every GPU that loads
- * the library; larger meshes are rejected with PFEM2_INVALID_ARG. The first
- * call on a device looks the array up (make it before any stream capture);
- * calls that overlap on the GPU race on the shared array.
+ * the library; larger meshes are rejected with PFEM2_INVALID_ARG. A call on
+ * a stream that is not being captured looks the array's device address up
+ * (the first call on a device must come before any stream capture, which
+ * then reuses the address; PFEM2_BAD_STATE otherwise); calls that overlap on
+ * the GPU race on the shared array.
  *   vertex_cell_ptr [n_vertices+1], vertex_cell / vertex_cell_local: cells
- *   around each vertex (ascending) and the vertex's local index there;
- *   cell_start [n_cells+1]: particle offsets, particles sorted by cell;
- *   xi, u [n_particles][dim]; out node_u [n_vertices][dim], node_w [n_vertices]
- *   (node_u = 0 where node_w = 0); stream: a cudaStream_t or NULL. */
+ *   around each vertex (ascending) and the vertex's local index there, each
+ *   in [0, n_cells) / [0, 2^dim) (a vertex with an entry out of range gets
+ *   NaN in node_u and node_w, nothing else is read for it);
+ *   cell_start [n_cells+1]: particle offsets (non-decreasing, within xi and
+ *   u), particles sorted by cell; xi, u [n_particles][dim];
+ *   zero_flag [n_vertices] or NULL: vertices whose velocity is set to 0 after
+ *   the projection (the wall DoFs of pfem2_case.zero_after_projection_mask,
+ *   TurekBenchmarkCuda/pfem2particle.cu:866-869; NULL zeroes none);
+ *   out node_u [n_vertices][dim], node_w [n_vertices] (node_u = 0 where
+ *   node_w = 0); stream: a cudaStream_t or NULL. */
 #define PFEM2_NOALLOC_MAX_CELLS 65536
 pfem2_status pfem2_project_noalloc(int32_t dim, int32_t n_cells, int32_t n_vertices,
                                    const int32_t* vertex_cell_ptr, const int32_t* vertex_cell,
                                    const int32_t* vertex_cell_local, const int32_t* cell_start,
-                                   const double* xi, const double* u, double* node_u, double* node_w,
-                                   void* stream);
+                                   const double* xi, const double* u, const uint8_t* zero_flag,
+                                   double* node_u, double* node_w, void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

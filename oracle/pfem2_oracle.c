@@ -1150,8 +1150,15 @@ static int solve_bicgstab(const omodel* m, const double* A, double* x, const dou
   return it;
 }
 
-static int solve(omodel* m, int slot, const double* A, double* x, const double* b, int kind, int pk, double tol) {
+/* tol: the absolute tolerance; rtol > 0 raises it to rtol |b| (the library's
+ * relative stopping rule, pfem2_case.vel_rtol / p_rtol) */
+static int solve(omodel* m, int slot, const double* A, double* x, const double* b, int kind, int pk, double tol,
+                 double rtol) {
   double res = 0.0;
+  if (rtol > 0.0) {
+    const double bn = sqrt(dot(m->nv, b, b));
+    if (rtol * bn > tol) tol = rtol * bn;
+  }
   int it = kind == PFEM2_SOLVER_CG ? solve_cg(m, A, x, b, pk, tol, m->cs.max_iter, &res)
                                    : solve_bicgstab(m, A, x, b, pk, tol, m->cs.max_iter, &res);
   m->iters[slot] = it;
@@ -1182,7 +1189,7 @@ int or_fem_step(omodel* m, int precond_p) {
       apply_rhs_bc(m, rhs, m->isdir[c], m->shift_pred[c]);
       for (int i = 0; i < nv; ++i)
         if (m->isdir[c][i]) pred[i] = m->dirval[c][i];
-      bad |= solve(m, c, m->Apred[c], pred, rhs, m->cs.vel_solver, 0, m->cs.vel_tol);
+      bad |= solve(m, c, m->Apred[c], pred, rhs, m->cs.vel_solver, 0, m->cs.vel_tol, m->cs.vel_rtol);
     }
     const double* pr[3];
     for (int d = 0; d < dim; ++d) pr[d] = m->f[PFEM2_FIELD_PRED_VX + d];
@@ -1191,12 +1198,12 @@ int or_fem_step(omodel* m, int precond_p) {
     double* P = m->f[PFEM2_FIELD_P];
     for (int i = 0; i < nv; ++i)
       if (m->isdir[3][i]) P[i] = m->dirval[3][i];
-    bad |= solve(m, 3, m->Kp, P, rhs, m->cs.p_solver, precond_p, m->cs.p_tol);
+    bad |= solve(m, 3, m->Kp, P, rhs, m->cs.p_solver, precond_p, m->cs.p_tol, m->cs.p_rtol);
     for (int c = 0; c < dim; ++c) {
       rhs_correction(m, c, P, rhs);
       for (int i = 0; i < nv; ++i)
         if (m->isdir[c][i]) { rhs[i] = 0.0; m->corr[c][i] = 0.0; }
-      bad |= solve(m, 4 + c, m->Mc[c], m->corr[c], rhs, m->cs.vel_solver, 0, m->cs.vel_tol);
+      bad |= solve(m, 4 + c, m->Mc[c], m->corr[c], rhs, m->cs.vel_solver, 0, m->cs.vel_tol, m->cs.vel_rtol);
       for (int i = 0; i < nv; ++i) m->f[PFEM2_FIELD_VX + c][i] = m->f[PFEM2_FIELD_PRED_VX + c][i] + m->corr[c][i];
     }
     memcpy(m->f[PFEM2_FIELD_OLD_P], P, sizeof(double) * nv);
@@ -1239,9 +1246,19 @@ void or_loads(const omodel* m, int patch, double* out) {
       }
     }
   }
+  /* 2D: pressure difference p(a) - p(b) (TurekBenchmark/pfem2particle.cpp:953-956);
+   * 3D: the pressure at the probe, the mean over the listed probe DoFs
+   * (tubePoiseuille3D/pfem2particle.cpp:726-731) */
   double dp = 0.0;
-  if (m->cs.probe_a >= 0) dp += P[m->cs.probe_a];
-  if (m->cs.probe_b >= 0) dp -= P[m->cs.probe_b];
+  if (dim == 2) {
+    if (m->cs.probe_a >= 0) dp += P[m->cs.probe_a];
+    if (m->cs.probe_b >= 0) dp -= P[m->cs.probe_b];
+  } else {
+    int np = 0;
+    if (m->cs.probe_a >= 0) { dp += P[m->cs.probe_a]; ++np; }
+    if (m->cs.probe_b >= 0) { dp += P[m->cs.probe_b]; ++np; }
+    if (np) dp /= np;
+  }
   if (dim == 2) {
     double s = m->cs.rho * m->cs.load_umean * m->cs.load_umean * m->cs.load_diam;
     out[0] = 2.0 * Fx_nu / s; out[1] = 2.0 * Fx_p / s;

@@ -15,11 +15,15 @@ STATUS_NAMES = {
 }
 
 PREC_FP64, PREC_MIXED = 0, 1
+# PFEM2_FP32_* stage bits of Config.fp32_stages
+FP32_PARTICLES, FP32_ASSEMBLY, FP32_KRYLOV, FP32_PRESSURE_RHS = 1, 2, 4, 8
+FP32_ALL = FP32_PARTICLES | FP32_ASSEMBLY | FP32_KRYLOV | FP32_PRESSURE_RHS
+FP32_DEFAULT = FP32_KRYLOV
 
 (FIELD_VX, FIELD_VY, FIELD_VZ, FIELD_P, FIELD_OLD_VX, FIELD_OLD_VY, FIELD_OLD_VZ, FIELD_OLD_P,
  FIELD_PRED_VX, FIELD_PRED_VY, FIELD_PRED_VZ, FIELD_NODE_WEIGHT, FIELD_VORTICITY) = range(13)
 N_FIELDS = 13
-ABI_VERSION = 2  # PFEM2_ABI_VERSION of include/pfem2.h
+ABI_VERSION = 3  # PFEM2_ABI_VERSION of include/pfem2.h
 
 BC_CONSTANT, BC_PARABOLA = 0, 1
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
@@ -46,7 +50,8 @@ class Case(C.Structure):
         ("vel_tol", C.c_double), ("p_tol", C.c_double),
         ("max_iter", C.c_int32), ("vel_solver", C.c_int32), ("p_solver", C.c_int32),
         ("reassemble_every_step", C.c_int32),
-        ("wall_pushback", C.c_int32),
+        ("wall_pushback", C.c_int32), ("pad_", C.c_int32),
+        ("vel_rtol", C.c_double), ("p_rtol", C.c_double),
     ]
 
 
@@ -65,7 +70,7 @@ class Config(C.Structure):
         ("particles_per_cell_max", C.c_int32),
         ("particle_capacity_factor", C.c_double),
         ("far_mover_capacity", C.c_int32), ("use_graph", C.c_int32),
-        ("particles_only", C.c_int32),
+        ("particles_only", C.c_int32), ("fp32_stages", C.c_int32),
     ]
 
 

@@ -122,7 +122,7 @@ def pipe_3d(ny=64, nz=64, nx=256, steps=100, q=(3, 3, 3), dpdx=-1.0, seed=0, jit
         mu=nu, rho=1.0, dt=0.001,
         vel_bcs=[[const(2)], [const(2)], [const(2)]],
         p_bcs=[const(1)], open_ids=(0, 1), open_flux=dpdx,
-        probes=(M.nearest_vertex(mesh, (0.0, 0.0, 0.0)), M.nearest_vertex(mesh, (4.0, 0.0, 0.0))),
+        probes=(M.nearest_vertex(mesh, (2.0, 0.0, 0.0)), -1),
         **kw)
     return CaseSpec("pipe_3d", mesh, cs, q, seed, jitter, steps, meta={"nu": nu, "dpdx": dpdx})
 

@@ -299,9 +299,26 @@ static pfem2_status do_setup(Ctx& c) {
             if (((vb >> (fc / 2)) & 1) == fc % 2) zflag[cv[(size_t)ce * NV + vb]] = 1;
         }
   }
+  // solver kinds: one per system kind for the whole batch
+  for (auto& in : c.inst) {
+    const pfem2_case& k0 = c.inst[0].cs;
+    const bool okk = (in.cs.vel_solver == PFEM2_SOLVER_CG || in.cs.vel_solver == PFEM2_SOLVER_BICGSTAB) &&
+                     (in.cs.p_solver == PFEM2_SOLVER_CG || in.cs.p_solver == PFEM2_SOLVER_BICGSTAB);
+    if (!okk || in.cs.vel_solver != k0.vel_solver || in.cs.p_solver != k0.p_solver) {
+      set_error("vel_solver / p_solver: PFEM2_SOLVER_CG or PFEM2_SOLVER_BICGSTAB, the same in every instance");
+      return PFEM2_INVALID_ARG;
+    }
+    if (!(in.cs.vel_rtol >= 0.0) || !(in.cs.p_rtol >= 0.0) || !(in.cs.vel_tol >= 0.0) || !(in.cs.p_tol >= 0.0)) {
+      set_error("solver tolerances must be >= 0");
+      return PFEM2_INVALID_ARG;
+    }
+  }
+  c.vel_bicg = c.inst[0].cs.vel_solver == PFEM2_SOLVER_BICGSTAB;
+  c.p_bicg = c.inst[0].cs.p_solver == PFEM2_SOLVER_BICGSTAB;
+  if (c.p_bicg) c.two_level = false;
   // instance table
   c.h_inst.resize(c.inst.size());
-  std::vector<double> tols(2 * c.inst.size());
+  std::vector<double> tols(4 * c.inst.size());
   std::vector<int> maxit(c.inst.size());
   for (size_t i = 0; i < c.inst.size(); ++i) {
     auto& in = c.inst[i];
@@ -314,8 +331,11 @@ static pfem2_status do_setup(Ctx& c) {
     d.max_per_part = c.cfg.max_particles_per_cell_part;
     d.dt_sub = in.cs.dt / c.cfg.movement_steps;
     d.v_off = in.v_off; d.nv_pad = in.nv_pad; d.c_off = in.c_off; d.nc = in.nc;
+    const size_t ni = c.inst.size();
     tols[i] = in.cs.vel_tol;
-    tols[c.inst.size() + i] = in.cs.p_tol;
+    tols[ni + i] = in.cs.p_tol;
+    tols[2 * ni + i] = in.cs.vel_rtol;
+    tols[3 * ni + i] = in.cs.p_rtol;
     maxit[i] = in.cs.max_iter > 0 ? in.cs.max_iter : 10000;
   }
   // uploads
@@ -328,15 +348,15 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(upload(&c.v2c_cell, v2c_cell));
   PFEM2_TRY(upload(&c.v2c_loc, v2c_loc));
   PFEM2_TRY(upload(&c.v2c_dir, v2c_dir));
-  if (c.mixed) {
+  if (c.pmixed) {
     float* p = nullptr;
     PFEM2_TRY(upload(&p, v2c_dirf));
     c.v2c_dir_r = p;
   } else {
     c.v2c_dir_r = c.v2c_dir;
   }
-  if (dim == 2) PFEM2_TRY((c.mixed ? upload_cell_geo<2, float>(c, X, cv) : upload_cell_geo<2, double>(c, X, cv)));
-  else PFEM2_TRY((c.mixed ? upload_cell_geo<3, float>(c, X, cv) : upload_cell_geo<3, double>(c, X, cv)));
+  if (dim == 2) PFEM2_TRY((c.pmixed ? upload_cell_geo<2, float>(c, X, cv) : upload_cell_geo<2, double>(c, X, cv)));
+  else PFEM2_TRY((c.pmixed ? upload_cell_geo<3, float>(c, X, cv) : upload_cell_geo<3, double>(c, X, cv)));
   PFEM2_TRY(upload(&c.ring_ptr, ring_ptr));
   PFEM2_TRY(upload(&c.ring_cell, ring_cell));
   {
@@ -399,7 +419,7 @@ static pfem2_status do_setup(Ctx& c) {
     PFEM2_TRY(dalloc(&c.corr[k], nv));
     PFEM2_TRY(dalloc(&c.rhs[k], nv));
   }
-  const size_t rs = c.mixed ? 4 : 8;
+  const size_t rs = c.pmixed ? 4 : 8;
   {
     void* p;
     PFEM2_CUDA(cudaMalloc(&p, rs * 3 * nv));
@@ -439,7 +459,7 @@ static pfem2_status alloc_particles(Ctx& c, size_t seeded) {
   size_t cap = (size_t)std::ceil(seeded * f) + 1024;
   if (cap > (size_t)2000000000) cap = 2000000000;
   if ((int)cap <= c.pcap) return PFEM2_OK;
-  const size_t rs = c.mixed ? 4 : 8;
+  const size_t rs = c.pmixed ? 4 : 8;
   for (int b = 0; b < 2; ++b) {
     if (c.pcell[b]) cudaFree(c.pcell[b]);
     if (c.pxi[b]) cudaFree(c.pxi[b]);
@@ -481,6 +501,7 @@ static pfem2_status check_counters(Ctx& c, bool sync) {
   }
   if (cnt[CNT_SCAN_TIMEOUT]) {
     set_error("rebin: a wait of the single-pass scan timed out");
+    c.failed = true;
     return PFEM2_TIMEOUT;
   }
   if (cnt[CNT_FAR_OVERFLOW]) {
@@ -581,9 +602,18 @@ struct pfem2_ctx {
       return PFEM2_BAD_STATE;                       \
     }                                               \
   } while (0)
+// a context whose device-side wait timed out refuses further stepping
+#define LIVE_CHECK(ctx)                                                          \
+  do {                                                                           \
+    if ((ctx)->c.failed) {                                                       \
+      set_error("a device-side wait of this context timed out: destroy it");   \
+      return PFEM2_BAD_STATE;                                                    \
+    }                                                                            \
+  } while (0)
 #define SEED_CHECK(ctx)                             \
   do {                                              \
     SETUP_CHECK(ctx);                               \
+    LIVE_CHECK(ctx);                                \
     if (!(ctx)->c.seeded) {                         \
       set_error("no particles (seed first)");       \
       return PFEM2_BAD_STATE;                       \
@@ -613,7 +643,21 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   Ctx& c = x->c;
   c.cfg = *cfg;
   c.dim = cfg->dim;
-  c.mixed = cfg->precision == PFEM2_PREC_MIXED;
+  if (cfg->precision == PFEM2_PREC_MIXED) {
+    const int m = cfg->fp32_stages ? cfg->fp32_stages : PFEM2_FP32_DEFAULT;
+    c.pmixed = (m & PFEM2_FP32_PARTICLES) != 0;
+    c.amixed = (m & PFEM2_FP32_ASSEMBLY) != 0;
+    c.prmixed = (m & PFEM2_FP32_PRESSURE_RHS) != 0;
+    c.kmixed = (m & PFEM2_FP32_KRYLOV) != 0;
+  }
+  if (cfg->precision != PFEM2_PREC_FP64 && cfg->precision != PFEM2_PREC_MIXED) {
+    set_error("precision must be PFEM2_PREC_FP64 or PFEM2_PREC_MIXED");
+    return PFEM2_INVALID_ARG;
+  }
+  if (cfg->fp32_stages < 0 || cfg->fp32_stages > 15) {
+    set_error("fp32_stages: a mask of PFEM2_FP32_* bits");
+    return PFEM2_INVALID_ARG;
+  }
   c.device = cfg->device;
   PFEM2_CUDA(cudaSetDevice(c.device));
   cudaDeviceProp prop;
@@ -621,6 +665,7 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   c.num_sms = prop.multiProcessorCount;
   if (const char* v = getenv("PFEM2_ADVECT_SPLIT_MIN")) c.adv_split_min = atoll(v);
   if (const char* v = getenv("PFEM2_MG_WIDE_MIN")) c.mg_wide_min = atoll(v);
+  if (const char* v = getenv("PFEM2_SPIN_LIMIT")) c.spin_limit = (unsigned)std::min(atoll(v), (long long)c.spin_limit);
   PFEM2_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   for (int k = 0; k < 8; ++k) PFEM2_CUDA(cudaEventCreate(&c.ev[k]));
   *out = x;
@@ -632,14 +677,6 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   Ctx& c = x->c;
   cudaSetDevice(c.device);
   cudaStreamSynchronize(c.stream);
-  if (const char* path = getenv("PFEM2_SOLVER_PROFILE")) {
-    // solver phase profile (kind action:phases:mean us:max us:wait us), appended per context
-    const std::string pr = krylov_profile(c);
-    if (FILE* f = fopen(path, "a")) {
-      fprintf(f, "prec=%s\n%s", c.mixed ? "mixed" : "fp64", pr.c_str());
-      fclose(f);
-    }
-  }
   for (int k = 0; k < 2; ++k)
     if (x->graph[k]) cudaGraphExecDestroy(x->graph[k]);
   krylov_free(c);
@@ -651,7 +688,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
                   c.far_keys, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  if (c.mixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);
+  if (c.pmixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);
   for (int k = 0; k < kNumSys; ++k) {
     cudaFree(c.A64[k]); cudaFree(c.A32[k]); cudaFree(c.dinv64[k]); cudaFree(c.dinv32[k]);
   }
@@ -706,6 +743,7 @@ pfem2_status pfem2_setup(pfem2_ctx* x) {
 
 pfem2_status pfem2_seed(pfem2_ctx* x, int32_t instance, const uint32_t q[3], uint64_t seed, double jitter) {
   SETUP_CHECK(x);
+  LIVE_CHECK(x);
   Ctx& c = x->c;
   if (!q || q[0] < 1 || q[1] < 1 || (c.dim == 3 && q[2] < 1)) { set_error("bad q"); return PFEM2_INVALID_ARG; }
   int nb = (q[0] + 1) * (q[1] + 1) * (c.dim == 3 ? q[2] + 1 : 1);
@@ -779,6 +817,7 @@ pfem2_status pfem2_project(pfem2_ctx* x) {
 
 pfem2_status pfem2_fem_step(pfem2_ctx* x) {
   SETUP_CHECK(x);
+  LIVE_CHECK(x);
   if (x->c.cfg.particles_only) {
     set_error("pfem2_fem_step: the context was created with particles_only");
     return PFEM2_BAD_STATE;
@@ -853,18 +892,22 @@ static pfem2_status enqueue_loads(Ctx& c, int i, int patch) {
 }
 
 // the 5 published load values of instance i from its 7 raw values
-// (2D: drag and lift coefficients split into viscous and pressure parts,
-// 3D: the force; the last entry is the probe pressure difference)
+// (2D: drag and lift coefficients split into viscous and pressure parts and
+// the probe pressure difference p(a) - p(b), TurekBenchmark/pfem2particle.cpp:
+// 945-956; 3D: the pressure force and the pressure at the probe, the mean
+// over the listed probe vertices, tubePoiseuille3D/pfem2particle.cpp:720-731)
 static void finish_loads(const Ctx& c, int i, const double* raw, double* out) {
   const pfem2_case& cs = c.inst[i].cs;
   if (c.dim == 2) {
     const double s = cs.rho * cs.load_umean * cs.load_umean * cs.load_diam;
     for (int k = 0; k < 4; ++k) out[k] = s != 0 ? 2.0 * raw[k] / s : 0.0;
+    out[4] = (cs.probe_a >= 0 ? raw[5] : 0.0) - (cs.probe_b >= 0 ? raw[6] : 0.0);
   } else {
     for (int k = 0; k < 3; ++k) out[k] = raw[k];
     out[3] = 0.0;
+    const int np = (cs.probe_a >= 0) + (cs.probe_b >= 0);
+    out[4] = np ? ((cs.probe_a >= 0 ? raw[5] : 0.0) + (cs.probe_b >= 0 ? raw[6] : 0.0)) / np : 0.0;
   }
-  out[4] = (cs.probe_a >= 0 ? raw[5] : 0.0) - (cs.probe_b >= 0 ? raw[6] : 0.0);
 }
 
 pfem2_status pfem2_step_and_read(pfem2_ctx* x, double* loads_out, const int32_t* fields, int32_t n_fields,
@@ -938,6 +981,11 @@ pfem2_status pfem2_set_field(pfem2_ctx* x, int32_t instance, int32_t field, cons
     set_error("bad argument");
     return PFEM2_INVALID_ARG;
   }
+  for (int k = 0; k < c.inst[instance].nv; ++k)
+    if (!std::isfinite(host[k])) {
+      set_error("set_field: a value is not finite");
+      return PFEM2_INVALID_ARG;
+    }
   PFEM2_CUDA(cudaMemcpyAsync(c.F[field] + c.inst[instance].v_off, host, sizeof(double) * c.inst[instance].nv,
                              cudaMemcpyHostToDevice, c.stream));
   PFEM2_TRY(launch_sync_real_fields(c));
@@ -964,8 +1012,9 @@ pfem2_status pfem2_get_particles(pfem2_ctx* x, int32_t instance, int32_t* cell, 
 pfem2_status pfem2_set_particles(pfem2_ctx* x, const int32_t* counts, const int32_t* cell, const double* xi,
                                  const double* u) {
   SETUP_CHECK(x);
+  LIVE_CHECK(x);
   Ctx& c = x->c;
-  if (!counts) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  if (!counts || !cell || !xi || !u) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
   size_t total = 0;
   for (size_t i = 0; i < c.inst.size(); ++i) total += counts[i];
   for (auto& in : c.inst)

@@ -257,51 +257,11 @@ struct GridBarrier {
   unsigned* count;
   unsigned* gen;
   int* err;
+  unsigned spin_limit;  // polls before a wait gives up and sets *err = 1
 };
 
+// polls before a wait gives up (the default; contexts may lower it)
 #define PFEM2_BARRIER_SPIN_LIMIT (1u << 26)
-
-// `gl` is thread 0's copy of the generation counter (0 after the reset that
-// precedes every launch), so arriving costs one atomic and no extra read.
-// With `stop` non-null the last block to arrive also reads *stop_src and
-// publishes (*stop_src <= 0) in bit 31 of the release word, so every block
-// learns a global termination condition without another memory round trip.
-__device__ __forceinline__ bool grid_sync(const GridBarrier& gb, unsigned& gl, const int* stop_src = nullptr,
-                                          bool* stop = nullptr) {
-  __syncthreads();
-  __shared__ int s_ok, s_stop;
-  if (threadIdx.x == 0) {
-    volatile unsigned* vgen = gb.gen;
-    const unsigned g = gl;
-    __threadfence();
-    unsigned arrived = atomicAdd(gb.count, 1u);
-    int ok = 1;
-    unsigned word = g + 1;
-    if (arrived == gridDim.x - 1) {
-      *gb.count = 0;
-      __threadfence();
-      if (stop_src && *(volatile const int*)stop_src <= 0) word |= 0x80000000u;
-      atomicExch(gb.gen, word);
-    } else {
-      unsigned spins = 0;
-      while ((word = *vgen) == g) {
-        if (++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)gb.err) {
-          atomicExch(gb.err, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(20);
-      }
-    }
-    __threadfence();
-    gl = word;
-    s_stop = (word >> 31) & 1u;
-    s_ok = ok && (*(volatile int*)gb.err == 0);
-  }
-  __syncthreads();
-  if (stop) *stop = s_stop != 0;
-  return s_ok != 0;
-}
 
 // Release/acquire grid barrier on an arrival counter that is never reset
 // within a launch: barrier k is passed once the counter reaches
@@ -309,7 +269,7 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& gb, unsigned& gl, c
 // with gpu-scope acquire loads (no separate fences); the CTA barriers on
 // both sides extend the ordering to the other threads of the block. `k`
 // is the caller's barrier count (0 after the reset that precedes every
-// launch). The poll gives up after PFEM2_BARRIER_SPIN_LIMIT tries or when
+// launch). The poll gives up after gb.spin_limit tries or when
 // another block has flagged an error, sets gb.err = 1 and returns false.
 __device__ __forceinline__ bool grid_sync_ra(const GridBarrier& gb, unsigned& k) {
   __syncthreads();
@@ -324,7 +284,7 @@ __device__ __forceinline__ bool grid_sync_ra(const GridBarrier& gb, unsigned& k)
     while (true) {
       asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(gb.count) : "memory");
       if ((int)(v - target) >= 0) break;
-      if (++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)gb.err) {
+      if (++spins > gb.spin_limit || *(volatile int*)gb.err) {
         atomicExch(gb.err, 1);
         ok = 0;
         break;

@@ -49,7 +49,10 @@ struct Tile {
 struct Ctx {
   pfem2_config cfg{};
   int dim = 2;
-  bool mixed = false;
+  // FP32 stages (pfem2_config.fp32_stages of a mixed context): particle
+  // state and kernels, prediction/correction right-hand sides, pressure
+  // right-hand side, inner Krylov iterations
+  bool pmixed = false, amixed = false, prmixed = false, kmixed = false;
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -167,11 +170,19 @@ struct Ctx {
   int* d_sysinfo = nullptr;
   unsigned* barrier = nullptr;   // count, gen
   int* d_err = nullptr;
+  // polls of a bounded device-side wait before it gives up (PFEM2_TIMEOUT);
+  // the environment variable PFEM2_SPIN_LIMIT lowers it at creation (tests)
+  unsigned spin_limit = 1u << 26;
+  // a wait timed out: the device state is not trusted, stepping calls
+  // return PFEM2_BAD_STATE until the context is destroyed
+  bool failed = false;
   int coop_blocks = 0;
   int solve_threads = 256;
   int solve_blocks_per_sm = 1;  // persistent Krylov grid: blocks per SM
   long long mg_wide_min = 262144;  // rows from which one pressure system runs two blocks per SM
   bool two_level = true;        // pressure: multigrid preconditioner (else Jacobi)
+  bool vel_bicg = false;        // velocity systems solved by BiCGStab (else CG)
+  bool p_bicg = false;          // pressure solved by BiCGStab with Jacobi (else CG with multigrid)
   double refine_eta = 1e-3;     // mixed: inner residual reduction per FP64 refinement
 
   // graph
@@ -248,7 +259,6 @@ void krylov_free(Ctx& c);
 // which: 0 prediction (dim systems per instance), 1 pressure, 2 correction
 pfem2_status krylov_solve(Ctx& c, int which);
 pfem2_status krylov_read_stats(Ctx& c);
-std::string krylov_profile(Ctx& c);
 void krylov_sizes(Ctx& c, long long* out12);
 
 }  // namespace pfem2

@@ -467,8 +467,8 @@ static void rhs_pred_impl(Ctx& c) {
   c.launches++;
 }
 pfem2_status launch_rhs_prediction(Ctx& c) {
-  if (c.dim == 2) { if (c.mixed) rhs_pred_impl<2, float>(c); else rhs_pred_impl<2, double>(c); }
-  else { if (c.mixed) rhs_pred_impl<3, float>(c); else rhs_pred_impl<3, double>(c); }
+  if (c.dim == 2) { if (c.amixed) rhs_pred_impl<2, float>(c); else rhs_pred_impl<2, double>(c); }
+  else { if (c.amixed) rhs_pred_impl<3, float>(c); else rhs_pred_impl<3, double>(c); }
   return PFEM2_OK;
 }
 
@@ -480,8 +480,8 @@ static void rhs_p_impl(Ctx& c) {
   c.launches++;
 }
 pfem2_status launch_rhs_pressure(Ctx& c) {
-  if (c.dim == 2) { if (c.mixed) rhs_p_impl<2, float>(c); else rhs_p_impl<2, double>(c); }
-  else { if (c.mixed) rhs_p_impl<3, float>(c); else rhs_p_impl<3, double>(c); }
+  if (c.dim == 2) { if (c.prmixed) rhs_p_impl<2, float>(c); else rhs_p_impl<2, double>(c); }
+  else { if (c.prmixed) rhs_p_impl<3, float>(c); else rhs_p_impl<3, double>(c); }
   return PFEM2_OK;
 }
 
@@ -493,8 +493,8 @@ static void rhs_c_impl(Ctx& c) {
   c.launches++;
 }
 pfem2_status launch_rhs_correction(Ctx& c) {
-  if (c.dim == 2) { if (c.mixed) rhs_c_impl<2, float>(c); else rhs_c_impl<2, double>(c); }
-  else { if (c.mixed) rhs_c_impl<3, float>(c); else rhs_c_impl<3, double>(c); }
+  if (c.dim == 2) { if (c.amixed) rhs_c_impl<2, float>(c); else rhs_c_impl<2, double>(c); }
+  else { if (c.amixed) rhs_c_impl<3, float>(c); else rhs_c_impl<3, double>(c); }
   return PFEM2_OK;
 }
 
@@ -532,8 +532,8 @@ static void finish_impl(Ctx& c) {
   c.launches++;
 }
 pfem2_status launch_finish_fem(Ctx& c) {
-  if (c.dim == 2) { if (c.mixed) finish_impl<2, float>(c); else finish_impl<2, double>(c); }
-  else { if (c.mixed) finish_impl<3, float>(c); else finish_impl<3, double>(c); }
+  if (c.dim == 2) { if (c.pmixed) finish_impl<2, float>(c); else finish_impl<2, double>(c); }
+  else { if (c.pmixed) finish_impl<3, float>(c); else finish_impl<3, double>(c); }
   return PFEM2_OK;
 }
 
@@ -567,8 +567,8 @@ static void restore_impl(Ctx& c) {
   c.launches++;
 }
 pfem2_status launch_restore_frozen(Ctx& c) {
-  if (c.dim == 2) { if (c.mixed) restore_impl<2, float>(c); else restore_impl<2, double>(c); }
-  else { if (c.mixed) restore_impl<3, float>(c); else restore_impl<3, double>(c); }
+  if (c.dim == 2) { if (c.pmixed) restore_impl<2, float>(c); else restore_impl<2, double>(c); }
+  else { if (c.pmixed) restore_impl<3, float>(c); else restore_impl<3, double>(c); }
   return PFEM2_OK;
 }
 

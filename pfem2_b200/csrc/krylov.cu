@@ -59,7 +59,15 @@ constexpr int kWarps = kSolveThreads / 32;
 constexpr int kMaxLocalSys = 16;
 
 enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_UZ = 5, S_B2 = 6 };
-enum { ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_UZ = 6, ACT_B2 = 7 };
+enum {
+  ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_UZ = 6, ACT_B2 = 7,
+  ACT_P1 = 8,   // BiCGStab: finish the previous step, y = K^-1 p, v = A y
+  ACT_P2 = 9,   // BiCGStab: e += alpha y, s = r - alpha v, t = A K^-1 s
+  ACT_BF = 10   // BiCGStab: e += omega K^-1 s before a reliable update
+};
+// partial sums per tile: CG uses 2, BiCGStab 5 (and the FP64 residual
+// phase |r|^2 and |b|^2)
+constexpr int kMaxSums = 5;
 
 constexpr int kMaxBlockTiles = 64;
 
@@ -129,7 +137,14 @@ template <typename R> struct SolveArgs {
   const unsigned char* isd[3];
   const double* g[3];    // Dirichlet values preset in x (nullptr -> 0)
   const double* tol_i;   // per instance
+  const double* rtol_i;  // per instance: stop at max(tol, rtol |b|)
   const int* maxit_i;    // per instance
+  int nsum;              // partial sums per tile (2, or kMaxSums for BiCGStab)
+  int bicg;              // Jacobi path: BiCGStab instead of CG
+  // BiCGStab vectors (nv entries per component slot): zr = K^-1 r, y and
+  // w = K^-1 v double buffered (parity L.par; y in p), the shadow residual
+  // rh, s, t and kt = K^-1 t; v in q, r in r's first buffer
+  R *bz, *bw, *rh, *bs, *bt, *bkt;
   // workspace per component slot, nv entries each; r and p: 2 buffers
   R *e, *r, *z, *p, *q;
   double* r64;
@@ -138,18 +153,12 @@ template <typename R> struct SolveArgs {
   int* active;
   int* out_it;           // [nsys] iterations
   double* out_res;       // [nsys] final residual norm
+  double* out_tol;       // [nsys] tolerance the system was solved to
   int* out_outer;        // [nsys] FP64 residual evaluations
   double eta;
   int iter_cap;
   GridBarrier gb;
-  unsigned long long* prof;  // optional [grid][8 actions][3]: phases, work ns, barrier-wait ns (PFEM2_SOLVER_PROFILE)
 };
-
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 
 __device__ __forceinline__ float fma_r(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fma_r(double a, double b, double c) { return fma(a, b, c); }
@@ -224,9 +233,10 @@ struct LocalSys {
   int sys, state, it, outer, par, rpar, first, owner, maxit, act, chk;
   int t0, t1;                       // partial slots of the system
   int D3, off3, n2, off2, b2off;    // multigrid: coarse sizes and offsets
-  double tol, intol, res, rz_prev, alpha, beta;
+  double tol, rtol, intol, res, rz_prev, alpha, beta;
+  double omega;                     // BiCGStab (rz_prev holds rho = (rh, r))
   double rr_b;                      // split restriction: r'.r' of the B phase, for the UZ decision
-  double sum[2];
+  double sum[kMaxSums];
 };
 
 // copies src[lo, hi) into shared memory at `cur` (16-byte aligned pieces)
@@ -252,6 +262,9 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
   // entries of a SELL row (and of a long restriction row) whose loads are
   // issued together: more with one block per SM, which has the registers
   constexpr int CH = MINB == 1 ? 16 : 8;
+  // partial sums per work item: the multigrid path (CG) needs 2
+  constexpr int NSMAX = MG ? 2 : kMaxSums;
+  const int NS = MG ? 2 : a.nsum;
   __shared__ LocalSys ls[kMaxLocalSys];
   __shared__ Tile stile[kMaxBlockTiles];
   __shared__ int s_nls;
@@ -281,9 +294,10 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
       L.t1 = a.sys_slot0[s + 1];
       L.maxit = a.maxit_i[inst];
       L.tol = a.tol_i[inst];
+      L.rtol = a.rtol_i[inst];
       L.intol = 0.5 * L.tol;
-      L.res = L.rz_prev = L.alpha = L.beta = 0.0;
-      L.sum[0] = L.sum[1] = 0.0;
+      L.res = L.rz_prev = L.alpha = L.beta = L.omega = 0.0;
+      for (int q = 0; q < kMaxSums; ++q) L.sum[q] = 0.0;
       L.act = ACT_NONE;
       L.D3 = L.off3 = L.n2 = L.off2 = L.b2off = 0;
       if (MG) {
@@ -306,7 +320,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
   // the first item of local tile t. Every item's partial sums go to spart,
   // then each tile sums its items in order (deterministic).
   double* spart = reinterpret_cast<double*>(dyn_smem);
-  int* item0 = reinterpret_cast<int*>(dyn_smem + al16_dev((size_t)a.items_max * 2 * sizeof(double)));
+  int* item0 = reinterpret_cast<int*>(dyn_smem + al16_dev((size_t)a.items_max * NS * sizeof(double)));
   if (threadIdx.x == 0) {
     int n = 0;
     for (int t = 0; t < ntl; ++t) {
@@ -329,7 +343,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     return lo;
   };
   unsigned char* dyn_rest =
-      dyn_smem + al16_dev((size_t)a.items_max * 2 * sizeof(double)) + al16_dev((size_t)(a.ntl_max + 1) * sizeof(int));
+      dyn_smem + al16_dev((size_t)a.items_max * NS * sizeof(double)) + al16_dev((size_t)(a.ntl_max + 1) * sizeof(int));
 
   // ---- shared memory: multigrid vectors, then the staged static data
   R* sx1 = reinterpret_cast<R*>(dyn_rest);
@@ -442,19 +456,13 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
   __shared__ int s_stop;
   if (!grid_sync_ra(a.gb, bar_gen)) return;
 
-  // optional profile of every block: per action of its first local system,
-  // the phases run, the time from the end of the last barrier to the
-  // arrival at the next one (work) and the wait there
-  const bool prof = a.prof != nullptr && threadIdx.x == 0;
-  unsigned long long pacc[8][3] = {}, t_phase = prof ? gtimer() : 0, t_arrive = 0;
-  int plabel = ACT_NONE;
   for (int iter = 0;; ++iter) {
     if (iter >= a.iter_cap) {
       if (threadIdx.x == 0) atomicCAS(a.gb.err, 0, 2);
       break;
     }
     const bool phaseA = (iter & 1) == 0;
-    const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * 2;
+    const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * NS;
     // ---- wait for the previous phase of the block's running systems: every
     // tile adds 1 to its system's counter with a release add once its phase
     // is written, so iter x (tiles of the system) means that every tile of
@@ -477,7 +485,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
             fence_acq_rel_gpu();
             break;
           }
-          if (__any_sync(PFEM2_FULL_MASK, ++spins > PFEM2_BARRIER_SPIN_LIMIT || *(volatile int*)a.gb.err != 0)) {
+          if (__any_sync(PFEM2_FULL_MASK, ++spins > a.gb.spin_limit || *(volatile int*)a.gb.err != 0)) {
             if (lane == 0) atomicCAS(a.gb.err, 0, 1);
             stop = true;
             break;
@@ -511,23 +519,100 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           ls[k].sum[0] = s0;
           ls[k].sum[1] = s1;
         }
+        // BiCGStab's further sums, in the same fixed order
+#pragma unroll
+        for (int q = 2; q < NSMAX; ++q) {
+          if (q >= NS) break;
+          double sq = 0.0;
+          for (int tb = t0; tb < t1; tb += 256) {
+            double vq[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int t = tb + u * 32 + lane;
+              vq[u] = t < t1 ? __ldcg(prev + (size_t)q * a.ntiles + t) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) sq += vq[u];
+          }
+          sq = warp_sum(sq);
+          if (lane == 0) ls[k].sum[q] = sq;
+        }
       }
     }
     __syncthreads();
-    if (prof && iter > 0) {
-      const unsigned long long tn = gtimer();
-      pacc[plabel][0] += 1;
-      pacc[plabel][1] += t_arrive - t_phase;
-      pacc[plabel][2] += tn - t_arrive;
-      t_phase = tn;
-    }
     if (s_stop) break;
     // ---- decisions (thread 0; identical in every block owning the system)
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
         LocalSys& L = ls[k];
         int act = ACT_NONE;
-        if (!MG) {
+        // the first FP64 residual phase also summed |b|^2: the relative tolerance
+        if (L.state == S_OUT_B && L.outer == 0) L.tol = fmax(L.tol, L.rtol * sqrt(L.sum[1]));
+        if (!MG && a.bicg) {
+          // BiCGStab with the Jacobi preconditioner K (right-preconditioned,
+          // van der Vorst 1992) over the phases OUT_A (FP64 residual),
+          // OUT_B (restart: r = rh = r64, zr = K^-1 r), then P1 / P2 per
+          // iteration; BF completes the iterate before a reliable update
+          switch (L.state) {
+            case S_OUT_A:
+              act = ACT_OUT_A;
+              L.state = S_OUT_B;
+              break;
+            case S_OUT_B:
+              L.res = sqrt(L.sum[0]);
+              L.outer += 1;
+              if (L.res <= L.tol || L.it >= L.maxit || L.outer > L.maxit || !(L.res == L.res)) {
+                act = ACT_OUT_DONE;
+                L.state = S_DONE;
+              } else {
+                L.intol = fmax(a.eta * L.res, 0.5 * L.tol);
+                L.first = 1;
+                L.rz_prev = L.res * L.res;  // rho = (rh, r) with rh = r
+                act = ACT_OUT_B;
+                L.state = S_A;
+              }
+              break;
+            case S_A:
+              if (L.first) {
+                L.beta = 0.0;
+                act = ACT_P1;
+                L.state = S_B;
+              } else {
+                // sums of P2: (t,s), (t,t), (rh,s), (rh,t), (s,s)
+                const double ts = L.sum[0], tt = L.sum[1], rs = L.sum[2], rt = L.sum[3], ss = L.sum[4];
+                const double om = tt > 0.0 ? ts / tt : 0.0;
+                const double rr = sqrt(fmax(ss - 2.0 * om * ts + om * om * tt, 0.0));
+                const double rho = rs - om * rt;
+                L.omega = om;
+                L.it += 1;
+                if (!(om != 0.0) || !(rho != 0.0) || rr <= L.intol || L.it >= L.maxit || !(rr == rr)) {
+                  act = ACT_BF;  // x += omega K^-1 s, then a reliable update
+                  L.state = S_OUT_A;
+                } else {
+                  L.beta = (rho / L.rz_prev) * (L.alpha / om);
+                  L.rz_prev = rho;
+                  act = ACT_P1;
+                  L.state = S_B;
+                }
+              }
+              break;
+            case S_B: {
+              const double rv = L.sum[0];  // (rh, v)
+              L.first = 0;
+              if (!(rv != 0.0) || !(rv == rv)) {
+                act = ACT_OUT_A;  // breakdown: restart from the FP64 residual
+                L.state = S_OUT_B;
+              } else {
+                L.alpha = L.rz_prev / rv;
+                act = ACT_P2;
+                L.state = S_A;
+              }
+              break;
+            }
+            default:
+              break;
+          }
+        } else if (!MG) {
           if (phaseA) {
             if (L.state == S_OUT_A) {
               act = ACT_OUT_A;
@@ -623,7 +708,6 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         }
         L.act = act;
       }
-      plabel = nls > 0 ? ls[0].act : ACT_NONE;
     }
     __syncthreads();
     // ---- coarse-level work of the block (multigrid; pressure = component 0)
@@ -865,7 +949,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
       const LocalSys& L = ls[T.lk];
       const int act = L.act;
       if (act == ACT_NONE) continue;
-      double v0 = 0.0, v1 = 0.0;
+      double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0, v4 = 0.0;
       const R* dinv = a.dinv[k];
       R* e = a.e + k * nv;
       R* r = a.r + (2 * k + L.rpar) * nv;
@@ -880,9 +964,11 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           const double acc = sell_dot<double, CH>(
               0.0, SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
               [&](int col) { return __ldcg(xk + col) + (double)ldm(e, me, col, own0, nown); });
-          const double rr = a.b[k][row] - acc;
+          const double bb = a.b[k][row];
+          const double rr = bb - acc;
           r64[row] = rr;
           v0 += rr * rr;
+          v1 += bb * bb;
         }
       } else if (act == ACT_OUT_B || act == ACT_OUT_DONE) {
         {
@@ -894,7 +980,10 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
             const R rr = R(r64[row]);
             r[row] = rr;
             if (me) mr[L.rpar][row - own0] = rr;
-            if (!MG) {
+            if (!MG && a.bicg) {
+              a.rh[k * nv + row] = rr;
+              a.bz[(2 * k + L.par) * nv + row] = rr * dinv[row];
+            } else if (!MG) {
               const R zz = rr * dinv[row];
               z[row] = zz;
               v0 += (double)rr * (double)zz;
@@ -902,6 +991,63 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
             }
           }
         }
+      } else if (!MG && act == ACT_P1) {
+        // y' = zr' + beta (y - omega w), zr' = zr - alpha w - omega kt the
+        // preconditioned new residual (first step after a restart: y' = zr),
+        // v = A y' with y' formed on the fly at the columns, w' = K^-1 v
+        const int row = sl * 32 + lane;
+        const bool first = L.first != 0;
+        const R al = R(L.alpha), om = R(L.omega), be = R(L.beta);
+        const R* zo = a.bz + (2 * k + L.par) * nv;
+        const R* wo = a.bw + (2 * k + L.par) * nv;
+        const R* yo = a.p + (2 * k + L.par) * nv;
+        const R* kt = a.bkt + k * nv;
+        const auto ynew = [&](int j) -> R {
+          if (first) return zo[j];
+          const R zr = fma_r(-om, kt[j], fma_r(-al, wo[j], zo[j]));
+          return fma_r(be, fma_r(-om, wo[j], yo[j]), zr);
+        };
+        R zr_row = zo[row];
+        if (!first) {
+          const R zs = fma_r(-al, wo[row], zo[row]);
+          e[row] = fma_r(om, zs, e[row]);
+          r[row] = fma_r(-om, a.bt[k * nv + row], a.bs[k * nv + row]);
+          zr_row = fma_r(-om, kt[row], zs);
+        }
+        const R yrow = ynew(row);
+        const R* A = a.Ain[k];
+        const R acc = sell_dot<R, CH>(R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; }, ynew);
+        a.bz[(2 * k + (L.par ^ 1)) * nv + row] = zr_row;
+        a.p[(2 * k + (L.par ^ 1)) * nv + row] = yrow;
+        a.bw[(2 * k + (L.par ^ 1)) * nv + row] = acc * dinv[row];
+        q[row] = acc;
+        v0 += (double)a.rh[k * nv + row] * (double)acc;
+      } else if (!MG && act == ACT_P2) {
+        // e += alpha y, s = r - alpha v, t = A K^-1 s (K^-1 s = zr - alpha w
+        // formed on the fly), kt = K^-1 t; sums (t,s) (t,t) (rh,s) (rh,t) (s,s)
+        const int row = sl * 32 + lane;
+        const R al = R(L.alpha);
+        const R* zc = a.bz + (2 * k + L.par) * nv;
+        const R* wc = a.bw + (2 * k + L.par) * nv;
+        e[row] = fma_r(al, a.p[(2 * k + L.par) * nv + row], e[row]);
+        const R sv = fma_r(-al, q[row], r[row]);
+        const R* A = a.Ain[k];
+        const R tv = sell_dot<R, CH>(R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
+                                     [&](int j) { return fma_r(-al, wc[j], zc[j]); });
+        a.bs[k * nv + row] = sv;
+        a.bt[k * nv + row] = tv;
+        a.bkt[k * nv + row] = tv * dinv[row];
+        const double rh = (double)a.rh[k * nv + row];
+        v0 += (double)tv * (double)sv;
+        v1 += (double)tv * (double)tv;
+        v2 += rh * (double)sv;
+        v3 += rh * (double)tv;
+        v4 += (double)sv * (double)sv;
+      } else if (!MG && act == ACT_BF) {
+        // the last step's x += omega K^-1 s (K^-1 s = zr - alpha w)
+        const int row = sl * 32 + lane;
+        const R zs = fma_r(-R(L.alpha), a.bw[(2 * k + L.par) * nv + row], a.bz[(2 * k + L.par) * nv + row]);
+        e[row] = fma_r(R(L.omega), zs, e[row]);
       } else if (act == ACT_A) {
         const R beta = R(L.beta);
         R* pn = a.p + (2 * k + L.par) * nv;
@@ -966,8 +1112,18 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
       v0 = warp_sum(v0);
       v1 = warp_sum(v1);
       if (lane == 0) {
-        spart[2 * it] = v0;
-        spart[2 * it + 1] = v1;
+        spart[NS * it] = v0;
+        spart[NS * it + 1] = v1;
+      }
+      if (NSMAX > 2 && NS > 2) {
+        v2 = warp_sum(v2);
+        v3 = warp_sum(v3);
+        v4 = warp_sum(v4);
+        if (lane == 0) {
+          spart[NS * it + 2] = v2;
+          spart[NS * it + 3] = v3;
+          spart[NS * it + 4] = v4;
+        }
       }
     }
     __syncthreads();
@@ -978,14 +1134,18 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     for (int tl = threadIdx.x; tl < ntl; tl += kSolveThreads) {
       const Tile T = tile_at(t_lo + tl);
       if (ls[T.lk].act != ACT_NONE) {
-        double s0 = 0.0, s1 = 0.0;
+        double sm[NSMAX];
+#pragma unroll
+        for (int q = 0; q < NSMAX; ++q) sm[q] = 0.0;
         for (int it = item0[tl]; it < item0[tl + 1]; ++it) {
-          s0 += spart[2 * it];
-          s1 += spart[2 * it + 1];
+#pragma unroll
+          for (int q = 0; q < NSMAX; ++q)
+            if (q < NS) sm[q] += spart[NS * it + q];
         }
-        double* dst = a.part + (size_t)(iter & 1) * a.ntiles * 2 + T.slot;
-        dst[0] = s0;
-        dst[a.ntiles] = s1;
+        double* dst = a.part + (size_t)(iter & 1) * a.ntiles * NS + T.slot;
+#pragma unroll
+        for (int q = 0; q < NSMAX; ++q)
+          if (q < NS) dst[(size_t)q * a.ntiles] = sm[q];
       }
       red_release_add_u32(a.scount + (size_t)T.sys * 32, 1u);
     }
@@ -997,20 +1157,18 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           L.par ^= 1;
           if (MG) L.rpar ^= 1;
         }
+        if (L.act == ACT_P1) L.par ^= 1;
         if (L.act == ACT_OUT_DONE && L.owner) {
           a.out_it[L.sys] = L.it;
           a.out_res[L.sys] = L.res;
+          a.out_tol[L.sys] = L.tol;
           a.out_outer[L.sys] = L.outer;
           atomicSub(a.active, 1);
         }
         L.act = ACT_NONE;
       }
     }
-    if (prof) t_arrive = gtimer();
   }
-  if (prof)
-    for (int k = 0; k < 8; ++k)
-      for (int j = 0; j < 3; ++j) atomicAdd(a.prof + ((size_t)blockIdx.x * 8 + k) * 3 + j, pacc[k][j]);
 }
 
 // ------------------------------------------------------------------ host
@@ -1031,13 +1189,15 @@ struct KrylovWs {
   size_t l0_meta[2] = {0, 0}, l0_col[2] = {0, 0};  // max bytes per block of the level-0 categories
   int ntl_max[2] = {0, 0}, items_max[2] = {0, 0};  // per block: tiles, (tile, slice) items
   size_t items_bytes[2] = {0, 0};                  // shared memory of the item partials and offsets
+  int nsum[2] = {2, 2};                            // partial sums per tile of each phase
+  bool bicg[2] = {false, false};                   // phase solved by BiCGStab
+  void *bz = nullptr, *bw = nullptr, *rh = nullptr, *bs = nullptr, *bt = nullptr, *bkt = nullptr;
   // multigrid of the pressure phase (phase 0)
   bool mg = false;
   int mg_minb = 1;  // resident blocks per SM of the pressure solve: 2 for batches (many tiles per block)
   int nls0 = 1;
   int dmax = 1, s1max = 0, s2max = 0, s3max = 0, b2max = 0, o2max = 0, emax = 0;
   int n1 = 0, n2 = 0, n3 = 0;
-  std::string mg_info;                   // hierarchy summary for the profile
   long long mg_sizes[12] = {};           // see pfem2_solver_sizes
   int *toff[4] = {}, *lk[3] = {};
   int *r01_ptr = nullptr, *r01_col = nullptr, *r02_ptr = nullptr, *r02_col = nullptr;
@@ -1062,8 +1222,8 @@ struct KrylovWs {
   int* active = nullptr;
   int* out_it[3];
   double* out_res[3];
+  double* out_tol[3];
   int* out_outer[3];
-  unsigned long long* prof[3] = {};     // per solve kind: [grid][8 actions][3]
   std::vector<void*> allocs;            // every device allocation of the workspace
 };
 
@@ -1185,7 +1345,7 @@ pfem2_status krylov_setup(Ctx& c) {
     // the multigrid grid is sized before its shared memory is known
     // (mg_minb blocks per SM); krylov_setup_precond checks residency
     // afterwards. The Jacobi kernel runs two blocks per SM.
-    const int occ = ph == 0 ? w->mg_minb : std::min(2, occupancy_any<false>(c.mixed, 2, 0));
+    const int occ = ph == 0 ? w->mg_minb : std::min(2, occupancy_any<false>(c.kmixed, 2, 0));
     if (occ < 1) {
       set_error("krylov: the solver kernel cannot be resident");
       return PFEM2_CUDA_ERROR;
@@ -1251,7 +1411,10 @@ pfem2_status krylov_setup(Ctx& c) {
     w->l0_col[ph] = col;
     w->ntl_max[ph] = ntl_max;
     w->items_max[ph] = items_max;
-    w->items_bytes[ph] = al16(sizeof(double) * 2 * (size_t)items_max) + al16(sizeof(int) * (size_t)(ntl_max + 1));
+    w->bicg[ph] = ph == 0 ? c.p_bicg : c.vel_bicg;
+    w->nsum[ph] = w->bicg[ph] ? kMaxSums : 2;
+    w->items_bytes[ph] =
+        al16(sizeof(double) * w->nsum[ph] * (size_t)items_max) + al16(sizeof(int) * (size_t)(ntl_max + 1));
     if (ph == 0) {
       w->h_tiles0 = tiles;
       w->h_sys_t0_0 = slot0;
@@ -1270,7 +1433,7 @@ pfem2_status krylov_setup(Ctx& c) {
         w->stage[1] |= ST_L0COL;
         w->smem[1] += col;
       }
-      const int occ2 = occupancy_any<false>(c.mixed, 2, w->smem[1]);
+      const int occ2 = occupancy_any<false>(c.kmixed, 2, w->smem[1]);
       if (occ2 * c.num_sms < G) {
         w->stage[1] = 0;
         w->smem[1] = w->items_bytes[1];
@@ -1290,7 +1453,7 @@ pfem2_status krylov_setup(Ctx& c) {
     maxtiles = std::max(maxtiles, T);
     maxsys = std::max(maxsys, nsys);
   }
-  if (c.mixed) {
+  if (c.kmixed) {
     float *e, *r, *z, *q, *p;
     PFEM2_TRY(ws_alloc(w, &e, nv * dim));
     PFEM2_TRY(ws_alloc(w, &r, 2 * nv * dim));
@@ -1308,14 +1471,21 @@ pfem2_status krylov_setup(Ctx& c) {
     w->e = e; w->r = r; w->z = z; w->q = q; w->p = p;
   }
   PFEM2_TRY(ws_alloc(w, &w->r64, nv * dim));
-  PFEM2_TRY(ws_alloc(w, &w->part, 4 * (size_t)maxtiles));
+  PFEM2_TRY(ws_alloc(w, &w->part, 2 * (size_t)kMaxSums * maxtiles));
+  if (c.vel_bicg || c.p_bicg) {
+    // BiCGStab vectors: zr and w double buffered, rh, s, t, kt
+    const size_t rs = c.kmixed ? sizeof(float) : sizeof(double);
+    unsigned char* b[6];
+    const size_t n[6] = {2 * nv * dim, 2 * nv * dim, nv * dim, nv * dim, nv * dim, nv * dim};
+    for (int k = 0; k < 6; ++k) PFEM2_TRY(ws_alloc(w, &b[k], n[k] * rs));
+    w->bz = b[0]; w->bw = b[1]; w->rh = b[2]; w->bs = b[3]; w->bt = b[4]; w->bkt = b[5];
+  }
   PFEM2_TRY(ws_alloc(w, &w->scount, 32 * (size_t)maxsys));
   PFEM2_TRY(ws_alloc(w, &w->active, 1));
-  if (getenv("PFEM2_SOLVER_PROFILE"))
-    for (int k = 0; k < 3; ++k) PFEM2_TRY(ws_alloc(w, &w->prof[k], (size_t)w->grid[k == 1 ? 0 : 1] * 8 * 3));
   for (int k = 0; k < 3; ++k) {
     PFEM2_TRY(ws_alloc(w, &w->out_it[k], maxsys));
     PFEM2_TRY(ws_alloc(w, &w->out_res[k], maxsys));
+    PFEM2_TRY(ws_alloc(w, &w->out_tol[k], maxsys));
     PFEM2_TRY(ws_alloc(w, &w->out_outer[k], maxsys));
   }
   // pressure phase without multigrid: level-0 staging only
@@ -1349,7 +1519,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   // must leave room in the two-blocks-per-SM shared-memory budget
   const int coarse_max = w->mg_minb == 1 ? 160 : 128;
   PFEM2_TRY(mg_build(c, A, col, len, w->h_tiles0, w->h_sys_t0_0, w->h_blk_t0_0, w->split, coarse_max, H));
-  const size_t rs = c.mixed ? sizeof(float) : sizeof(double);
+  const size_t rs = c.kmixed ? sizeof(float) : sizeof(double);
   w->dmax = H.dmax;
   w->s1max = H.s1max;
   w->s2max = H.s2max;
@@ -1417,7 +1587,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
     set_error("krylov: the pressure multigrid's per-block data exceed shared memory");
     return PFEM2_INVALID_ARG;
   }
-  const int occ = occupancy_any<true>(c.mixed, w->mg_minb, smem);
+  const int occ = occupancy_any<true>(c.kmixed, w->mg_minb, smem);
   if (occ * c.num_sms < w->grid[0]) {
     set_error("krylov: the multigrid solver grid cannot be resident");
     return PFEM2_CUDA_ERROR;
@@ -1425,15 +1595,6 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   w->stage[0] = stage;
   w->smem[0] = smem;
   {
-    char buf[512];
-    snprintf(buf, sizeof(buf),
-             "multigrid: dofs %d %d %d %d; per block max lists S1 %d S2 %d S3 %d; nnz R01 %zu R02/Pt1^T %zu C3 %zu "
-             "J1 %zu P1 %zu J2 %zu P2 %zu P0 %zu; staged 0x%x, %zu bytes of shared memory\n",
-             c.nv, H.n[1], H.n[2], H.n[3], H.s1max, H.s2max, H.s3max, H.r01_col.size(),
-             w->split ? H.q2_col.size() : H.r02_col.size(),
-             H.c3_col.size(), H.s_jcol[1].size(), H.s_pcol[1].size(), H.s_jcol[2].size(), H.s_pcol[2].size(),
-             H.p0_col.size(), stage, smem);
-    w->mg_info = buf;
     const long long sz[12] = {c.nv, H.n[1], H.n[2], H.n[3], (long long)H.r01_col.size(),
                               (long long)(w->split ? H.q2_col.size() : H.r02_col.size()),
                               (long long)H.c3_col.size(), (long long)H.p0_col.size(), (long long)H.s_jcol[1].size(),
@@ -1450,38 +1611,38 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   }
   PFEM2_TRY(ws_upload(w, &w->r01_ptr, H.r01_ptr));
   PFEM2_TRY(ws_upload(w, &w->r01_col, H.r01_col));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r01_val, H.r01_val));
+  PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->r01_val, H.r01_val));
   PFEM2_TRY(ws_upload(w, &w->r02_ptr, H.r02_ptr));
   PFEM2_TRY(ws_upload(w, &w->r02_col, H.r02_col));
   PFEM2_TRY(ws_upload(w, &w->q2_ptr, H.q2_ptr));
   PFEM2_TRY(ws_upload(w, &w->q2_col, H.q2_col));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->q2_val, H.q2_val));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->r02_val, H.r02_val));
+  PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->q2_val, H.q2_val));
+  PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->r02_val, H.r02_val));
   PFEM2_TRY(ws_upload(w, &w->c3_blk, H.c3_blk));
   PFEM2_TRY(ws_upload(w, &w->c3_ptr, H.c3_ptr));
   PFEM2_TRY(ws_upload(w, &w->c3_col, H.c3_col));
   PFEM2_TRY(ws_upload(w, &w->c3_lk, H.c3_lk));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->c3_val, H.c3_val));
+  PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->c3_val, H.c3_val));
   PFEM2_TRY(ws_upload(w, &w->g3_ptr, H.g3_ptr));
   PFEM2_TRY(ws_upload(w, &w->c3_pos, H.c3_pos));
   {
     std::vector<double> zero(std::max<size_t>(1, H.c3_lk.size()), 0.0);
-    PFEM2_TRY(ws_upload_r(w, c.mixed, &w->contrib, zero));
+    PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->contrib, zero));
   }
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->j0, H.j0));
+  PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->j0, H.j0));
   PFEM2_TRY(ws_upload(w, &w->p0_ptr, H.p0_ptr));
   PFEM2_TRY(ws_upload(w, &w->p0_len, H.p0_len));
   PFEM2_TRY(ws_upload(w, &w->p0_col, H.p0_col));
-  PFEM2_TRY(ws_upload_r(w, c.mixed, &w->p0_val, H.p0_val));
+  PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->p0_val, H.p0_val));
   for (int l = 1; l <= 2; ++l) {
     PFEM2_TRY(ws_upload(w, &w->blk_s[l], H.blk_s[l]));
     PFEM2_TRY(ws_upload(w, &w->s_lk[l], H.s_sys[l]));
     PFEM2_TRY(ws_upload(w, &w->s_jptr[l], H.s_jptr[l]));
     PFEM2_TRY(ws_upload(w, &w->s_jcol[l], H.s_jcol[l]));
-    PFEM2_TRY(ws_upload_r(w, c.mixed, &w->s_jval[l], H.s_jval[l]));
+    PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->s_jval[l], H.s_jval[l]));
     PFEM2_TRY(ws_upload(w, &w->s_pptr[l], H.s_pptr[l]));
     PFEM2_TRY(ws_upload(w, &w->s_pcol[l], H.s_pcol[l]));
-    PFEM2_TRY(ws_upload_r(w, c.mixed, &w->s_pval[l], H.s_pval[l]));
+    PFEM2_TRY(ws_upload_r(w, c.kmixed, &w->s_pval[l], H.s_pval[l]));
   }
   PFEM2_TRY(ws_upload(w, &w->blk_s3, H.blk_s3));
   PFEM2_TRY(ws_upload(w, &w->s3_lk, H.s3_sys));
@@ -1493,7 +1654,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   PFEM2_TRY(ws_upload(w, &w->sys_off3, H.sys_off3));
   PFEM2_TRY(ws_upload(w, &w->sys_n2, H.sys_n2));
   PFEM2_TRY(ws_upload(w, &w->sys_off2, H.sys_off2));
-  if (c.mixed) {
+  if (c.kmixed) {
     float *b1, *b2;
     PFEM2_TRY(ws_alloc(w, &b1, H.n[1]));
     PFEM2_TRY(ws_alloc(w, &b2, H.n[2]));
@@ -1573,8 +1734,8 @@ static pfem2_status solve_impl(Ctx& c, int which) {
     const int kk = k < ncomp ? k : 0;
     const int mtx = which == 0 ? kk : (which == 1 ? 3 : 4 + kk);
     a.A64[k] = c.A64[mtx];
-    a.Ain[k] = c.mixed ? (const R*)c.A32[mtx] : (const R*)c.A64[mtx];
-    a.dinv[k] = c.mixed ? (const R*)c.dinv32[mtx] : (const R*)c.dinv64[mtx];
+    a.Ain[k] = c.kmixed ? (const R*)c.A32[mtx] : (const R*)c.A64[mtx];
+    a.dinv[k] = c.kmixed ? (const R*)c.dinv32[mtx] : (const R*)c.dinv64[mtx];
     if (which == 0) {
       a.x[k] = c.F[PFEM2_FIELD_PRED_VX + kk];
       a.b[k] = c.rhs[kk];
@@ -1593,6 +1754,10 @@ static pfem2_status solve_impl(Ctx& c, int which) {
     }
   }
   a.tol_i = (const double*)c.sys_scalars + (which == 1 ? ni : 0);
+  a.rtol_i = (const double*)c.sys_scalars + 2 * ni + (which == 1 ? ni : 0);
+  a.bicg = w->bicg[ph] ? 1 : 0;
+  a.nsum = mg ? 2 : w->nsum[ph];
+  a.bz = (R*)w->bz; a.bw = (R*)w->bw; a.rh = (R*)w->rh; a.bs = (R*)w->bs; a.bt = (R*)w->bt; a.bkt = (R*)w->bkt;
   a.maxit_i = c.d_sysinfo;
   a.e = (R*)w->e; a.r = (R*)w->r; a.z = (R*)w->z; a.q = (R*)w->q; a.p = (R*)w->p;
   a.r64 = w->r64;
@@ -1601,15 +1766,17 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.active = w->active;
   a.out_it = w->out_it[which];
   a.out_res = w->out_res[which];
+  a.out_tol = w->out_tol[which];
   a.out_outer = w->out_outer[which];
-  a.eta = c.mixed ? c.refine_eta : 0.0;
+  a.eta = c.kmixed ? c.refine_eta : 0.0;
   int mx = 0;
   for (auto& in : c.inst) mx = std::max(mx, in.cs.max_iter > 0 ? in.cs.max_iter : 10000);
-  a.iter_cap = (mg ? (w->split ? 4 : 3) : 2) * mx + 256;
+  // phases per iteration, and BiCGStab's restarts (three phases each, at most max_iter)
+  a.iter_cap = (mg ? (w->split ? 4 : 3) : (a.bicg ? 5 : 2)) * mx + 256;
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
-  a.prof = w->prof[which];
+  a.gb.spin_limit = c.spin_limit;
   k_init_solve<<<std::max(1, std::min(64, (32 * a.nsys + 255) / 256)), 256, 0, c.stream>>>(
       a.nsys, w->active, c.barrier, c.d_err, w->scount, 32 * a.nsys);
   c.launches++;
@@ -1626,7 +1793,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
 }
 
 pfem2_status krylov_solve(Ctx& c, int which) {
-  return c.mixed ? solve_impl<float>(c, which) : solve_impl<double>(c, which);
+  return c.kmixed ? solve_impl<float>(c, which) : solve_impl<double>(c, which);
 }
 
 // per-system iteration counts / residuals into c.stats (max over
@@ -1636,9 +1803,10 @@ static pfem2_status read_stats_phase(Ctx& c, int which) {
   const int ph = which == 1 ? 0 : 1;
   const int ns = w->nsys[ph];
   std::vector<int> it(ns), outer(ns);
-  std::vector<double> res(ns);
+  std::vector<double> res(ns), tolv(ns);
   PFEM2_CUDA(cudaMemcpyAsync(it.data(), w->out_it[which], sizeof(int) * ns, cudaMemcpyDeviceToHost, c.stream));
   PFEM2_CUDA(cudaMemcpyAsync(res.data(), w->out_res[which], sizeof(double) * ns, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaMemcpyAsync(tolv.data(), w->out_tol[which], sizeof(double) * ns, cudaMemcpyDeviceToHost, c.stream));
   PFEM2_CUDA(cudaMemcpyAsync(outer.data(), w->out_outer[which], sizeof(int) * ns, cudaMemcpyDeviceToHost, c.stream));
   PFEM2_CUDA(cudaStreamSynchronize(c.stream));
   const int ni = (int)c.inst.size();
@@ -1653,8 +1821,8 @@ static pfem2_status read_stats_phase(Ctx& c, int which) {
       mit = std::max(mit, it[s]);
       mo = std::max(mo, outer[s]);
       mres = std::max(mres, res[s]);
-      const double tol = which == 1 ? c.inst[i].cs.p_tol : c.inst[i].cs.vel_tol;
-      if (res[s] > tol) notconv = true;
+      // (the tolerance the kernel applied: max(tol, rtol |b|))
+      if (!(res[s] <= tolv[s])) notconv = true;
     }
     c.stats.iters[slot] = mit;
     c.stats.residual[slot] = mres;
@@ -1669,42 +1837,6 @@ void krylov_sizes(Ctx& c, long long* out12) {
   for (int k = 0; k < 12; ++k) out12[k] = (w && w->mg) ? w->mg_sizes[k] : 0;
 }
 
-std::string krylov_profile(Ctx& c) {
-  // per solve kind and action: phases (block 0), mean and max over blocks
-  // of the work per phase, and block 0's mean barrier wait, in microseconds
-  KrylovWs* w = (KrylovWs*)c.kws;
-  std::string out;
-  if (!w) return out;
-  static const char* kind[3] = {"prediction", "pressure", "correction"};
-  static const char* act[8] = {"-", "out_a", "out_b", "out_done", "a", "b", "uz", "b2"};
-  out += w->mg_info;
-  for (int k = 0; k < 3; ++k) {
-    if (!w->prof[k]) continue;
-    const int G = w->grid[k == 1 ? 0 : 1];
-    std::vector<unsigned long long> h((size_t)G * 24);
-    if (cudaMemcpy(h.data(), w->prof[k], sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
-      return out;
-    char buf[160];
-    out += kind[k];
-    for (int a = 0; a < 8; ++a) {
-      const unsigned long long n0 = h[a * 3];
-      if (n0 == 0) continue;
-      double mean = 0.0, mx = 0.0;
-      for (int b = 0; b < G; ++b) {
-        const double n = (double)h[((size_t)b * 8 + a) * 3];
-        const double wk = n > 0 ? h[((size_t)b * 8 + a) * 3 + 1] / n : 0.0;
-        mean += wk / G;
-        mx = std::max(mx, wk);
-      }
-      snprintf(buf, sizeof(buf), " %s:%llu:%.2f:%.2f:%.2f", act[a], n0, mean * 1e-3, mx * 1e-3,
-               (double)h[a * 3 + 2] / n0 * 1e-3);
-      out += buf;
-    }
-    out += "\n";
-  }
-  return out;
-}
-
 pfem2_status krylov_read_stats(Ctx& c) {
   pfem2_status worst = PFEM2_OK;
   for (int wch = 0; wch < 3; ++wch) {
@@ -1715,6 +1847,7 @@ pfem2_status krylov_read_stats(Ctx& c) {
   PFEM2_CUDA(cudaMemcpy(&err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err == 1) {
     set_error("krylov: a wait for the other blocks timed out");
+    c.failed = true;
     return PFEM2_TIMEOUT;
   }
   if (err == 2) {

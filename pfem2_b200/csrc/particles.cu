@@ -16,6 +16,7 @@
 //                   (:723-772), with the projection partials fused in
 //   k_project_*     distribute_particle_velocities_to_grid (:858-918)
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 #include "common.cuh"
@@ -106,8 +107,8 @@ static pfem2_status seed_impl(Ctx& c, uint64_t seed, double jitter) {
 
 pfem2_status launch_seed(Ctx& c, int instance, const uint32_t q[3], uint64_t seed, double jitter) {
   (void)instance;
-  if (c.dim == 2) return c.mixed ? seed_impl<2, float>(c, seed, jitter) : seed_impl<2, double>(c, seed, jitter);
-  return c.mixed ? seed_impl<3, float>(c, seed, jitter) : seed_impl<3, double>(c, seed, jitter);
+  if (c.dim == 2) return c.pmixed ? seed_impl<2, float>(c, seed, jitter) : seed_impl<2, double>(c, seed, jitter);
+  return c.pmixed ? seed_impl<3, float>(c, seed, jitter) : seed_impl<3, double>(c, seed, jitter);
 }
 
 // -------------------------------------------------------- real mirrors
@@ -138,8 +139,8 @@ static pfem2_status sync_real_impl(Ctx& c) {
 }
 
 pfem2_status launch_sync_real_fields(Ctx& c) {
-  if (c.dim == 2) return c.mixed ? sync_real_impl<2, float>(c) : sync_real_impl<2, double>(c);
-  return c.mixed ? sync_real_impl<3, float>(c) : sync_real_impl<3, double>(c);
+  if (c.dim == 2) return c.pmixed ? sync_real_impl<2, float>(c) : sync_real_impl<2, double>(c);
+  return c.pmixed ? sync_real_impl<3, float>(c) : sync_real_impl<3, double>(c);
 }
 
 // --------------------------------------------------------------- correct
@@ -179,8 +180,8 @@ static pfem2_status correct_impl(Ctx& c) {
 }
 
 pfem2_status launch_correct(Ctx& c) {
-  if (c.dim == 2) return c.mixed ? correct_impl<2, float>(c) : correct_impl<2, double>(c);
-  return c.mixed ? correct_impl<3, float>(c) : correct_impl<3, double>(c);
+  if (c.dim == 2) return c.pmixed ? correct_impl<2, float>(c) : correct_impl<2, double>(c);
+  return c.pmixed ? correct_impl<3, float>(c) : correct_impl<3, double>(c);
 }
 
 // ---------------------------------------------------------------- advect
@@ -597,8 +598,8 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
 pfem2_status launch_advect(Ctx& c, bool fuse) {
   PFEM2_CUDA(cudaMemsetAsync(c.d_counters, 0, sizeof(int) * CNT_N, c.stream));
   PFEM2_CUDA(cudaMemsetAsync(c.dest_mask, 0, sizeof(unsigned) * c.nc, c.stream));
-  if (c.dim == 2) return c.mixed ? advect_impl<2, float>(c, fuse) : advect_impl<2, double>(c, fuse);
-  return c.mixed ? advect_impl<3, float>(c, fuse) : advect_impl<3, double>(c, fuse);
+  if (c.dim == 2) return c.pmixed ? advect_impl<2, float>(c, fuse) : advect_impl<2, double>(c, fuse);
+  return c.pmixed ? advect_impl<3, float>(c, fuse) : advect_impl<3, double>(c, fuse);
 }
 
 // ----------------------------------------------------------------- rebin
@@ -719,7 +720,6 @@ __device__ __forceinline__ int far_lower_bound(const unsigned long long* keys, i
 // bits 62-63 = 1 (tile aggregate known) or 2 (inclusive prefix known), the
 // low bits the value
 constexpr unsigned long long kTileAgg = 1ull << 62, kTilePre = 2ull << 62, kTileVal = (1ull << 62) - 1;
-constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 // One pass: a block takes tiles of kRebinWarps consecutive target cells in
 // ticket order (an atomic counter, so a block waits only on tiles taken by
@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(kRebinWarps * 32, RebinMinBlocks<DIM, R>::valu
     const unsigned* __restrict__ dest_mask, const unsigned long long* __restrict__ far_keys, int far_cap,
     const DevInst* __restrict__ inst, const int* __restrict__ cell_inst, const int* __restrict__ cv,
     const R* __restrict__ Vr, int nv, R* __restrict__ partial, int list_cap, int* __restrict__ counters,
-    unsigned long long* __restrict__ tiles) {
+    unsigned long long* __restrict__ tiles, unsigned spin_limit) {
   constexpr int NV = Dims<DIM>::NV;
   extern __shared__ int smem[];
   __shared__ int s_tile, s_base;
@@ -931,7 +931,7 @@ __global__ void __launch_bounds__(kRebinWarps * 32, RebinMinBlocks<DIM, R>::valu
           const int lp = pre ? __ffs(pre) - 1 : 31;
           const unsigned upto = lp == 31 ? PFEM2_FULL_MASK : (2u << lp) - 1u;
           if (wait & upto) {
-            if (++spins > kLookbackSpinLimit) {
+            if (++spins > spin_limit) {
               if (lane == 0) atomicExch(counters + CNT_SCAN_TIMEOUT, 1);
               break;
             }
@@ -1023,7 +1023,8 @@ static void rebin_launch(Ctx& c, const int* newcell) {
       c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, c.pcell[nb], (R*)c.pxi[nb],
       (R*)c.pu[nb], c.cell_start[nb], c.d_np + nb, c.nc, c.ring_ptr, c.ring_cell, c.ring_rev, c.dest_mask, c.far_keys,
       c.far_cap, c.d_inst,
-      c.cell_inst, c.cv, (const R*)c.Vr, c.nv, (R*)c.partial, c.list_cap, c.d_counters, c.rebin_tiles);
+      c.cell_inst, c.cv, (const R*)c.Vr, c.nv, (R*)c.partial, c.list_cap, c.d_counters, c.rebin_tiles,
+      c.spin_limit >> 2);
   c.launches += 1;
   c.cur = nb;
 }
@@ -1054,8 +1055,8 @@ pfem2_status launch_rebin(Ctx& c, bool check, bool proj, bool from_advect) {
     // no movers: make sure the far list is empty
     PFEM2_CUDA(cudaMemsetAsync(c.d_counters + CNT_FAR, 0, sizeof(int), c.stream));
   }
-  if (c.dim == 2) return c.mixed ? rebin_impl<2, float>(c, check, proj, from_advect) : rebin_impl<2, double>(c, check, proj, from_advect);
-  return c.mixed ? rebin_impl<3, float>(c, check, proj, from_advect) : rebin_impl<3, double>(c, check, proj, from_advect);
+  if (c.dim == 2) return c.pmixed ? rebin_impl<2, float>(c, check, proj, from_advect) : rebin_impl<2, double>(c, check, proj, from_advect);
+  return c.pmixed ? rebin_impl<3, float>(c, check, proj, from_advect) : rebin_impl<3, double>(c, check, proj, from_advect);
 }
 
 // --------------------------------------------------------------- project
@@ -1201,8 +1202,8 @@ static pfem2_status project_impl(Ctx& c, bool partials_ready) {
 }
 
 pfem2_status launch_project(Ctx& c, bool partials_ready) {
-  if (c.dim == 2) return c.mixed ? project_impl<2, float>(c, partials_ready) : project_impl<2, double>(c, partials_ready);
-  return c.mixed ? project_impl<3, float>(c, partials_ready) : project_impl<3, double>(c, partials_ready);
+  if (c.dim == 2) return c.pmixed ? project_impl<2, float>(c, partials_ready) : project_impl<2, double>(c, partials_ready);
+  return c.pmixed ? project_impl<3, float>(c, partials_ready) : project_impl<3, double>(c, partials_ready);
 }
 
 // -------------------------------------------------- particle state access
@@ -1252,8 +1253,8 @@ static pfem2_status read_impl(Ctx& c, int instance, int* cell, double* xi, doubl
 }
 
 pfem2_status read_particles(Ctx& c, int instance, int* cell, double* xi, double* u, int* n) {
-  if (c.dim == 2) return c.mixed ? read_impl<2, float>(c, instance, cell, xi, u, n) : read_impl<2, double>(c, instance, cell, xi, u, n);
-  return c.mixed ? read_impl<3, float>(c, instance, cell, xi, u, n) : read_impl<3, double>(c, instance, cell, xi, u, n);
+  if (c.dim == 2) return c.pmixed ? read_impl<2, float>(c, instance, cell, xi, u, n) : read_impl<2, double>(c, instance, cell, xi, u, n);
+  return c.pmixed ? read_impl<3, float>(c, instance, cell, xi, u, n) : read_impl<3, double>(c, instance, cell, xi, u, n);
 }
 
 // unsorted particles in, stable sort by cell through the rebin machinery:
@@ -1292,6 +1293,11 @@ static pfem2_status set_impl(Ctx& c, const int* counts, const int* cell, const d
         set_error("set_particles: cell out of range");
         return PFEM2_INVALID_ARG;
       }
+      for (int d = 0; d < DIM; ++d)
+        if (!std::isfinite(xi[k * DIM + d]) || !std::isfinite(u[k * DIM + d])) {
+          set_error("set_particles: a coordinate or velocity is not finite");
+          return PFEM2_INVALID_ARG;
+        }
       gcell[k] = lc + c.inst[i].c_off;
       cnt[gcell[k] + 1]++;
     }
@@ -1325,8 +1331,8 @@ static pfem2_status set_impl(Ctx& c, const int* counts, const int* cell, const d
 }
 
 pfem2_status launch_set_particles(Ctx& c, const int* counts, const int* cell, const double* xi, const double* u) {
-  if (c.dim == 2) return c.mixed ? set_impl<2, float>(c, counts, cell, xi, u) : set_impl<2, double>(c, counts, cell, xi, u);
-  return c.mixed ? set_impl<3, float>(c, counts, cell, xi, u) : set_impl<3, double>(c, counts, cell, xi, u);
+  if (c.dim == 2) return c.pmixed ? set_impl<2, float>(c, counts, cell, xi, u) : set_impl<2, double>(c, counts, cell, xi, u);
+  return c.pmixed ? set_impl<3, float>(c, counts, cell, xi, u) : set_impl<3, double>(c, counts, cell, xi, u);
 }
 
 }  // namespace pfem2

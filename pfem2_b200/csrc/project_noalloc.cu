@@ -10,13 +10,16 @@
 // the library holds until the process exits.
 //
 // The host code cannot use the array's name as a device address (in host
-// code it is a stand-in symbol), so the first call on each device, with that
-// device current, looks the address up with cudaGetSymbolAddress and caches
-// it; that first call should therefore not happen inside a stream capture.
-// All calls share the array: calls that overlap on the GPU (other streams,
-// other threads) race on it and must be serialized by the caller. Every
-// entry a call reads has been written by the same call, so no clearing is
-// needed between calls.
+// code it is a stand-in symbol), so a call on a stream that is not being
+// captured, with the device current, looks the address up with
+// cudaGetSymbolAddress (again each time, so that a reloaded module after
+// cudaDeviceReset is found) and caches it per device; a call made while its
+// stream is being captured uses the cached address, so the first call on a
+// device must come before any capture. All calls share the array: calls
+// that overlap on the GPU (other streams, other threads) race on it and must
+// be serialized by the caller. Every scratch entry a call reads has been
+// written by the same call (incidences naming a cell outside [0, n_cells)
+// are not read: the vertex gets NaN), so no clearing is needed between calls.
 #include <mutex>
 
 #include "common.cuh"
@@ -68,24 +71,40 @@ __global__ void __launch_bounds__(256) k_noalloc_cells(int nc, const int* __rest
   }
 }
 
+// node sums over the incident cells' partials in incidence order; an
+// incidence whose cell or local vertex index is out of range makes the
+// vertex NaN instead of reading scratch that this call did not write; a
+// vertex flagged in zero_flag (may be null) gets velocity 0, as the wall
+// vertices after distribute_particle_velocities_to_grid
+// (TurekBenchmarkCuda/pfem2particle.cu:866-869)
 template <int DIM>
-__global__ void __launch_bounds__(256) k_noalloc_nodes(int nv, const int* __restrict__ v2c_ptr,
+__global__ void __launch_bounds__(256) k_noalloc_nodes(int nv, int nc, const int* __restrict__ v2c_ptr,
                                                        const int* __restrict__ v2c_cell,
                                                        const int* __restrict__ v2c_local,
+                                                       const unsigned char* __restrict__ zero_flag,
                                                        const double* __restrict__ partial,
                                                        double* __restrict__ node_u, double* __restrict__ node_w) {
+  constexpr int NV = Dims<DIM>::NV;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
     double s[DIM + 1];
 #pragma unroll
     for (int k = 0; k <= DIM; ++k) s[k] = 0.0;
+    bool bad = false;
     for (int k = v2c_ptr[v]; k < v2c_ptr[v + 1]; ++k) {
-      const double* pp = partial + (size_t)v2c_cell[k] * kNoallocK + v2c_local[k] * (DIM + 1);
+      const int c = v2c_cell[k], l = v2c_local[k];
+      if (c < 0 || c >= nc || l < 0 || l >= NV) {
+        bad = true;
+        continue;
+      }
+      const double* pp = partial + (size_t)c * kNoallocK + l * (DIM + 1);
 #pragma unroll
       for (int q = 0; q <= DIM; ++q) s[q] += pp[q];
     }
-    const double w = s[DIM];
+    const double w = bad ? nan("") : s[DIM];
+    const bool zero = zero_flag != nullptr && zero_flag[v] != 0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) node_u[(size_t)v * DIM + d] = w != 0.0 ? s[d] / w : 0.0;
+    for (int d = 0; d < DIM; ++d)
+      node_u[(size_t)v * DIM + d] = bad ? w : ((w != 0.0 && !zero) ? s[d] / w : 0.0);
     node_w[v] = w;
   }
 }
@@ -97,8 +116,8 @@ using namespace pfem2;
 extern "C" pfem2_status pfem2_project_noalloc(int32_t dim, int32_t n_cells, int32_t n_vertices,
                                               const int32_t* vertex_cell_ptr, const int32_t* vertex_cell,
                                               const int32_t* vertex_cell_local, const int32_t* cell_start,
-                                              const double* xi, const double* u, double* node_u, double* node_w,
-                                              void* stream) {
+                                              const double* xi, const double* u, const uint8_t* zero_flag,
+                                              double* node_u, double* node_w, void* stream) {
   if (dim != 2 && dim != 3) {
     set_error("pfem2_project_noalloc: dim must be 2 or 3");
     return PFEM2_INVALID_ARG;
@@ -121,30 +140,35 @@ extern "C" pfem2_status pfem2_project_noalloc(int32_t dim, int32_t n_cells, int3
     set_error("pfem2_project_noalloc: device ordinal out of range");
     return PFEM2_INVALID_ARG;
   }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PFEM2_CUDA(cudaStreamIsCapturing(st, &cap));
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       PFEM2_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partial));
       g_noalloc_addr[dev] = (double*)p;
+    } else if (!g_noalloc_addr[dev]) {
+      set_error("pfem2_project_noalloc: the first call on a device must come before any stream capture");
+      return PFEM2_BAD_STATE;
     }
     scratch = g_noalloc_addr[dev];
   }
   if (n_cells == 0 && n_vertices == 0) return PFEM2_OK;
-  cudaStream_t st = (cudaStream_t)stream;
   const int cgrid = (int)std::min<long long>(((long long)n_cells * 32 + 255) / 256, 148LL * 16);
   const int vgrid = (int)std::min<long long>(((long long)n_vertices + 255) / 256, 148LL * 16);
   if (dim == 2) {
     if (n_cells) k_noalloc_cells<2><<<cgrid, 256, 0, st>>>(n_cells, cell_start, xi, u, scratch);
     if (n_vertices)
-      k_noalloc_nodes<2><<<vgrid, 256, 0, st>>>(n_vertices, vertex_cell_ptr, vertex_cell, vertex_cell_local, scratch,
-                                               node_u, node_w);
+      k_noalloc_nodes<2><<<vgrid, 256, 0, st>>>(n_vertices, n_cells, vertex_cell_ptr, vertex_cell, vertex_cell_local,
+                                               zero_flag, scratch, node_u, node_w);
   } else {
     if (n_cells) k_noalloc_cells<3><<<cgrid, 256, 0, st>>>(n_cells, cell_start, xi, u, scratch);
     if (n_vertices)
-      k_noalloc_nodes<3><<<vgrid, 256, 0, st>>>(n_vertices, vertex_cell_ptr, vertex_cell, vertex_cell_local, scratch,
-                                               node_u, node_w);
+      k_noalloc_nodes<3><<<vgrid, 256, 0, st>>>(n_vertices, n_cells, vertex_cell_ptr, vertex_cell, vertex_cell_local,
+                                               zero_flag, scratch, node_u, node_w);
   }
   PFEM2_CUDA(cudaGetLastError());
   return PFEM2_OK;

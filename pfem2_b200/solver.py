@@ -78,7 +78,7 @@ def load_library(path=LIB_PATH):
         "pfem2_enable_stage_timing": [vp, C.c_int32],
         "pfem2_get_stream": [vp, C.POINTER(vp)],
     }
-    sig["pfem2_project_noalloc"] = [C.c_int32, C.c_int32, C.c_int32] + [vp] * 8 + [vp]
+    sig["pfem2_project_noalloc"] = [C.c_int32, C.c_int32, C.c_int32] + [vp] * 9 + [vp]
     for name, args in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -102,7 +102,8 @@ class Solver:
     """pfem2Solver over a batch of instances (one instance = one case)."""
 
     def __init__(self, specs, precision=A.PREC_MIXED, device=0, movement_steps=None, max_per_part=None,
-                 use_graph=True, capacity_factor=2.0, per_cell_max=0, particles_only=False):
+                 use_graph=True, capacity_factor=2.0, per_cell_max=0, particles_only=False, fp32_stages=0,
+                 far_capacity=0):
         if not isinstance(specs, (list, tuple)):
             specs = [specs]
         self.L = load_library()
@@ -116,9 +117,10 @@ class Solver:
         cfg.max_particles_per_cell_part = max_per_part if max_per_part is not None else specs[0].max_per_part
         cfg.particles_per_cell_max = per_cell_max
         cfg.particle_capacity_factor = capacity_factor
-        cfg.far_mover_capacity = 0
+        cfg.far_mover_capacity = far_capacity
         cfg.use_graph = 1 if use_graph else 0
         cfg.particles_only = 1 if particles_only else 0
+        cfg.fp32_stages = fp32_stages
         self.cfg = cfg
         h = C.c_void_p()
         self._check(self.L.pfem2_create(C.byref(cfg), C.byref(h)))
@@ -261,7 +263,13 @@ class Solver:
             b = np.tile(cv, (1, nvc)).reshape(-1)
             nnz += len(np.unique(a * sp.mesh.n_vertices + b))
             rows += sp.mesh.n_vertices
-        return {"rows": rows, "nnz": nnz, "real_bytes": 4 if self.cfg.precision == A.PREC_MIXED else 8}
+        return {"rows": rows, "nnz": nnz, "real_bytes": 4 if A.FP32_KRYLOV & self.fp32_stages() else 8}
+
+    def fp32_stages(self):
+        """The PFEM2_FP32_* stages this context runs in FP32."""
+        if self.cfg.precision != A.PREC_MIXED:
+            return 0
+        return self.cfg.fp32_stages or A.FP32_DEFAULT
 
     def enable_stage_timing(self, on=True):
         self._check(self.L.pfem2_enable_stage_timing(self.h, 1 if on else 0))

@@ -36,6 +36,7 @@ def compare_particles(o, g, eps_face, xi_tol, u_tol):
     du = np.abs(ou[idx_o] - gu[idx_g]).max(initial=0.0)
     bad_cells = np.nonzero(~same)[0]
     flips = 0
+    max_flip_dist = 0.0
     for c in bad_cells:
         a = ox[so[c]:so[c + 1]]
         b = gx[sg[c]:sg[c + 1]]
@@ -46,7 +47,25 @@ def compare_particles(o, g, eps_face, xi_tol, u_tol):
                     continue
                 assert near_face(p[None, :], eps_face)[0], f"membership differs away from faces in cell {c}: {p}"
                 flips += 1
+                max_flip_dist = max(max_flip_dist, float(np.min(np.minimum(p, 1.0 - p))))
     assert dxi <= xi_tol, f"max |xi diff| {dxi} > {xi_tol}"
     assert du <= u_tol, f"max |u diff| {du} > {u_tol}"
     return {"dxi": dxi, "du": du, "flip_cells": len(bad_cells), "flips": flips,
-            "n_o": len(oc), "n_g": len(gc)}
+            "max_flip_dist": max_flip_dist, "n_o": len(oc), "n_g": len(gc)}
+
+
+# Precision modes of the library under test:
+#   fp64   everything FP64 (PFEM2_PREC_FP64)
+#   mixed  the default mixed path: FP32 inner Krylov iterations refined in
+#          FP64, everything else FP64 (fields within 1e-6 of fp64)
+#   fp32   every stage that can run in FP32 does (particles, right-hand
+#          sides, inner Krylov): the fast path, looser bars
+MODES = ["fp64", "mixed", "fp32"]
+
+
+def solver_kw(mode):
+    from pfem2_b200 import _abi as A
+
+    return {"fp64": {"precision": A.PREC_FP64, "fp32_stages": 0},
+            "mixed": {"precision": A.PREC_MIXED, "fp32_stages": 0},
+            "fp32": {"precision": A.PREC_MIXED, "fp32_stages": A.FP32_ALL}}[mode]

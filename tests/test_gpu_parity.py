@@ -1,8 +1,11 @@
 """Parity of the CUDA library (through the C ABI) against the FP64 oracle.
 
-Membership must match exactly except for particles within 1e-6 (FP64 path)
-or 2e-5 (mixed path, FP32 reference coordinates) of a cell face; floating
-point results are compared with the tolerances written in each test.
+Three precision modes (tests/helpers.py MODES): fp64, the default mixed path
+(FP32 inner Krylov iterations refined in FP64) and fp32 (every FP32 stage,
+FP32 particle coordinates). Membership must match exactly except for
+particles within 1e-6 of a cell face (fp64, mixed) or within the measured
+2e-5 band of FP32 reference coordinates (fp32); floating point results are
+compared with the tolerances written in each test.
 """
 import numpy as np
 import pytest
@@ -11,13 +14,13 @@ import oracle as O
 from pfem2_b200 import _abi as A
 from pfem2_b200 import cases
 from pfem2_b200.solver import Solver
-from tests.helpers import compare_particles, rel_l2
+from tests.helpers import MODES, compare_particles, rel_l2, solver_kw
 
 pytestmark = pytest.mark.gpu
 
-PRECS = [A.PREC_FP64, A.PREC_MIXED]
-FACE_EPS = {A.PREC_FP64: 1e-6, A.PREC_MIXED: 2e-5}
-XI_TOL = {A.PREC_FP64: 1e-11, A.PREC_MIXED: 2e-5}
+PRECS = MODES
+FACE_EPS = {"fp64": 1e-6, "mixed": 1e-6, "fp32": 2e-5}
+XI_TOL = {"fp64": 1e-11, "mixed": 1e-11, "fp32": 2e-5}
 
 
 def smooth_field(X, scale=1.0):
@@ -48,7 +51,13 @@ def spec_3d(dt=0.02, **kw):
 
 
 def make_pair(sp, prec, **kw):
-    g = Solver(sp, precision=prec, **kw)
+    """the library in mode `prec` (a MODES name, or a pfem2_precision value
+    with fp32_stages in kw) and the oracle on the same spec"""
+    if isinstance(prec, str):
+        kw = dict(kw, **solver_kw(prec))
+    else:
+        kw = dict(kw, precision=prec)
+    g = Solver(sp, **kw)
     o = O.Oracle(sp.mesh, sp.case, movement_steps=kw.get("movement_steps", sp.movement_steps),
                  max_per_part=kw.get("max_per_part", sp.max_per_part))
     return g, o
@@ -77,7 +86,7 @@ def test_seed(prec, dim):
     gc, gx, gu = g.particles()
     oc, ox, ou = o.particles()
     assert np.array_equal(gc, oc)
-    tol = 1e-14 if prec == A.PREC_FP64 else 1e-6
+    tol = 1e-6 if prec == "fp32" else 1e-14
     assert np.abs(gx - ox).max() <= tol
     assert np.abs(gu - ou).max() <= tol * 4
 
@@ -100,7 +109,7 @@ def test_correct(prec, dim):
     gc, gx, gu = g.particles()
     oc, ox, ou = o.particles()
     assert np.array_equal(gc, oc)
-    tol = 1e-13 if prec == A.PREC_FP64 else 2e-6
+    tol = 2e-6 if prec == "fp32" else 1e-13
     assert np.abs(gu - ou).max() <= tol
 
 
@@ -125,13 +134,17 @@ def test_move(prec, dim, check):
             g.advect()
             o.advect()
     r = compare_particles(o.particles(), g.particles(), FACE_EPS[prec], XI_TOL[prec],
-                          1e-12 if prec == A.PREC_FP64 else 1e-5)
+                          1e-5 if prec == "fp32" else 1e-12)
     gs, os_ = g.stats(), o.stats()
-    if prec == A.PREC_FP64:
+    # membership: exact in fp64 and mixed; with FP32 reference coordinates a
+    # particle may change cell only within the band of FACE_EPS (the largest
+    # face distance of a flipped particle measured here is reported)
+    if prec != "fp32":
         assert r["flips"] == 0
-        assert gs["deleted"] == os_["deleted"]
-        if check:
-            assert gs["removed"] == os_["removed"] and gs["reseeded"] == os_["reseeded"]
+    assert r["max_flip_dist"] <= FACE_EPS[prec]
+    assert gs["deleted"] == os_["deleted"]
+    if check:
+        assert gs["removed"] == os_["removed"] and gs["reseeded"] == os_["reseeded"]
     assert gs["far"] == 0
 
 
@@ -148,7 +161,7 @@ def test_project(prec, dim):
     o.seed_particles(q, seed=5, jitter=0.1)
     g.distribute_particle_velocities_to_grid()
     o.distribute_particle_velocities_to_grid()
-    tol = 1e-13 if prec == A.PREC_FP64 else 3e-7
+    tol = 3e-7 if prec == "fp32" else 1e-13
     for d in range(dim):
         assert rel_l2(g.field(A.FIELD_VX + d), o.field(A.FIELD_VX + d)) <= tol
     assert rel_l2(g.field(A.FIELD_NODE_WEIGHT), o.field(A.FIELD_NODE_WEIGHT)) <= tol
@@ -165,9 +178,9 @@ def test_fem_step(prec, dim):
     set_vel(g, o, sp, f)
     g.fem_step()
     o.fem_step(1)
-    # FP64: both solve to absolute residuals of 1e-13 (velocity) / 1e-12
-    # (pressure); mixed: FP32 assembly of the right-hand sides
-    tol = {A.PREC_FP64: 1e-8, A.PREC_MIXED: 2e-5}[prec]
+    # both solve to absolute residuals of 1e-13 (velocity) / 1e-12
+    # (pressure); fp32: FP32 assembly of the right-hand sides
+    tol = {"fp64": 1e-8, "mixed": 1e-8, "fp32": 2e-5}[prec]
     for fld in [A.FIELD_PRED_VX + d for d in range(dim)] + [A.FIELD_P] + [A.FIELD_VX + d for d in range(dim)]:
         e = rel_l2(g.field(fld), o.field(fld))
         assert e <= tol, (fld, e)
@@ -183,7 +196,7 @@ def test_steps_2d(prec):
     for _ in range(3):
         g.step()
         o.step(1)
-    tol = {A.PREC_FP64: 1e-8, A.PREC_MIXED: 1e-4}[prec]
+    tol = {"fp64": 1e-8, "mixed": 1e-7, "fp32": 1e-4}[prec]
     for fld in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P):
         e = rel_l2(g.field(fld), o.field(fld))
         assert e <= tol, (fld, e)
@@ -249,7 +262,7 @@ def test_deterministic():
 def test_particles_only_step(prec):
     """the particle-kernel workload: correct -> move -> project on a frozen field"""
     sp = cases.stress_2d(n=24)
-    g = Solver(sp, precision=prec, particles_only=True)
+    g = Solver(sp, particles_only=True, **solver_kw(prec))
     o = O.Oracle(sp.mesh, sp.case, movement_steps=sp.movement_steps, max_per_part=sp.max_per_part)
     ux, uy = sp.meta["ux"], sp.meta["uy"]
     for f, v in ((A.FIELD_VX, ux), (A.FIELD_VY, uy), (A.FIELD_PRED_VX, ux), (A.FIELD_PRED_VY, uy)):
@@ -270,30 +283,42 @@ def test_particles_only_step(prec):
         o.set_field(A.FIELD_VY, uy)
         oproj = proj
     gproj = [g.field(A.FIELD_OLD_VX), g.field(A.FIELD_OLD_VY)]
-    tol = {A.PREC_FP64: 1e-12, A.PREC_MIXED: 1e-4}[prec]
+    tol = {"fp64": 1e-12, "mixed": 1e-12, "fp32": 1e-4}[prec]
     for d in range(2):
         assert rel_l2(gproj[d], oproj[d]) <= tol
     r = compare_particles(o.particles(), g.particles(), FACE_EPS[prec], XI_TOL[prec],
-                          1e-12 if prec == A.PREC_FP64 else 1e-4)
-    if prec == A.PREC_FP64:
+                          1e-4 if prec == "fp32" else 1e-12)
+    if prec != "fp32":
         assert r["flips"] == 0
 
 
-def test_ensemble_batch_runs():
-    """a small batch of uneven channel instances converges in every stage"""
+def test_ensemble_batch_matches_oracle():
+    """a batch of four uneven channel instances (2k-6k cells, different
+    Reynolds numbers and radii) in one context: every instance equals the
+    oracle run of that instance alone (mixed path, solves to 1e-12 relative)"""
     specs = cases.ensemble(n=4, cells_lo=2000, cells_hi=6000)
+    for sp in specs:
+        sp.case.vel_tol = sp.case.p_tol = 0.0
+        sp.case.vel_rtol = sp.case.p_rtol = 1e-12
+    assert len({sp.mesh.n_cells for sp in specs}) == 4
     s = Solver(specs, precision=A.PREC_MIXED)
     s.seed_particles(specs[0].q, 2, 0.0)
     for _ in range(2):
         s.step()
-    st = s.stats()
-    assert st["status"] == A.OK
-    for i in range(len(specs)):
-        v = s.field(A.FIELD_VX, i)
-        assert np.all(np.isfinite(v)) and np.abs(v).max() < 10.0
+    assert s.stats()["status"] == A.OK
+    for i, sp in enumerate(specs):
+        o = O.Oracle(sp.mesh, sp.case, movement_steps=sp.movement_steps, max_per_part=sp.max_per_part)
+        o.seed_particles(specs[0].q, 2, 0.0)
+        for _ in range(2):
+            o.step(1)
+        for fld in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P):
+            e = rel_l2(s.field(fld, i), o.field(fld))
+            assert e <= 1e-7, (i, fld, e)
+        assert s.n_particles(i) == o.n_particles()
 
 
-def test_advect_split_equals_one_kernel(monkeypatch):
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_advect_split_equals_one_kernel(monkeypatch, prec):
     """the two-kernel advection (used from ~8M particle slots: fast sub-steps,
     then the particles that left their cell) equals the one-kernel form bit
     for bit; forced here on a small case through PFEM2_ADVECT_SPLIT_MIN"""
@@ -301,7 +326,7 @@ def test_advect_split_equals_one_kernel(monkeypatch):
     outs = []
     for split_min in ("0", str(1 << 40)):
         monkeypatch.setenv("PFEM2_ADVECT_SPLIT_MIN", split_min)
-        s = Solver(sp, precision=A.PREC_MIXED)
+        s = Solver(sp, **solver_kw(prec))
         s.seed_particles(sp.q, seed=0, jitter=0.1)
         for _ in range(3):
             s.step()
@@ -320,7 +345,7 @@ def test_vorticity(prec):
     """calculate_vorticity on the library's own fields after two steps
     against the oracle's restatement on the same fields (FP64 in both)"""
     sp = cases.channel_disk(h=0.05, dt=0.01)
-    g = Solver(sp, precision=prec)
+    g = Solver(sp, **solver_kw(prec))
     g.seed_particles(sp.q, seed=0, jitter=0.1)
     for _ in range(2):
         g.step()
@@ -354,7 +379,7 @@ def test_wall_pushback_steps(prec):
     for _ in range(3):
         g.step()
         o.step(1)
-    tol = {A.PREC_FP64: 1e-8, A.PREC_MIXED: 1e-4}[prec]
+    tol = {"fp64": 1e-8, "mixed": 1e-7, "fp32": 1e-4}[prec]
     for fld in (A.FIELD_VX, A.FIELD_VY, A.FIELD_P):
         e = rel_l2(g.field(fld), o.field(fld))
         assert e <= tol, (fld, e)
@@ -362,7 +387,7 @@ def test_wall_pushback_steps(prec):
     # the run differs by more than the tolerance
     sp0 = cases.channel_disk(h=0.05, dt=0.01, zero_ids=(3, 4), wall_pushback=0)
     sp0.case.vel_tol, sp0.case.p_tol = 1e-13, 1e-12
-    g0 = Solver(sp0, precision=prec)
+    g0 = Solver(sp0, **solver_kw(prec))
     g0.seed_particles(sp0.q, seed=0, jitter=0.1)
     for _ in range(3):
         g0.step()

@@ -60,10 +60,13 @@ def test_clockwise_quads_are_reoriented(tmp_path):
     assert key(r) == key(m)
 
 
-REF_MESH = "/root/reference/cylinder2D/scaled3.unv"
+# the reference's own cylinder2D mesh, read where the reference tree is
+# checked out (PFEM2_REFERENCE_DIR); skipped without it
+REF_MESH = os.path.join(os.environ.get("PFEM2_REFERENCE_DIR", ""), "cylinder2D", "scaled3.unv")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_MESH), reason="the reference tree is not present")
+@pytest.mark.skipif(not os.environ.get("PFEM2_REFERENCE_DIR") or not os.path.exists(REF_MESH),
+                    reason="PFEM2_REFERENCE_DIR does not name the reference tree")
 def test_reference_cylinder_mesh():
     """the reference's cylinder2D mesh: 7050 quads, boundary groups 1-4
     (inlet, outlet, cylinder, walls) with 75, 75, 60 and 170 faces"""
@@ -77,7 +80,8 @@ def test_reference_cylinder_mesh():
         assert d1[0] * d2[1] - d1[1] * d2[0] > 0
 
 
-@pytest.mark.skipif(not os.path.exists(REF_MESH), reason="the reference tree is not present")
+@pytest.mark.skipif(not os.environ.get("PFEM2_REFERENCE_DIR") or not os.path.exists(REF_MESH),
+                    reason="PFEM2_REFERENCE_DIR does not name the reference tree")
 def test_reference_cylinder_case_runs_in_the_oracle():
     """the reference's cylinder2D case on its own mesh: three oracle steps
     give finite fields, a drag on the cylinder and the inlet velocity kept"""
@@ -122,7 +126,8 @@ def test_repair_drops_preamble_and_unlisted_elements(tmp_path):
     assert np.array_equal(a.face_bid, m.face_bid)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_MESH), reason="the reference tree is not present")
+@pytest.mark.skipif(not os.environ.get("PFEM2_REFERENCE_DIR") or not os.path.exists(REF_MESH),
+                    reason="PFEM2_REFERENCE_DIR does not name the reference tree")
 def test_repair_reference_mesh(tmp_path):
     q = tmp_path / "repaired.unv"
     kept, dropped = unv.repair_unv(REF_MESH, q)

@@ -33,17 +33,33 @@ def vertex_cells(mesh):
     return ptr, c[order].astype(np.int32), loc[order].astype(np.int32)
 
 
-def call_noalloc(lib, torch, mesh, particles):
+def wall_flags(mesh, bids):
+    """1 on the vertices of boundary faces with the given ids (the context's
+    zero_after_projection vertices): face f of a cell lies on axis f // 2 at
+    side f % 2, its vertices have that bit of their local index set to f % 2"""
+    flag = np.zeros(mesh.n_vertices, np.uint8)
+    nvc = mesh.cells.shape[1]
+    for f in range(mesh.face_bid.shape[1]):
+        on = np.isin(mesh.face_bid[:, f], bids)
+        for b in range(nvc):
+            if ((b >> (f // 2)) & 1) == f % 2:
+                flag[mesh.cells[on, b]] = 1
+    return flag
+
+
+def call_noalloc(lib, torch, mesh, particles, zero_flag=None, incidences=None):
     cell, xi, u = particles
     dim = mesh.dim
-    ptr, vc, vl = vertex_cells(mesh)
+    ptr, vc, vl = incidences if incidences is not None else vertex_cells(mesh)
     start = np.concatenate([[0], np.cumsum(np.bincount(cell, minlength=mesh.n_cells))]).astype(np.int32)
     dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()
     t = [dev(ptr), dev(vc), dev(vl), dev(start), dev(xi.astype(np.float64)), dev(u.astype(np.float64))]
+    zf = dev(zero_flag) if zero_flag is not None else None
     node_u = torch.full((mesh.n_vertices, dim), float("nan"), dtype=torch.float64, device="cuda")
     node_w = torch.full((mesh.n_vertices,), float("nan"), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     st = lib.pfem2_project_noalloc(dim, mesh.n_cells, mesh.n_vertices, *[C.c_void_p(x.data_ptr()) for x in t],
+                                   C.c_void_p(zf.data_ptr() if zf is not None else 0),
                                    C.c_void_p(node_u.data_ptr()), C.c_void_p(node_w.data_ptr()),
                                    C.c_void_p(stream.cuda_stream))
     assert st == A.OK, lib.pfem2_last_error().decode()
@@ -84,11 +100,62 @@ def test_noalloc_projection_matches_context_twice(dim):
     g.close()
 
 
+def test_noalloc_wall_vertices():
+    """a channel whose disk and walls are zeroed after the projection
+    (zero_after_projection_mask): with the same zero flags the entry point
+    equals the context's projection; without flags the wall vertices keep
+    their projected velocity"""
+    torch = pytest.importorskip("torch")
+    lib = load_library()
+    sp = cases.channel_disk(h=0.05, zero_ids=(3, 4))
+    g = Solver(sp, precision=A.PREC_FP64)
+    X = sp.mesh.vertices
+    g.set_field(A.FIELD_VX, 1.0 + 0.3 * np.sin(2.0 * X[:, 1]))
+    g.set_field(A.FIELD_VY, 0.2 * np.cos(1.5 * X[:, 0]))
+    g.seed_particles(sp.q, seed=4, jitter=0.1)
+    g.distribute_particle_velocities_to_grid()
+    ref_u = np.stack([g.field(A.FIELD_VX + d) for d in range(2)], axis=1)
+    ref_w = g.field(A.FIELD_NODE_WEIGHT)
+    flags = wall_flags(sp.mesh, (3, 4))
+    assert flags.sum() > 0
+    for _ in range(2):
+        nu, nw = call_noalloc(lib, torch, sp.mesh, g.particles(), zero_flag=flags)
+        assert rel(nw, ref_w) <= TOL
+        assert rel(nu, ref_u) <= TOL
+    nu, _ = call_noalloc(lib, torch, sp.mesh, g.particles())
+    wall = flags != 0
+    assert np.array_equal(nu[~wall], call_noalloc(lib, torch, sp.mesh, g.particles(), zero_flag=flags)[0][~wall])
+    assert np.abs(nu[wall]).max() > 0.1 and np.all(ref_u[wall] == 0.0)
+    g.close()
+
+
+def test_noalloc_out_of_range_incidence():
+    """an incidence naming a cell beyond n_cells makes that vertex NaN and
+    leaves the others exact"""
+    torch = pytest.importorskip("torch")
+    lib = load_library()
+    sp = cases.poiseuille_2d(nx=16, ny=6)
+    g = Solver(sp, precision=A.PREC_FP64)
+    g.set_field(A.FIELD_VX, np.ones(sp.mesh.n_vertices))
+    g.seed_particles((3, 3), seed=1, jitter=0.1)
+    parts = g.particles()
+    good_u, good_w = call_noalloc(lib, torch, sp.mesh, parts)
+    ptr, vc, vl = vertex_cells(sp.mesh)
+    v = 40
+    vc = vc.copy()
+    vc[ptr[v]] = sp.mesh.n_cells
+    bad_u, bad_w = call_noalloc(lib, torch, sp.mesh, parts, incidences=(ptr, vc, vl))
+    assert np.isnan(bad_w[v]) and np.all(np.isnan(bad_u[v]))
+    keep = np.arange(sp.mesh.n_vertices) != v
+    assert np.array_equal(bad_u[keep], good_u[keep]) and np.array_equal(bad_w[keep], good_w[keep])
+    g.close()
+
+
 def test_noalloc_rejects_too_many_cells():
     torch = pytest.importorskip("torch")
     lib = load_library()
     buf = torch.zeros(16, dtype=torch.float64, device="cuda")
     p = C.c_void_p(buf.data_ptr())
-    st = lib.pfem2_project_noalloc(2, 65536 + 1, 4, p, p, p, p, p, p, p, p, C.c_void_p(0))
+    st = lib.pfem2_project_noalloc(2, 65536 + 1, 4, p, p, p, p, p, p, C.c_void_p(0), p, p, C.c_void_p(0))
     assert st == A.INVALID_ARG
     assert b"PFEM2_NOALLOC_MAX_CELLS" in lib.pfem2_last_error()
