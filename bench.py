@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--h", type=float, default=0.0088, help="cell size of the channel mesh (~52k cells)")
-    ap.add_argument("--rtol", type=float, default=1e-10,
+    ap.add_argument("--rtol", type=float, default=1e-8,
                     help="relative tolerance |r| <= rtol |b| of every solve, both paths")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--ensemble-n", type=int, default=64, help="instances of the batched leg (0 = skip)")
     ap.add_argument("--pipe-n", type=int, default=64,
                     help="3D pipe leg: n x n x 4n hex cells, mixed and FP64 (0 = skip)")
-    ap.add_argument("--pipe-rtol", type=float, default=1e-13, help="relative tolerance of the pipe leg's solves")
+    ap.add_argument("--pipe-rtol", type=float, default=1e-11, help="relative tolerance of the pipe leg's solves")
     ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of the stress and ensemble legs")
     ap.add_argument("--only", default="all", choices=["all", "channel", "stress", "pipe", "ensemble", "budget"],
                     help="run one leg alone and print its JSON (for profilers); 'all' prints the bench line")

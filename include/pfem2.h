@@ -296,6 +296,31 @@ pfem2_status pfem2_solver_sizes(pfem2_ctx* ctx, int64_t* out);
 const char* pfem2_last_error(void);
 int32_t pfem2_abi_version(void);
 
+/* ---- launch shapes and their autotuning ----
+ * No counterpart in the reference (its kernels have fixed launch shapes).
+ * Each field 0 = automatic. None of them changes the particle kernels'
+ * arithmetic (their results are bitwise the same under every setting); the
+ * velocity tile size changes the order of the solver's partial sums and the
+ * pressure width its preconditioner, both within the solver tolerance. */
+typedef struct {
+  int32_t advect_blocks_per_sm;  /* advection grid in 256-thread blocks per SM (sets particles per block) */
+  int32_t advect_split;          /* 1: one advection kernel, 2: stayers then leavers in two kernels */
+  int32_t rebin_blocks_per_sm;   /* re-sort grid in 256-thread blocks per SM (tiles of 8 cells) */
+  int32_t vel_tile_slices;       /* velocity solves: SELL slices of 32 rows per Krylov tile */
+  int32_t p_blocks_per_sm;       /* pressure multigrid of a single system: 1 or 2 blocks per SM */
+  int32_t pad_;
+} pfem2_tuning;
+/* Sets the launch shapes (before pfem2_setup). Fields left at 0 are taken
+ * from the tuning cache named by the environment variable PFEM2_TUNING_CACHE
+ * (written by the autotuner, pfem2_b200/autotune.py) when it holds an entry
+ * for this context's key, else chosen by size. */
+pfem2_status pfem2_set_tuning(pfem2_ctx* ctx, const pfem2_tuning* t);
+/* The launch shapes in use (after pfem2_setup: every field resolved). */
+pfem2_status pfem2_get_tuning(pfem2_ctx* ctx, pfem2_tuning* t);
+/* The key of the tuning cache for this context (after pfem2_add_instance):
+ * "<device name> <dim> <fp32 stages, -1 for FP64> <log2 cells> <log2 instances>". */
+pfem2_status pfem2_tuning_key(pfem2_ctx* ctx, char* buf, int32_t len);
+
 /* ---- projection without allocation ----
  * No counterpart in the reference. For callers that cannot let the library
  * call cudaMalloc (a host code that owns all device memory through its own

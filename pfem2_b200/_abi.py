@@ -82,3 +82,15 @@ class Stats(C.Structure):
         ("iters", C.c_int32 * 7), ("residual", C.c_double * 7),
         ("refinements_p", C.c_int32), ("pad_", C.c_int32),
     ]
+
+
+class Tuning(C.Structure):
+    """pfem2_tuning: launch shapes (0 = automatic)"""
+    _fields_ = [
+        ("advect_blocks_per_sm", C.c_int32), ("advect_split", C.c_int32),
+        ("rebin_blocks_per_sm", C.c_int32), ("vel_tile_slices", C.c_int32),
+        ("p_blocks_per_sm", C.c_int32), ("pad_", C.c_int32),
+    ]
+
+
+TUNING_FIELDS = ["advect_blocks_per_sm", "advect_split", "rebin_blocks_per_sm", "vel_tile_slices", "p_blocks_per_sm"]

@@ -1,0 +1,120 @@
+"""Autotuner of the library's launch shapes (pfem2_tuning, include/pfem2.h).
+
+The particle kernels and the persistent Krylov solver have shapes that the
+best choice of depends on the GPU and the mesh size: the advection grid
+(particles per block) and whether advection runs as one kernel or as two
+(stayers, then leavers), the re-sort grid, the velocity solver's tile size
+(SELL slices per tile) and the blocks per SM of a single pressure system's
+multigrid solve. `tune` times whole steps (the device time of every stage,
+CUDA events inside the library) for candidate shapes by coordinate descent
+and appends the fastest to a cache file under the context's key: device
+name, dim, FP32 stages, log2 cells, log2 instances (pfem2_tuning_key). A
+later context with the same key reads the entry at pfem2_setup when the
+environment variable PFEM2_TUNING_CACHE names the file; fields the caller
+sets explicitly win over the cache.
+
+    from pfem2_b200 import autotune, cases
+    res = autotune.tune([cases.channel_disk()], cache="pfem2_tuning.txt")
+
+The particle shapes never change results (bitwise); the solver shapes change
+the order of partial sums (tile size) or the preconditioner (blocks per SM),
+within the solver tolerance.
+"""
+import os
+
+import numpy as np
+
+from . import _abi as A
+from .solver import Pfem2Error, Solver
+
+DEFAULT_SPACE = {
+    "advect_blocks_per_sm": [2, 4, 8, 16],
+    "advect_split": [1, 2],
+    "rebin_blocks_per_sm": [2, 4, 6, 8, 12],
+    "vel_tile_slices": [4, 8, 16, 32],
+    "p_blocks_per_sm": [1, 2],
+}
+
+
+def measure(specs, tuning, steps=5, warmup=2, seed_q=None, prepare=None, **solver_kw):
+    """median device time of a step (ms) with the given shapes, and the
+    shapes the context resolved; (None, None) if the context refuses them"""
+    try:
+        s = Solver(specs, tuning=tuning, use_graph=True, **solver_kw)
+    except Pfem2Error:
+        return None, None
+    try:
+        if prepare:
+            prepare(s)
+        sp = specs[0] if isinstance(specs, (list, tuple)) else specs
+        s.seed_particles(seed_q or sp.q, sp.seed, sp.jitter)
+        for _ in range(warmup):
+            s.step()
+        s.synchronize()
+        s.enable_stage_timing(True)
+        times = []
+        s.stage_times(reset=True)
+        for _ in range(steps):
+            s.step()
+            times.append(float(np.sum(s.stage_times(reset=True))))
+        resolved = s.tuning()
+        s.stats()  # raises on a failed step
+        return float(np.median(times)), resolved
+    except Pfem2Error:
+        return None, None
+    finally:
+        s.close()
+
+
+def cache_line(key, tuning, ms):
+    vals = " ".join(str(int(tuning[k])) for k in A.TUNING_FIELDS)
+    return f"{key} {vals} {ms:.4f}\n"
+
+
+def tune(specs, space=None, steps=5, warmup=2, cache=None, rounds=1, prepare=None, **solver_kw):
+    """Coordinate descent over `space` (knob -> candidate values) starting from
+    the automatic shapes. Returns {"key", "tuning", "ms_per_step",
+    "baseline_ms", "trials"}; with `cache` the best entry is appended there."""
+    space = DEFAULT_SPACE if space is None else space
+    t0, best = measure(specs, None, steps, warmup, prepare=prepare, **solver_kw)
+    if t0 is None:
+        raise RuntimeError("the automatic launch shapes failed")
+    probe = Solver(specs, use_graph=True, **solver_kw)
+    key = probe.tuning_key()
+    probe.close()
+    best = {k: v for k, v in best.items() if k in space or v}
+    best_t = t0
+    trials = [({k: best[k] for k in best}, t0)]
+    for _ in range(rounds):
+        for knob, values in space.items():
+            for v in values:
+                if best.get(knob) == v:
+                    continue
+                cand = dict(best, **{knob: v})
+                t, resolved = measure(specs, cand, steps, warmup, prepare=prepare, **solver_kw)
+                trials.append((cand, t))
+                if t is not None and t < best_t:
+                    best_t, best = t, {k: resolved[k] for k in best}
+    full = {k: int(best.get(k, 0)) for k in A.TUNING_FIELDS}
+    if cache:
+        with open(cache, "a") as f:
+            f.write(cache_line(key, full, best_t))
+    return {"key": key, "tuning": full, "ms_per_step": best_t, "baseline_ms": t0, "trials": trials}
+
+
+def read_cache(path):
+    """{key: (tuning dict, ms)} of a cache file, the last entry per key"""
+    out = {}
+    if not os.path.exists(path):
+        return out
+    for ln in open(path):
+        if ln.startswith("#") or not ln.strip():
+            continue
+        parts = ln.split()
+        if len(parts) < 10:
+            continue
+        key = " ".join(parts[:5])
+        vals = [int(x) for x in parts[5:10]]
+        ms = float(parts[10]) if len(parts) > 10 else None
+        out[key] = (dict(zip(A.TUNING_FIELDS, vals)), ms)
+    return out

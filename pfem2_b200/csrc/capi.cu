@@ -120,8 +120,79 @@ static pfem2_status upload_cell_geo(Ctx& c, const std::vector<double>& X, const 
   return PFEM2_OK;
 }
 
+// ------------------------------------------------------- launch shapes
+// key of the tuning cache: device name (spaces as '_'), dim, FP32 stages
+// (-1 for an FP64 context), floor(log2(cells)), floor(log2(instances))
+static std::string tuning_key(const Ctx& c) {
+  long long cells = 0;
+  for (const auto& in : c.inst) cells += in.nc;
+  int lc = 0, li = 0;
+  while ((2LL << lc) <= cells) ++lc;
+  while ((2LL << li) <= (long long)c.inst.size()) ++li;
+  const int stages = c.cfg.precision == PFEM2_PREC_FP64
+                         ? -1
+                         : (c.cfg.fp32_stages ? c.cfg.fp32_stages : PFEM2_FP32_DEFAULT);
+  std::string name = c.device_name;
+  for (char& ch : name)
+    if (ch == ' ' || ch == '\t') ch = '_';
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s %d %d %d %d", name.c_str(), c.dim, stages, lc, li);
+  return buf;
+}
+
+// The tuning cache (PFEM2_TUNING_CACHE): one entry per line,
+//   <device> <dim> <stages> <log2 cells> <log2 instances>
+//   <advect bps> <advect split> <rebin bps> <vel tile slices> <p bps> [ms per step]
+// '#' starts a comment; the last entry with this context's key wins. Its
+// values fill the fields the caller left at 0.
+static void apply_tuning_cache(Ctx& c) {
+  c.tune = c.tune_req;
+  c.tune_source = "caller";
+  const char* path = getenv("PFEM2_TUNING_CACHE");
+  if (!path || !*path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  const std::string key = tuning_key(c);
+  char line[512];
+  int best[5] = {0, 0, 0, 0, 0};
+  bool found = false;
+  while (fgets(line, sizeof(line), f)) {
+    if (line[0] == '#') continue;
+    char dev[256];
+    int dim, st, lc, li, v[5];
+    if (sscanf(line, "%255s %d %d %d %d %d %d %d %d %d", dev, &dim, &st, &lc, &li, &v[0], &v[1], &v[2], &v[3],
+               &v[4]) != 10)
+      continue;
+    char k[320];
+    snprintf(k, sizeof(k), "%s %d %d %d %d", dev, dim, st, lc, li);
+    if (key != k) continue;
+    std::copy(v, v + 5, best);
+    found = true;
+  }
+  fclose(f);
+  if (!found) return;
+  int32_t* dst[5] = {&c.tune.advect_blocks_per_sm, &c.tune.advect_split, &c.tune.rebin_blocks_per_sm,
+                     &c.tune.vel_tile_slices, &c.tune.p_blocks_per_sm};
+  for (int i = 0; i < 5; ++i)
+    if (*dst[i] == 0 && best[i] > 0) *dst[i] = best[i];
+  c.tune_source = "cache";
+}
+
+static pfem2_status check_tuning(const pfem2_tuning& t) {
+  if (t.advect_blocks_per_sm < 0 || t.advect_blocks_per_sm > 32 || t.advect_split < 0 || t.advect_split > 2 ||
+      t.rebin_blocks_per_sm < 0 || t.rebin_blocks_per_sm > 32 || t.vel_tile_slices < 0 || t.vel_tile_slices > 4096 ||
+      t.p_blocks_per_sm < 0 || t.p_blocks_per_sm > 2) {
+    set_error("tuning: a field is out of range");
+    return PFEM2_INVALID_ARG;
+  }
+  return PFEM2_OK;
+}
+
 // --------------------------------------------------------------- setup
 static pfem2_status do_setup(Ctx& c) {
+  apply_tuning_cache(c);
+  if (!c.tune.advect_blocks_per_sm) c.tune.advect_blocks_per_sm = 8;
+  if (!c.tune.rebin_blocks_per_sm) c.tune.rebin_blocks_per_sm = 8;
   const int dim = c.dim, NV = 1 << dim, NF = 2 * dim;
   // offsets
   int v = 0, cc = 0;
@@ -440,6 +511,7 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(dalloc(&c.far_keys, c.far_cap));
   PFEM2_TRY(dalloc(&c.barrier, 2));
   PFEM2_TRY(dalloc(&c.d_err, 1));
+  PFEM2_TRY(dalloc(&c.d_err_sticky, 1));
   PFEM2_TRY(dalloc(&c.loads_dev, 7 * c.inst.size()));
   PFEM2_CUDA(cudaMallocHost(&c.loads_host, sizeof(double) * 7 * c.inst.size()));
   c.list_cap = c.cfg.particles_per_cell_max > 0 ? c.cfg.particles_per_cell_max : (dim == 2 ? 512 : 1024);
@@ -471,7 +543,7 @@ static pfem2_status alloc_particles(Ctx& c, size_t seeded) {
   if (c.newcell) cudaFree(c.newcell);
   PFEM2_CUDA(cudaMalloc(&c.newcell, sizeof(int) * cap));
   // the advection queue: one region per warp of the fast kernel's grid
-  c.adv_grid = grid_for(c, (long long)cap, 256, 8);
+  c.adv_grid = grid_for(c, (long long)cap, 256, c.tune.advect_blocks_per_sm);
   if (c.adv_queue) cudaFree(c.adv_queue);
   if (c.adv_wcount) cudaFree(c.adv_wcount);
   if (c.adv_qstep) cudaFree(c.adv_qstep);
@@ -495,6 +567,9 @@ static pfem2_status check_counters(Ctx& c, bool sync) {
   c.stats.n_removed_last_check = cnt[CNT_REMOVED];
   c.stats.n_reseeded_last_check = cnt[CNT_RESEEDED];
   c.stats.n_far_movers_last_move = cnt[CNT_FAR];
+  // the error flags are read once: clear them for the passes to come
+  if (cnt[CNT_LIST_OVERFLOW] | cnt[CNT_CAP_OVERFLOW] | cnt[CNT_FAR_OVERFLOW] | cnt[CNT_SCAN_TIMEOUT])
+    PFEM2_CUDA(cudaMemset(c.d_counters + CNT_N_STATS, 0, sizeof(int) * (CNT_N - CNT_N_STATS)));
   if (cnt[CNT_LIST_OVERFLOW]) {
     set_error("rebin: more incoming particles than the per-cell capacity (particles_per_cell_max)");
     return PFEM2_PARTICLE_OVERFLOW;
@@ -663,6 +738,7 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   cudaDeviceProp prop;
   PFEM2_CUDA(cudaGetDeviceProperties(&prop, c.device));
   c.num_sms = prop.multiProcessorCount;
+  c.device_name = prop.name;
   if (const char* v = getenv("PFEM2_ADVECT_SPLIT_MIN")) c.adv_split_min = atoll(v);
   if (const char* v = getenv("PFEM2_MG_WIDE_MIN")) c.mg_wide_min = atoll(v);
   if (const char* v = getenv("PFEM2_SPIN_LIMIT")) c.spin_limit = (unsigned)std::min(atoll(v), (long long)c.spin_limit);
@@ -685,7 +761,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.wall_dv,
                   c.wall_cells, c.ring_rev, c.dest_mask, c.d_inst,
                   c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.rebin_tiles, c.d_np, c.d_counters,
-                  c.far_keys, c.barrier, c.d_err, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
+                  c.far_keys, c.barrier, c.d_err, c.d_err_sticky, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c.pmixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);
@@ -793,7 +869,7 @@ pfem2_status pfem2_advect(pfem2_ctx* x) {
 
 pfem2_status pfem2_check_empty(pfem2_ctx* x) {
   SEED_CHECK(x);
-  PFEM2_CUDA(cudaMemsetAsync(x->c.d_counters, 0, sizeof(int) * CNT_N, x->c.stream));
+  PFEM2_CUDA(cudaMemsetAsync(x->c.d_counters, 0, sizeof(int) * CNT_N_STATS, x->c.stream));
   PFEM2_TRY(launch_rebin(x->c, true, false, false));
   PFEM2_CUDA(cudaGetLastError());
   return check_counters(x->c, true);
@@ -1091,6 +1167,35 @@ pfem2_status pfem2_enable_stage_timing(pfem2_ctx* x, int32_t on) {
 pfem2_status pfem2_get_stream(pfem2_ctx* x, void** stream) {
   CTX_CHECK(x);
   if (stream) *stream = (void*)x->c.stream;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_set_tuning(pfem2_ctx* x, const pfem2_tuning* t) {
+  CTX_CHECK(x);
+  if (!t) { set_error("pfem2_set_tuning: null argument"); return PFEM2_INVALID_ARG; }
+  if (x->c.setup_done) { set_error("pfem2_set_tuning: call it before pfem2_setup"); return PFEM2_BAD_STATE; }
+  PFEM2_TRY(check_tuning(*t));
+  x->c.tune_req = *t;
+  x->c.tune_req.pad_ = 0;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_get_tuning(pfem2_ctx* x, pfem2_tuning* t) {
+  CTX_CHECK(x);
+  if (!t) { set_error("pfem2_get_tuning: null argument"); return PFEM2_INVALID_ARG; }
+  const Ctx& c = x->c;
+  *t = c.setup_done ? c.tune : c.tune_req;
+  if (c.setup_done && !t->advect_split) t->advect_split = (long long)c.pcap >= c.adv_split_min ? 2 : 1;
+  return PFEM2_OK;
+}
+
+pfem2_status pfem2_tuning_key(pfem2_ctx* x, char* buf, int32_t len) {
+  CTX_CHECK(x);
+  if (!buf || len <= 0) { set_error("pfem2_tuning_key: no buffer"); return PFEM2_INVALID_ARG; }
+  if (x->c.inst.empty()) { set_error("pfem2_tuning_key: no instances"); return PFEM2_BAD_STATE; }
+  const std::string k = tuning_key(x->c);
+  if ((int)k.size() >= len) { set_error("pfem2_tuning_key: buffer too small"); return PFEM2_INVALID_ARG; }
+  std::memcpy(buf, k.c_str(), k.size() + 1);
   return PFEM2_OK;
 }
 

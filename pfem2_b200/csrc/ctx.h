@@ -169,7 +169,8 @@ struct Ctx {
   double* tile_part = nullptr;
   int* d_sysinfo = nullptr;
   unsigned* barrier = nullptr;   // count, gen
-  int* d_err = nullptr;
+  int* d_err = nullptr;         // abort flag of the running solve (reset per launch)
+  int* d_err_sticky = nullptr;  // bits of the solves' exit codes since the host last read them
   // polls of a bounded device-side wait before it gives up (PFEM2_TIMEOUT);
   // the environment variable PFEM2_SPIN_LIMIT lowers it at creation (tests)
   unsigned spin_limit = 1u << 26;
@@ -185,6 +186,13 @@ struct Ctx {
   bool p_bicg = false;          // pressure solved by BiCGStab with Jacobi (else CG with multigrid)
   double refine_eta = 1e-3;     // mixed: inner residual reduction per FP64 refinement
 
+  // launch shapes: as set by the caller (0 = automatic) and as resolved at
+  // setup (caller, else the tuning cache, else by size)
+  pfem2_tuning tune_req{};
+  pfem2_tuning tune{};
+  std::string tune_source = "size";  // "caller", "cache" or "size" (per field: the first that set it)
+  std::string device_name;
+
   // graph
   cudaGraphExec_t graph = nullptr;
   bool graph_valid = false;
@@ -196,15 +204,20 @@ struct Ctx {
   pfem2_stats stats{};
 };
 
+// device counters of the particle passes: statistics of the last pass
+// (reset at every advection), then error flags that stay set until the
+// host reads them (check_counters), so that a failure inside a run of
+// graph-launched steps is still reported
 enum Counter {
   CNT_DELETED = 0,
   CNT_REMOVED = 1,
   CNT_RESEEDED = 2,
   CNT_FAR = 3,
-  CNT_LIST_OVERFLOW = 4,
-  CNT_CAP_OVERFLOW = 5,
-  CNT_FAR_OVERFLOW = 6,
-  CNT_ZERO_WEIGHT = 7,
+  CNT_ZERO_WEIGHT = 4,
+  CNT_N_STATS = 5,
+  CNT_LIST_OVERFLOW = 5,
+  CNT_CAP_OVERFLOW = 6,
+  CNT_FAR_OVERFLOW = 7,
   CNT_SCAN_TIMEOUT = 8,
   CNT_N = 9
 };

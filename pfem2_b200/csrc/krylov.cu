@@ -1299,6 +1299,9 @@ pfem2_status krylov_setup(Ctx& c) {
   // warps bring); a batch, or one system from mg_wide_min rows on (where the
   // solve is bound by memory parallelism, not by latency): two
   w->mg_minb = (c.inst.size() > 1 || (long long)c.nv >= c.mg_wide_min) ? 2 : 1;
+  // a single system below the wide size may be tuned to two blocks per SM
+  if (c.inst.size() == 1 && (long long)c.nv < c.mg_wide_min && c.tune.p_blocks_per_sm) w->mg_minb = c.tune.p_blocks_per_sm;
+  c.tune.p_blocks_per_sm = w->mg_minb;
   const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
   const int bps = std::max(1, c.solve_blocks_per_sm);
@@ -1329,7 +1332,8 @@ pfem2_status krylov_setup(Ctx& c) {
       const long long slices = (long long)c.nslices * ncomp;
       const long long target = 4LL * bps * c.num_sms;
       int ts = (int)std::max<long long>(8, (slices + target - 1) / target);
-      if (c.tile_slices > 0) ts = c.tile_slices;
+      if (c.tune.vel_tile_slices > 0) ts = c.tune.vel_tile_slices;
+      c.tune.vel_tile_slices = ts;
       for (int i = 0; i < ni; ++i) {
         const int sl0 = c.inst[i].v_off / kSlice, sl1 = (c.inst[i].v_off + c.inst[i].nv_pad) / kSlice;
         for (int a = sl0; a < sl1; a += ts)
@@ -1669,13 +1673,19 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   return PFEM2_OK;
 }
 
+// resets the solve's state; the previous solve's exit code (1 timeout,
+// 2 iteration cap) is kept as bit (1 << code) in *sticky until the host
+// reads it, so that the stats read after a whole step see every solve
 __global__ void k_init_solve(int nsys, int* __restrict__ active, unsigned* __restrict__ barrier,
-                             int* __restrict__ err, unsigned* __restrict__ scount, int ncount) {
+                             int* __restrict__ err, int* __restrict__ sticky, unsigned* __restrict__ scount,
+                             int ncount) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
     *active = nsys;
     barrier[0] = 0;
     barrier[1] = 0;
+    const int e = *err;
+    if (e > 0 && e < 8) *sticky |= 1 << e;
     *err = 0;
   }
   for (int j = i; j < ncount; j += gridDim.x * blockDim.x) scount[j] = 0u;
@@ -1778,7 +1788,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.gb.err = c.d_err;
   a.gb.spin_limit = c.spin_limit;
   k_init_solve<<<std::max(1, std::min(64, (32 * a.nsys + 255) / 256)), 256, 0, c.stream>>>(
-      a.nsys, w->active, c.barrier, c.d_err, w->scount, 32 * a.nsys);
+      a.nsys, w->active, c.barrier, c.d_err, c.d_err_sticky, w->scount, 32 * a.nsys);
   c.launches++;
   void* args[] = {&a};
   const void* kmg = w->mg_minb == 1 ? (const void*)k_krylov<R, true, 1> : (const void*)k_krylov<R, true, 2>;
@@ -1843,14 +1853,21 @@ pfem2_status krylov_read_stats(Ctx& c) {
     pfem2_status s = read_stats_phase(c, wch);
     if (s != PFEM2_OK && worst == PFEM2_OK) worst = s;
   }
-  int err = 0;
+  // the last solve's exit code and those of the solves before it
+  int err = 0, sticky = 0;
   PFEM2_CUDA(cudaMemcpy(&err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err == 1) {
+  PFEM2_CUDA(cudaMemcpy(&sticky, c.d_err_sticky, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err > 0 && err < 8) sticky |= 1 << err;
+  if (sticky) {
+    PFEM2_CUDA(cudaMemset(c.d_err_sticky, 0, sizeof(int)));
+    PFEM2_CUDA(cudaMemset(c.d_err, 0, sizeof(int)));
+  }
+  if (sticky & 2) {
     set_error("krylov: a wait for the other blocks timed out");
     c.failed = true;
     return PFEM2_TIMEOUT;
   }
-  if (err == 2) {
+  if (sticky & 4) {
     set_error("krylov: iteration cap reached");
     return PFEM2_NOT_CONVERGED;
   }

@@ -557,8 +557,9 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
   int b = c.cur;
   const int G = c.adv_grid;
   int S = c.cfg.movement_steps;
-  if ((long long)c.pcap < c.adv_split_min) {
-    const int grid = grid_for(c, c.pcap, 256, 8);
+  const bool split = c.tune.advect_split ? c.tune.advect_split == 2 : (long long)c.pcap >= c.adv_split_min;
+  if (!split) {
+    const int grid = grid_for(c, c.pcap, 256, c.tune.advect_blocks_per_sm);
     if (fuse)
       k_advect_one<DIM, R, true><<<grid, 256, 0, c.stream>>>(
           c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
@@ -596,7 +597,7 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
 }
 
 pfem2_status launch_advect(Ctx& c, bool fuse) {
-  PFEM2_CUDA(cudaMemsetAsync(c.d_counters, 0, sizeof(int) * CNT_N, c.stream));
+  PFEM2_CUDA(cudaMemsetAsync(c.d_counters, 0, sizeof(int) * CNT_N_STATS, c.stream));
   PFEM2_CUDA(cudaMemsetAsync(c.dest_mask, 0, sizeof(unsigned) * c.nc, c.stream));
   if (c.dim == 2) return c.pmixed ? advect_impl<2, float>(c, fuse) : advect_impl<2, double>(c, fuse);
   return c.pmixed ? advect_impl<3, float>(c, fuse) : advect_impl<3, double>(c, fuse);
@@ -1017,7 +1018,7 @@ static void rebin_launch(Ctx& c, const int* newcell) {
   const int o = c.cur, nb = 1 - c.cur;
   const size_t smem = (size_t)kRebinWarps * (c.list_cap + kMaxBuckets) * sizeof(int);
   const int ntiles = (c.nc + kRebinWarps - 1) / kRebinWarps;
-  const int grid = grid_for(c, (long long)c.nc * 32, kRebinWarps * 32, 8);
+  const int grid = grid_for(c, (long long)c.nc * 32, kRebinWarps * 32, c.tune.rebin_blocks_per_sm);
   cudaMemsetAsync(c.rebin_tiles, 0, sizeof(unsigned long long) * ((size_t)ntiles + 1), c.stream);
   k_rebin<DIM, R, CHECK, PROJ><<<grid, kRebinWarps * 32, smem, c.stream>>>(
       c.cell_start[o], newcell, (const R*)c.pxi[o], (const R*)c.pu[o], (size_t)c.pcap, c.pcell[nb], (R*)c.pxi[nb],

@@ -37,7 +37,7 @@ EXPORTS = [
     "pfem2_get_particles", "pfem2_set_particles", "pfem2_get_stats", "pfem2_get_time", "pfem2_synchronize",
     "pfem2_launch_count", "pfem2_stage_times", "pfem2_enable_stage_timing", "pfem2_get_stream",
     "pfem2_last_error", "pfem2_abi_version", "pfem2_project_noalloc", "pfem2_solver_sizes",
-    "pfem2_calculate_vorticity",
+    "pfem2_calculate_vorticity", "pfem2_set_tuning", "pfem2_get_tuning", "pfem2_tuning_key",
 ]
 
 
@@ -77,6 +77,9 @@ def load_library(path=LIB_PATH):
         "pfem2_calculate_vorticity": [vp],
         "pfem2_enable_stage_timing": [vp, C.c_int32],
         "pfem2_get_stream": [vp, C.POINTER(vp)],
+        "pfem2_set_tuning": [vp, C.POINTER(A.Tuning)],
+        "pfem2_get_tuning": [vp, C.POINTER(A.Tuning)],
+        "pfem2_tuning_key": [vp, C.c_char_p, C.c_int32],
     }
     sig["pfem2_project_noalloc"] = [C.c_int32, C.c_int32, C.c_int32] + [vp] * 9 + [vp]
     for name, args in sig.items():
@@ -103,7 +106,10 @@ class Solver:
 
     def __init__(self, specs, precision=A.PREC_MIXED, device=0, movement_steps=None, max_per_part=None,
                  use_graph=True, capacity_factor=2.0, per_cell_max=0, particles_only=False, fp32_stages=0,
-                 far_capacity=0):
+                 far_capacity=0, tuning=None):
+        """tuning: a dict of pfem2_tuning fields (launch shapes) set before
+        setup; unset or 0 fields come from the tuning cache named by
+        PFEM2_TUNING_CACHE, else from the sizes"""
         if not isinstance(specs, (list, tuple)):
             specs = [specs]
         self.L = load_library()
@@ -135,6 +141,11 @@ class Solver:
             mv = A.MeshView(m.n_vertices, m.n_cells, _dptr(X), _iptr(cv), _iptr(fb))
             inst = C.c_int32()
             self._check(self.L.pfem2_add_instance(self.h, C.byref(mv), C.byref(sp.case), C.byref(inst)))
+        if tuning:
+            t = A.Tuning()
+            for k, v in tuning.items():
+                setattr(t, k, int(v))
+            self._check(self.L.pfem2_set_tuning(self.h, C.byref(t)))
         self._check(self.L.pfem2_setup(self.h))
         self._keep = []
 
@@ -270,6 +281,18 @@ class Solver:
         if self.cfg.precision != A.PREC_MIXED:
             return 0
         return self.cfg.fp32_stages or A.FP32_DEFAULT
+
+    def tuning(self):
+        """the launch shapes in use (pfem2_get_tuning)"""
+        t = A.Tuning()
+        self._check(self.L.pfem2_get_tuning(self.h, C.byref(t)))
+        return {k: getattr(t, k) for k in A.TUNING_FIELDS}
+
+    def tuning_key(self):
+        """the key this context looks the tuning cache up with"""
+        buf = C.create_string_buffer(512)
+        self._check(self.L.pfem2_tuning_key(self.h, buf, 512))
+        return buf.value.decode()
 
     def enable_stage_timing(self, on=True):
         self._check(self.L.pfem2_enable_stage_timing(self.h, 1 if on else 0))

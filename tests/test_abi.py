@@ -20,11 +20,13 @@ STRUCTS = {
     "pfem2_case": (A.Case, ["mu", "rho", "dt", "n_dirichlet", "dirichlet", "open_boundary_mask",
                             "open_boundary_pressure_flux", "zero_after_projection_mask", "load_patch_id",
                             "probe_a", "probe_b", "outer_corrections", "load_diam", "load_umean", "vel_tol",
-                            "p_tol", "max_iter", "vel_solver", "p_solver", "reassemble_every_step"]),
+                            "p_tol", "max_iter", "vel_solver", "p_solver", "reassemble_every_step",
+                            "wall_pushback", "vel_rtol", "p_rtol"]),
     "pfem2_mesh_view": (A.MeshView, ["n_vertices", "n_cells", "vertices", "cells", "face_boundary_id"]),
     "pfem2_config": (A.Config, ["dim", "precision", "device", "movement_steps", "max_particles_per_cell_part",
                                 "particles_per_cell_max", "particle_capacity_factor", "far_mover_capacity",
-                                "use_graph", "particles_only"]),
+                                "use_graph", "particles_only", "fp32_stages"]),
+    "pfem2_tuning": (A.Tuning, A.TUNING_FIELDS),
     "pfem2_stats": (A.Stats, ["n_particles", "n_deleted_last_move", "n_removed_last_check",
                               "n_reseeded_last_check", "n_far_movers_last_move", "iters", "residual",
                               "refinements_p"]),

@@ -295,11 +295,11 @@ def test_particles_only_step(prec):
 def test_ensemble_batch_matches_oracle():
     """a batch of four uneven channel instances (2k-6k cells, different
     Reynolds numbers and radii) in one context: every instance equals the
-    oracle run of that instance alone (mixed path, solves to 1e-12 relative)"""
+    oracle run of that instance alone (mixed path, solves to 1e-11 relative)"""
     specs = cases.ensemble(n=4, cells_lo=2000, cells_hi=6000)
     for sp in specs:
         sp.case.vel_tol = sp.case.p_tol = 0.0
-        sp.case.vel_rtol = sp.case.p_rtol = 1e-12
+        sp.case.vel_rtol = sp.case.p_rtol = 1e-11
     assert len({sp.mesh.n_cells for sp in specs}) == 4
     s = Solver(specs, precision=A.PREC_MIXED)
     s.seed_particles(specs[0].q, 2, 0.0)
