@@ -339,7 +339,8 @@ def run_ours(args, rank, world, local):
                      "algorithmic_bytes_per_step": cgb / args.steps,
                      "bytes_model": "CG per row: SpMV 9 nnz x (4+4) + 12, 2 dots 16, 3 axpy 36, Jacobi 8 = 144 B "
                                     "x rows x live iterations, + FP64 refinements 136 B/row",
-                     "traffic": KRYLOV_TRAFFIC_PER_ITER * it_p / args.steps if KRYLOV_TRAFFIC_PER_ITER else None,
+                     "traffic": KRYLOV_TRAFFIC_PER_LAUNCH,
+                     "traffic_per_algorithmic_byte": KRYLOV_TRAFFIC_PER_LAUNCH / (cgb / args.steps) if cgb else None,
                      "traffic_source": KRYLOV_TRAFFIC_SOURCE,
                      "with_multigrid_operators": {"achieved": gbs(mgb), "frac": (gbs(mgb) / hbm) if gbs(mgb) else None,
                                                   "bytes_per_step": mgb / args.steps}},
@@ -363,11 +364,17 @@ def run_ours(args, rank, world, local):
         print(json.dumps(res), flush=True)
 
 
-# DRAM bytes (read + write) per CG iteration of the channel pressure solve,
-# from an ncu capture of one solve launch in the timed window of this bench
-# (None until captured)
-KRYLOV_TRAFFIC_PER_ITER = None
-KRYLOV_TRAFFIC_SOURCE = None
+# DRAM bytes (read + write) of one pressure-solve launch of the channel in
+# the timed window (steps 5 and 6 after 4 warm-up steps, 31 and 30 CG
+# iterations, rtol 1e-8): ncu dram__bytes_read.sum + dram__bytes_write.sum
+# of `bench.py --only channel --steps 3 --warmup 4`, mean of the two
+# launches. Under ncu every launch starts with a flushed L2, so this is one
+# cold read of the solve's working set, which then stays in L2: it does
+# not grow with the iteration count.
+KRYLOV_TRAFFIC_PER_LAUNCH = 0.5 * ((33015552 + 136448) + (33057024 + 7424))
+KRYLOV_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_krylov<float, MG> launches "
+                         "of steps 5-6 (31 and 30 iterations) of `bench.py --only channel --steps 3 --warmup 4`; "
+                         "per launch = per step")
 
 
 def speedups(value, cells, fp64, ensemble):
@@ -682,7 +689,7 @@ def ensemble_leg(args, rank, world, local, flush, fp64_single):
         "sharding": f"lpt over {world} ranks" if world > 1 else "one batch",
         "ms_per_batch_step": ms / args.extra_steps, "instance_timesteps_per_s": inst_steps,
         "cell_updates_per_s": cells * args.extra_steps / (ms / 1e3),
-        "max_pressure_cg_iters": st["iters"][3],
+        "max_pressure_cg_iters": st["iters"][3], "far_movers_last_step": st["far"],
     }
     s.close()
     return out

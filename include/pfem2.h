@@ -79,7 +79,10 @@ typedef enum {
   PFEM2_FIELD_PRED_VX = 8, PFEM2_FIELD_PRED_VY = 9, PFEM2_FIELD_PRED_VZ = 10,
   PFEM2_FIELD_NODE_WEIGHT = 11,  /* sum of shape values from the last projection */
   PFEM2_FIELD_VORTICITY = 12,    /* nodal vorticity from the last pfem2_calculate_vorticity (2D) */
-  PFEM2_N_FIELDS = 13
+  PFEM2_FIELD_DISP_X = 13,       /* mesh displacement of the last pfem2_mesh_elasticity */
+  PFEM2_FIELD_DISP_Y = 14,
+  PFEM2_FIELD_DISP_Z = 15,
+  PFEM2_N_FIELDS = 16
 } pfem2_field;
 
 typedef enum {
@@ -177,7 +180,7 @@ typedef struct {
   int32_t max_particles_per_cell_part; /* MAX_PARTICLES_PER_CELL_PART (pfem2particle.h:5) */
   int32_t particles_per_cell_max;  /* per-cell capacity of the rebin pass (0 = auto) */
   double particle_capacity_factor; /* particle storage = factor * seeded count (0 = 2.0) */
-  int32_t far_mover_capacity;      /* particles that leave the 1-ring of their cell in one step (0 = auto) */
+  int32_t far_mover_capacity;      /* particles that leave the 1-ring of their cell in one step (0 = 16384, the most) */
   int32_t use_graph;               /* capture pfem2_step as a CUDA graph */
   /* 1: no FEM (no matrices are set up; pfem2_fem_step is refused). pfem2_step
    * then runs correct -> move -> project on a frozen velocity field held in
@@ -187,6 +190,12 @@ typedef struct {
   /* PFEM2_PREC_MIXED only: the PFEM2_FP32_* stages that run in FP32
    * (0 = PFEM2_FP32_DEFAULT). Ignored by PFEM2_PREC_FP64. */
   int32_t fp32_stages;
+  /* 1: the mesh moves (pfem2_mesh_elasticity / pfem2_move_mesh, 2D, one
+   * instance): the matrices are reassembled every step and the pressure is
+   * solved without the multigrid hierarchy, which is built once on the host
+   * (CG with Jacobi, or BiCGStab with Jacobi as p_solver says). */
+  int32_t moving_mesh;
+  int32_t pad_;
 } pfem2_config;
 
 typedef struct pfem2_ctx pfem2_ctx;
@@ -256,10 +265,49 @@ pfem2_status pfem2_step_and_read(pfem2_ctx* ctx, double* loads_out,
                                  const int32_t* fields, int32_t n_fields,
                                  double* host_fields);
 
+/* ---- moving mesh (cylinderDyM) ----
+ * The reference's moving-mesh driver advances, per time step
+ * (cylinderDyM/cylinderDyM.cc:1146-1160): correct -> move -> distribute ->
+ * fem_step -> calculate_loads -> the body displacement from its motion ODE
+ * (the driver's own code) -> problem_of_elasticity -> reinterpolate_fields
+ * -> transform_grid -> sort_particles_into_subdomains_and_cells ->
+ * check_empty_cells. The two calls below replace the members from
+ * problem_of_elasticity on; they need pfem2_config.moving_mesh. */
+typedef struct {
+  double lambda, mu;     /* Lame parameters of the mesh's pseudo-solid */
+  uint32_t fixed_mask;   /* boundary ids (bit mask) held at zero displacement */
+  int32_t body_id;       /* boundary id displaced by body_disp (-1: none) */
+  double tol, rtol;      /* CG stops at |r| <= max(tol, rtol |b|) */
+  int32_t max_iter;
+  int32_t pad_;
+} pfem2_elasticity;
+/* problem_of_elasticity + solveU (cylinderDyM/cylinderDyM.cc:926-976,
+ * 886-903): the displacement of every vertex from the linear elasticity
+ * system sum_q [lambda d_ci N_a d_cj N_b + mu d_cj N_a d_ci N_b
+ * + delta_ci,cj mu grad N_a . grad N_b] JxW on the current mesh, u = 0 on
+ * fixed_mask, u = body_disp on body_id, solved by CG (Jacobi) into
+ * PFEM2_FIELD_DISP_X/Y; iterations and the final residual norm out
+ * (either may be NULL). NOT_CONVERGED past max_iter. */
+pfem2_status pfem2_mesh_elasticity(pfem2_ctx* ctx, int32_t instance, const pfem2_elasticity* e,
+                                   const double body_disp[3], int32_t* iterations, double* residual);
+/* reinterpolate_fields + transform_grid + sort_particles_into_subdomains_and_
+ * cells + check_empty_cells (cylinderDyM/pfem2particle.cpp:1144-1261): every
+ * interior vertex takes Vx, Vy, P interpolated at its displaced position in
+ * the old mesh (boundary vertices keep theirs), the vertices move by the
+ * displacement, every particle keeps its physical position and is located
+ * in the moved mesh (its cell, else the reference's vertex-patch search
+ * along the direction it moved relative to the mesh; deleted when found
+ * nowhere), then the empty sub-cells are refilled. PFEM2_MESH_ERROR if a
+ * cell turned inside out. */
+pfem2_status pfem2_move_mesh(pfem2_ctx* ctx);
+
 /* ---- state access (public data members of pfem2Solver) ---- */
 pfem2_status pfem2_get_field(pfem2_ctx* ctx, int32_t instance, int32_t field, double* host);
 pfem2_status pfem2_set_field(pfem2_ctx* ctx, int32_t instance, int32_t field, const double* host);
 pfem2_status pfem2_particle_count(pfem2_ctx* ctx, int32_t instance, int32_t* n);
+/* Vertex coordinates of an instance [n_vertices][dim] (they change with
+ * pfem2_move_mesh; the reference's Triangulation vertices). */
+pfem2_status pfem2_get_vertices(pfem2_ctx* ctx, int32_t instance, double* host);
 /* Particles of an instance in storage order (sorted by cell): local cell id,
  * reference coordinates [n][dim] and velocity [n][dim]. */
 pfem2_status pfem2_get_particles(pfem2_ctx* ctx, int32_t instance, int32_t* cell,

@@ -68,6 +68,12 @@ def _load():
     lib.or_boundary_measure.restype = C.c_double
     lib.or_rhs.argtypes = [vp, C.c_int, _dp]
     lib.or_get_dirichlet.argtypes = [vp, C.c_int, _bp, _dp]
+    lib.or_elasticity.argtypes = [vp, C.c_double, C.c_double, C.c_uint, C.c_int, _dp, C.c_double, C.c_double,
+                                  C.c_int, C.POINTER(C.c_double)]
+    lib.or_elasticity.restype = C.c_int
+    lib.or_reinterpolate.argtypes = [vp]
+    lib.or_transform_grid.argtypes = [vp]
+    lib.or_get_vertices.argtypes = [vp, _dp]
     return lib
 
 
@@ -142,6 +148,37 @@ class Oracle:
 
     def step(self, precond_p=1):
         return self.L.or_step(self.h, precond_p)
+
+    # moving mesh (cylinderDyM)
+    def problem_of_elasticity(self, lam, mu, fixed_ids, body_id, disp, tol=0.0, rtol=1e-12, max_iter=10000):
+        """mesh displacement into FIELD_DISP_*; returns (iterations, residual)"""
+        mask = 0
+        for b in fixed_ids:
+            mask |= 1 << b
+        d = np.zeros(3)
+        d[:len(disp)] = disp
+        res = C.c_double()
+        it = self.L.or_elasticity(self.h, lam, mu, mask, body_id, d, tol, rtol, max_iter, C.byref(res))
+        return it, res.value
+
+    def reinterpolate_fields(self):
+        self.L.or_reinterpolate(self.h)
+
+    def transform_grid(self):
+        """moves the mesh by FIELD_DISP_* and relocates the particles"""
+        self.L.or_transform_grid(self.h)
+
+    def move_mesh(self):
+        """reinterpolate_fields, transform_grid, sort_particles_into_subdomains_and_cells,
+        check_empty_cells (cylinderDyM/cylinderDyM.cc:1157-1160)"""
+        self.reinterpolate_fields()
+        self.transform_grid()
+        self.check_empty()
+
+    def vertices(self):
+        out = np.zeros(self.nv * self.dim)
+        self.L.or_get_vertices(self.h, out)
+        return out.reshape(self.nv, self.dim)
 
     # state
     def n_particles(self):

@@ -1269,6 +1269,247 @@ void or_loads(const omodel* m, int patch, double* out) {
   out[4] = dp;
 }
 
+/* ------------------------------------------------------------------ */
+/* Moving mesh (cylinderDyM)                                           */
+/* ------------------------------------------------------------------ */
+/* vertices on any boundary face (isBoundaryNode of
+ * initialize_moving_mesh_nodes, cylinderDyM/pfem2particle.cpp:1131-1136) */
+static unsigned char* boundary_vertices(const omodel* m) {
+  unsigned char* b = (unsigned char*)xcalloc(m->nv, 1);
+  for (int c = 0; c < m->nc; ++c)
+    for (int f = 0; f < m->nfc; ++f) {
+      if (m->fb[(size_t)c * m->nfc + f] < 0) continue;
+      for (int v = 0; v < m->nvc; ++v)
+        if (((v >> (f / 2)) & 1) == f % 2) b[m->cv[(size_t)c * m->nvc + v]] = 1;
+    }
+  return b;
+}
+
+/* direction vertex -> cell centre of every incidence (after the mesh moved) */
+static void update_v2c_dir(omodel* m) {
+  int dim = m->dim, nvc = m->nvc;
+  for (int v = 0; v < m->nv; ++v)
+    for (int k = m->v2c_ptr[v]; k < m->v2c_ptr[v + 1]; ++k) {
+      int c = m->v2c_cell[k];
+      double ctr[MAXD] = {0, 0, 0}, nn = 0.0;
+      for (int b = 0; b < nvc; ++b)
+        for (int a = 0; a < dim; ++a) ctr[a] += m->X[(size_t)m->cv[(size_t)c * nvc + b] * dim + a];
+      for (int a = 0; a < dim; ++a) {
+        ctr[a] = ctr[a] / nvc - m->X[(size_t)v * dim + a];
+        nn += ctr[a] * ctr[a];
+      }
+      nn = sqrt(nn);
+      for (int a = 0; a < dim; ++a) m->v2c_dir[(size_t)k * dim + a] = ctr[a] / nn;
+    }
+}
+
+/* problem_of_elasticity (cylinderDyM/cylinderDyM.cc:926-976) and solveU
+ * (:886-903): the mesh displacement u (dim components per vertex) from
+ *   a(u, v) = sum_q [ lambda d_ci N_a d_cj N_b + mu d_cj N_a d_ci N_b
+ *                     + delta_ci,cj mu grad N_a . grad N_b ] JxW,
+ * zero right-hand side, u = 0 on the boundary ids of fixed_mask and
+ * u = disp on body_id (both components), solved by CG to
+ * max(tol, rtol |b|) (the reference uses CG with an incomplete Cholesky
+ * preconditioner; Jacobi reaches the same solution). Into
+ * f[PFEM2_FIELD_DISP_X + d]. Returns the iteration count (-1: no convergence). */
+int or_elasticity(omodel* m, double lambda, double mu, unsigned fixed_mask, int body_id, const double* disp,
+                  double tol, double rtol, int maxit, double* res_out) {
+  const int dim = m->dim, nvc = m->nvc, nv = m->nv, nnz = m->nnz;
+  double* K[MAXD][MAXD];
+  for (int a = 0; a < dim; ++a)
+    for (int b = 0; b < dim; ++b) K[a][b] = (double*)xcalloc(nnz, sizeof(double));
+  qpoint qs[8];
+  for (int c = 0; c < m->nc; ++c) {
+    int nq = cell_qpoints(m, c, qs);
+    for (int iq = 0; iq < nq; ++iq) {
+      const qpoint* q = &qs[iq];
+      for (int ia = 0; ia < nvc; ++ia) {
+        const int va = m->cv[(size_t)c * nvc + ia];
+        const double* Ga = q->G + ia * dim;
+        for (int ib = 0; ib < nvc; ++ib) {
+          const int vb = m->cv[(size_t)c * nvc + ib];
+          const double* Gb = q->G + ib * dim;
+          const int slot = csr_slot(m, va, vb);
+          double gg = 0.0;
+          for (int d = 0; d < dim; ++d) gg += Ga[d] * Gb[d];
+          for (int ci = 0; ci < dim; ++ci)
+            for (int cj = 0; cj < dim; ++cj) {
+              double v = lambda * Ga[ci] * Gb[cj] + mu * Ga[cj] * Gb[ci];
+              if (ci == cj) v += mu * gg;
+              K[ci][cj][slot] += v * q->JxW;
+            }
+        }
+      }
+    }
+  }
+  /* constrained vertices and their values */
+  unsigned char* fix = (unsigned char*)xcalloc(nv, 1);
+  double* g = (double*)xcalloc((size_t)nv * dim, sizeof(double));
+  for (int c = 0; c < m->nc; ++c)
+    for (int f = 0; f < m->nfc; ++f) {
+      int bid = m->fb[(size_t)c * m->nfc + f];
+      if (bid < 0) continue;
+      int isfix = bid < 32 && ((fixed_mask >> bid) & 1u);
+      int isbody = bid == body_id;
+      if (!isfix && !isbody) continue;
+      for (int v = 0; v < nvc; ++v)
+        if (((v >> (f / 2)) & 1) == f % 2) {
+          int gv = m->cv[(size_t)c * nvc + v];
+          fix[gv] = 1;
+          for (int d = 0; d < dim; ++d) g[(size_t)gv * dim + d] = isbody ? disp[d] : 0.0;
+        }
+    }
+  /* symmetric elimination: constrained rows keep their diagonal, the
+   * columns of constrained vertices move to the right-hand side */
+  double* rhs = (double*)xcalloc((size_t)nv * dim, sizeof(double));
+  for (int i = 0; i < nv; ++i)
+    for (int k = m->rp[i]; k < m->rp[i + 1]; ++k) {
+      int j = m->ci[k];
+      for (int a = 0; a < dim; ++a)
+        for (int b = 0; b < dim; ++b) {
+          if (fix[i]) {
+            if (!(j == i && a == b)) K[a][b][k] = 0.0;
+          } else if (fix[j]) {
+            rhs[(size_t)i * dim + a] -= K[a][b][k] * g[(size_t)j * dim + b];
+            K[a][b][k] = 0.0;
+          }
+        }
+    }
+  for (int i = 0; i < nv; ++i)
+    if (fix[i])
+      for (int a = 0; a < dim; ++a) rhs[(size_t)i * dim + a] = K[a][a][m->diag[i]] * g[(size_t)i * dim + a];
+  /* CG with Jacobi on the block system (vertex-major vectors) */
+  const size_t n = (size_t)nv * dim;
+  double *x = (double*)xcalloc(n, sizeof(double)), *r = (double*)xcalloc(n, sizeof(double));
+  double *z = (double*)xcalloc(n, sizeof(double)), *p = (double*)xcalloc(n, sizeof(double));
+  double *qv = (double*)xcalloc(n, sizeof(double));
+  for (int i = 0; i < nv; ++i)
+    if (fix[i])
+      for (int a = 0; a < dim; ++a) x[(size_t)i * dim + a] = g[(size_t)i * dim + a];
+#define OR_KMUL(xx, yy)                                                       \
+  for (int i = 0; i < nv; ++i)                                                \
+    for (int a = 0; a < dim; ++a) {                                           \
+      double s_ = 0.0;                                                        \
+      for (int k = m->rp[i]; k < m->rp[i + 1]; ++k)                           \
+        for (int b = 0; b < dim; ++b) s_ += K[a][b][k] * (xx)[(size_t)m->ci[k] * dim + b]; \
+      (yy)[(size_t)i * dim + a] = s_;                                         \
+    }
+  OR_KMUL(x, qv);
+  for (size_t i = 0; i < n; ++i) r[i] = rhs[i] - qv[i];
+  double bn = sqrt(dot((int)n, rhs, rhs));
+  if (rtol * bn > tol) tol = rtol * bn;
+  double res = sqrt(dot((int)n, r, r));
+  int it = 0, ok = res <= tol;
+  if (!ok) {
+    for (int i = 0; i < nv; ++i)
+      for (int a = 0; a < dim; ++a) z[(size_t)i * dim + a] = r[(size_t)i * dim + a] / K[a][a][m->diag[i]];
+    memcpy(p, z, sizeof(double) * n);
+    double rho = dot((int)n, r, z);
+    for (it = 1; it <= maxit; ++it) {
+      OR_KMUL(p, qv);
+      double alpha = rho / dot((int)n, p, qv);
+      for (size_t i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * qv[i]; }
+      res = sqrt(dot((int)n, r, r));
+      if (res <= tol) { ok = 1; break; }
+      for (int i = 0; i < nv; ++i)
+        for (int a = 0; a < dim; ++a) z[(size_t)i * dim + a] = r[(size_t)i * dim + a] / K[a][a][m->diag[i]];
+      double rn = dot((int)n, r, z);
+      double beta = rn / rho;
+      rho = rn;
+      for (size_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    }
+  }
+#undef OR_KMUL
+  for (int d = 0; d < dim; ++d)
+    for (int i = 0; i < nv; ++i) m->f[PFEM2_FIELD_DISP_X + d][i] = x[(size_t)i * dim + d];
+  for (int a = 0; a < dim; ++a)
+    for (int b = 0; b < dim; ++b) free(K[a][b]);
+  free(fix); free(g); free(rhs); free(x); free(r); free(z); free(p); free(qv);
+  if (res_out) *res_out = res;
+  return ok ? it : -1;
+}
+
+/* is_inside_unit_cell(p, eps) */
+static int inside_unit_eps(int dim, const double* xi, double eps) {
+  for (int d = 0; d < dim; ++d)
+    if (!(xi[d] >= -eps && xi[d] <= 1.0 + eps)) return 0;
+  return 1;
+}
+
+/* reinterpolate_fields (cylinderDyM/pfem2particle.cpp:1144-1235): every
+ * interior vertex takes Vx, Vy(, Vz), P interpolated at its displaced
+ * position x + u in the old mesh, searched in the lowest-index cell around
+ * it first, then the other cells around it in ascending order (inside with
+ * tolerance 1e-5); boundary vertices and vertices found nowhere keep their
+ * values. A failed inverse map counts as "not inside" (the reference then
+ * tests the previous point, a quirk not reproduced). */
+void or_reinterpolate(omodel* m) {
+  const int dim = m->dim, nvc = m->nvc, nv = m->nv;
+  const int flds[4] = {PFEM2_FIELD_VX, PFEM2_FIELD_VY, dim == 3 ? PFEM2_FIELD_VZ : -1, PFEM2_FIELD_P};
+  unsigned char* bnd = boundary_vertices(m);
+  double* nw[4];
+  for (int k = 0; k < 4; ++k) {
+    nw[k] = (double*)xcalloc(nv, sizeof(double));
+    if (flds[k] >= 0) memcpy(nw[k], m->f[flds[k]], sizeof(double) * nv);
+  }
+  for (int v = 0; v < nv; ++v) {
+    if (bnd[v] || m->v2c_ptr[v + 1] == m->v2c_ptr[v]) continue;
+    double x[MAXD], xi[MAXD];
+    for (int d = 0; d < dim; ++d) x[d] = m->X[(size_t)v * dim + d] + m->f[PFEM2_FIELD_DISP_X + d][v];
+    int found = -1;
+    for (int k = m->v2c_ptr[v]; k < m->v2c_ptr[v + 1] && found < 0; ++k) {
+      int c = m->v2c_cell[k];
+      if (map_to_unit(m, c, x, xi) && inside_unit_eps(dim, xi, 1e-5)) found = c;
+    }
+    if (found < 0) continue;
+    double N[MAXV];
+    shape_values(dim, xi, N);
+    for (int k = 0; k < 4; ++k) {
+      if (flds[k] < 0) continue;
+      double s = 0.0;
+      for (int b = 0; b < nvc; ++b) s += N[b] * m->f[flds[k]][m->cv[(size_t)found * nvc + b]];
+      nw[k][v] = s;
+    }
+  }
+  for (int k = 0; k < 4; ++k) {
+    if (flds[k] >= 0) memcpy(m->f[flds[k]], nw[k], sizeof(double) * nv);
+    free(nw[k]);
+  }
+  free(bnd);
+}
+
+/* transform_grid (cylinderDyM/pfem2particle.cpp:1237-1261): every vertex
+ * moves by the displacement; then sort_particles_into_subdomains_and_cells
+ * (:280-...) on the moved mesh: a particle keeps its physical position, is
+ * tried in its cell, else searched in the cells around the cell's vertex
+ * closest along the direction it moved relative to the mesh (the reference
+ * uses the particle's last advection velocity there); particles found
+ * nowhere are deleted. The caller then runs check_empty_cells. */
+void or_transform_grid(omodel* m) {
+  const int dim = m->dim;
+  for (int v = 0; v < m->nv; ++v)
+    for (int d = 0; d < dim; ++d) m->X[(size_t)v * dim + d] += m->f[PFEM2_FIELD_DISP_X + d][v];
+  update_v2c_dir(m);
+  m->assembled = 0;  /* the matrices follow the mesh */
+  int deleted = 0;
+  for (int p = 0; p < m->np; ++p) {
+    int c = m->pc[p];
+    if (c < 0) continue;
+    double xo[MAXD], uext[MAXD], xi[MAXD];
+    const double* x = m->px + (size_t)p * dim;
+    map_to_real(m, c, m->pxi + (size_t)p * dim, xo);
+    for (int d = 0; d < dim; ++d) uext[d] = x[d] - xo[d];
+    int nc = locate(m, c, x, xo, uext, xi);
+    if (nc < 0) { m->pc[p] = -1; ++deleted; continue; }
+    m->pc[p] = nc;
+    for (int d = 0; d < dim; ++d) m->pxi[(size_t)p * dim + d] = xi[d];
+  }
+  m->n_deleted = deleted;
+  sort_by_cell(m);
+}
+
+void or_get_vertices(const omodel* m, double* X) { memcpy(X, m->X, sizeof(double) * m->nv * m->dim); }
+
 /* one run() iteration: correct -> move -> distribute -> fem -> time advance */
 int or_step(omodel* m, int precond_p) {
   or_correct(m);

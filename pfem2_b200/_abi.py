@@ -21,8 +21,9 @@ FP32_ALL = FP32_PARTICLES | FP32_ASSEMBLY | FP32_KRYLOV | FP32_PRESSURE_RHS
 FP32_DEFAULT = FP32_KRYLOV
 
 (FIELD_VX, FIELD_VY, FIELD_VZ, FIELD_P, FIELD_OLD_VX, FIELD_OLD_VY, FIELD_OLD_VZ, FIELD_OLD_P,
- FIELD_PRED_VX, FIELD_PRED_VY, FIELD_PRED_VZ, FIELD_NODE_WEIGHT, FIELD_VORTICITY) = range(13)
-N_FIELDS = 13
+ FIELD_PRED_VX, FIELD_PRED_VY, FIELD_PRED_VZ, FIELD_NODE_WEIGHT, FIELD_VORTICITY,
+ FIELD_DISP_X, FIELD_DISP_Y, FIELD_DISP_Z) = range(16)
+N_FIELDS = 16
 ABI_VERSION = 3  # PFEM2_ABI_VERSION of include/pfem2.h
 
 BC_CONSTANT, BC_PARABOLA = 0, 1
@@ -71,6 +72,7 @@ class Config(C.Structure):
         ("particle_capacity_factor", C.c_double),
         ("far_mover_capacity", C.c_int32), ("use_graph", C.c_int32),
         ("particles_only", C.c_int32), ("fp32_stages", C.c_int32),
+        ("moving_mesh", C.c_int32), ("pad_", C.c_int32),
     ]
 
 
@@ -94,3 +96,11 @@ class Tuning(C.Structure):
 
 
 TUNING_FIELDS = ["advect_blocks_per_sm", "advect_split", "rebin_blocks_per_sm", "vel_tile_slices", "p_blocks_per_sm"]
+
+
+class Elasticity(C.Structure):
+    """pfem2_elasticity: the mesh's pseudo-solid and its CG controls"""
+    _fields_ = [
+        ("lam", C.c_double), ("mu", C.c_double), ("fixed_mask", C.c_uint32), ("body_id", C.c_int32),
+        ("tol", C.c_double), ("rtol", C.c_double), ("max_iter", C.c_int32), ("pad_", C.c_int32),
+    ]

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libpfem2b.so")
-SOURCES = ["capi.cu", "particles.cu", "fem.cu", "krylov.cu", "amg.cu", "project_noalloc.cu"]
+SOURCES = ["capi.cu", "particles.cu", "fem.cu", "krylov.cu", "amg.cu", "ale.cu", "project_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + [

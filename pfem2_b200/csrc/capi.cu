@@ -387,6 +387,16 @@ static pfem2_status do_setup(Ctx& c) {
   c.vel_bicg = c.inst[0].cs.vel_solver == PFEM2_SOLVER_BICGSTAB;
   c.p_bicg = c.inst[0].cs.p_solver == PFEM2_SOLVER_BICGSTAB;
   if (c.p_bicg) c.two_level = false;
+  if (c.moving) {
+    // the matrices follow the mesh: reassembled every step; the multigrid
+    // hierarchy (built once on the host) is not used
+    if (c.inst.size() != 1 || c.dim != 2 || c.cfg.particles_only) {
+      set_error("moving_mesh: one 2D instance with the FEM");
+      return PFEM2_INVALID_ARG;
+    }
+    c.two_level = false;
+    c.inst[0].cs.reassemble_every_step = 1;
+  }
   // instance table
   c.h_inst.resize(c.inst.size());
   std::vector<double> tols(4 * c.inst.size());
@@ -507,7 +517,9 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(dalloc(&c.rebin_tiles, (size_t)nc / 8 + 2));
   PFEM2_TRY(dalloc(&c.d_np, 2));
   PFEM2_TRY(dalloc(&c.d_counters, CNT_N));
-  c.far_cap = c.cfg.far_mover_capacity > 0 ? std::min(c.cfg.far_mover_capacity, 4096) : 4096;
+  // far movers are sorted by one CTA in shared memory (8 B per key)
+  c.far_cap = c.cfg.far_mover_capacity > 0 ? std::min(c.cfg.far_mover_capacity, kFarMax) : kFarMax;
+  PFEM2_TRY(far_sort_setup(c));
   PFEM2_TRY(dalloc(&c.far_keys, c.far_cap));
   PFEM2_TRY(dalloc(&c.barrier, 2));
   PFEM2_TRY(dalloc(&c.d_err, 1));
@@ -515,6 +527,7 @@ static pfem2_status do_setup(Ctx& c) {
   PFEM2_TRY(dalloc(&c.loads_dev, 7 * c.inst.size()));
   PFEM2_CUDA(cudaMallocHost(&c.loads_host, sizeof(double) * 7 * c.inst.size()));
   c.list_cap = c.cfg.particles_per_cell_max > 0 ? c.cfg.particles_per_cell_max : (dim == 2 ? 512 : 1024);
+  if (c.moving) PFEM2_TRY(ale_setup(c));
   if (!c.cfg.particles_only) {
     PFEM2_TRY(krylov_setup(c));
     PFEM2_TRY(assemble_matrices(c));
@@ -739,6 +752,7 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   PFEM2_CUDA(cudaGetDeviceProperties(&prop, c.device));
   c.num_sms = prop.multiProcessorCount;
   c.device_name = prop.name;
+  c.moving = cfg->moving_mesh != 0;
   if (const char* v = getenv("PFEM2_ADVECT_SPLIT_MIN")) c.adv_split_min = atoll(v);
   if (const char* v = getenv("PFEM2_MG_WIDE_MIN")) c.mg_wide_min = atoll(v);
   if (const char* v = getenv("PFEM2_SPIN_LIMIT")) c.spin_limit = (unsigned)std::min(atoll(v), (long long)c.spin_limit);
@@ -756,6 +770,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
   for (int k = 0; k < 2; ++k)
     if (x->graph[k]) cudaGraphExecDestroy(x->graph[k]);
   krylov_free(c);
+  ale_free(c);
   // device memory is released with the context's allocations; free the big ones
   void* ptrs[] = {c.cell_geo, c.X, c.cv, c.fb, c.cell_inst, c.vert_inst, c.v2c_ptr, c.v2c_cell, c.v2c_loc, c.v2c_dir,
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.wall_dv,
@@ -1069,6 +1084,16 @@ pfem2_status pfem2_set_field(pfem2_ctx* x, int32_t instance, int32_t field, cons
   return PFEM2_OK;
 }
 
+pfem2_status pfem2_get_vertices(pfem2_ctx* x, int32_t instance, double* host) {
+  SETUP_CHECK(x);
+  Ctx& c = x->c;
+  if (instance < 0 || instance >= (int)c.inst.size() || !host) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
+  PFEM2_CUDA(cudaMemcpyAsync(host, c.X + (size_t)c.inst[instance].v_off * c.dim,
+                             sizeof(double) * c.dim * c.inst[instance].nv, cudaMemcpyDeviceToHost, c.stream));
+  PFEM2_CUDA(cudaStreamSynchronize(c.stream));
+  return PFEM2_OK;
+}
+
 pfem2_status pfem2_particle_count(pfem2_ctx* x, int32_t instance, int32_t* n) {
   SEED_CHECK(x);
   if (!n || instance < 0 || instance >= (int)x->c.inst.size()) { set_error("bad argument"); return PFEM2_INVALID_ARG; }
@@ -1168,6 +1193,41 @@ pfem2_status pfem2_get_stream(pfem2_ctx* x, void** stream) {
   CTX_CHECK(x);
   if (stream) *stream = (void*)x->c.stream;
   return PFEM2_OK;
+}
+
+pfem2_status pfem2_mesh_elasticity(pfem2_ctx* x, int32_t instance, const pfem2_elasticity* e,
+                                   const double body_disp[3], int32_t* iterations, double* residual) {
+  SETUP_CHECK(x);
+  LIVE_CHECK(x);
+  Ctx& c = x->c;
+  if (!c.moving) { set_error("pfem2_mesh_elasticity: the context was not created with moving_mesh"); return PFEM2_BAD_STATE; }
+  if (instance != 0 || !e || !body_disp) { set_error("pfem2_mesh_elasticity: bad argument"); return PFEM2_INVALID_ARG; }
+  if (!(e->lambda >= 0.0) || !(e->mu > 0.0) || !(e->tol >= 0.0) || !(e->rtol >= 0.0) ||
+      !(e->tol > 0.0 || e->rtol > 0.0)) {
+    set_error("pfem2_mesh_elasticity: lambda >= 0, mu > 0 and a positive tolerance needed");
+    return PFEM2_INVALID_ARG;
+  }
+  for (int d = 0; d < c.dim; ++d)
+    if (!std::isfinite(body_disp[d])) { set_error("pfem2_mesh_elasticity: body_disp not finite"); return PFEM2_INVALID_ARG; }
+  PFEM2_CUDA(cudaSetDevice(c.device));
+  int it = 0;
+  double res = 0.0;
+  const pfem2_status st = ale_elasticity(c, *e, body_disp, &it, &res);
+  if (iterations) *iterations = it;
+  if (residual) *residual = res;
+  return st;
+}
+
+pfem2_status pfem2_move_mesh(pfem2_ctx* x) {
+  SETUP_CHECK(x);
+  LIVE_CHECK(x);
+  Ctx& c = x->c;
+  if (!c.moving) { set_error("pfem2_move_mesh: the context was not created with moving_mesh"); return PFEM2_BAD_STATE; }
+  PFEM2_CUDA(cudaSetDevice(c.device));
+  PFEM2_TRY(ale_move_mesh(c));
+  // the graphs hold kernels of the old particle capacity only: geometry is
+  // read from device memory, so they stay valid
+  return c.seeded ? check_counters(c, true) : PFEM2_OK;
 }
 
 pfem2_status pfem2_set_tuning(pfem2_ctx* x, const pfem2_tuning* t) {

@@ -15,6 +15,7 @@ constexpr int kSlice = 32;          // SELL slice height (rows per warp)
 constexpr int kMaxPatch = 32;       // max cells around a vertex
 constexpr int kMaxRing = 64;        // max cells sharing a vertex with a cell
 constexpr int kNumSys = 7;          // pred x,y,z, pressure, mass x,y,z
+constexpr int kFarMax = 16384;      // far-mover list capacity (sorted in 128 KB of shared memory)
 
 // Per-instance parameters visible to kernels.
 struct DevInst {
@@ -186,6 +187,28 @@ struct Ctx {
   bool p_bicg = false;          // pressure solved by BiCGStab with Jacobi (else CG with multigrid)
   double refine_eta = 1e-3;     // mixed: inner residual reduction per FP64 refinement
 
+  // moving mesh (pfem2_config.moving_mesh): boundary vertices, the
+  // elasticity blocks K[a * dim + b] on the SELL pattern, constraint table,
+  // right-hand side / inverse diagonal ([dim][nv]), CG vectors, particle
+  // positions before a move ([dim][pcap] FP64), reinterpolated fields, and
+  // the device status word of the mesh kernels (1: a cell turned inside out)
+  bool moving = false;
+  unsigned char* ale_bnd = nullptr;
+  double* ale_K[9] = {};
+  unsigned char* ale_fix = nullptr;
+  double* ale_g = nullptr;
+  double* ale_rhs = nullptr;
+  double* ale_dinv = nullptr;
+  double* ale_vec = nullptr;   // x, r, z, q, p[2]: 6 [dim][nv] blocks
+  double* ale_part = nullptr;  // [2][grid][4] partial sums of the CG
+  int* ale_out = nullptr;      // [2] iterations, converged; ale_res: residual and tolerance
+  double* ale_res = nullptr;
+  double* ale_xphys = nullptr;
+  size_t ale_xphys_cap = 0;
+  double* ale_new = nullptr;   // [4][nv]
+  int* ale_flag = nullptr;
+  int ale_grid = 0;
+
   // launch shapes: as set by the caller (0 = automatic) and as resolved at
   // setup (caller, else the tuning cache, else by size)
   pfem2_tuning tune_req{};
@@ -264,6 +287,17 @@ pfem2_status launch_finish_fem(Ctx& c);
 pfem2_status launch_restore_frozen(Ctx& c);
 pfem2_status launch_loads(Ctx& c, int instance, int patch, double* out_dev);
 pfem2_status launch_vorticity(Ctx& c);
+
+// ale.cu (moving mesh)
+pfem2_status ale_setup(Ctx& c);
+pfem2_status ale_elasticity(Ctx& c, const pfem2_elasticity& e, const double* body_disp, int* iters, double* res);
+pfem2_status ale_move_mesh(Ctx& c);
+void ale_free(Ctx& c);
+// particles.cu: positions before the mesh moves, relocation after it
+pfem2_status launch_particle_positions(Ctx& c, double* xphys);
+pfem2_status launch_relocate(Ctx& c, const double* xphys);
+pfem2_status launch_cell_geo(Ctx& c, int* flag);
+pfem2_status far_sort_setup(Ctx& c);
 
 // krylov.cu
 pfem2_status krylov_setup(Ctx& c);

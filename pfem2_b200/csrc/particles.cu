@@ -202,63 +202,24 @@ constexpr int kAdvWarps = 8;  // warps per block of the advection kernels (256 t
 
 constexpr int kAdvLeft = -2;  // advect_steps<.., false>: the particle left its cell
 
-// Sub-steps s0 .. S-1 of the S forward-Euler sub-steps of one particle with
-// the Q1-interpolated mesh velocity (move_particles,
-// TurekBenchmark/pfem2particle.cpp:813-856), starting in cell c0 at
-// reference coordinates x (updated). After a sub-step
-// the point is first tried in the current cell; if it left, FULL runs the
-// reference's search (sort_particles_into_subdomains_and_cells: the vertex
-// of the old cell best aligned with the velocity, then that vertex's cells
-// ordered by alignment with the directions to their centres, :276-507) and
-// returns the new cell, or -1 when no cell of the patch contains the point
-// (the particle is deleted); without FULL it returns kAdvLeft at the first
-// sub-step that leaves the cell, with x still at the start of that
-// sub-step and its index in s_left. Otherwise it returns the cell.
-template <int DIM, typename R, bool FULL>
-__device__ __forceinline__ int advect_steps(int c0, R* x, R dts, int s0, int& s_left, int S,
+// The reference's search for a point xn (cell-local frame of cell c, whose
+// record is G / L / x0) that left cell c (sort_particles_into_subdomains_and_
+// cells, TurekBenchmark/pfem2particle.cpp:276-507): the vertex of c best
+// aligned with the direction uf from the old position xo
+// (find_closest_vertex_of_cell, :142-166), then that vertex's cells ordered
+// by the alignment of their centre directions with vertex -> point
+// (compare_particle_association, :268-274), the first that contains the
+// point. On success c, G, L, x0 and the reference coordinates x are those of
+// the new cell; false when no cell of the patch contains the point.
+template <int DIM, typename R>
+__device__ __forceinline__ bool locate_from(int& c, CellGeo<DIM, R>& G, LocalCell<DIM, R>& L, double* x0,
+                                            const R* xo, const R* xn, const R* uf, R* x, const int* gvx,
                                             const CellGeo<DIM, R>* __restrict__ geo,
-                                            const int* __restrict__ cv, const R* __restrict__ Vr, int nv,
                                             const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
                                             const R* __restrict__ v2c_dir) {
   constexpr int NV = Dims<DIM>::NV;
-  int c = c0;
-  // vertex ids and velocities of the current cell, reloaded only when the
-  // particle changes cell
-  int gvx[NV];
-  R vv[NV][DIM], N[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
-#pragma unroll
-  for (int v = 0; v < NV; ++v)
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
-  CellGeo<DIM, R> G = geo[c];
-  LocalCell<DIM, R> L;
-  double x0[DIM];
-  geo_to_local<DIM, R>(G, L, x0);
-  for (int s = s0; s < S; ++s) {
-    shape_values<DIM, R>(x, N);
-    R uf[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) uf[d] = R(0);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * vv[v][d];
-    }
-    R xo[DIM], xn[DIM], x2[DIM];
-    local_map<DIM, R>(L, x, xo);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) xn[d] = xo[d] + uf[d] * dts;
-    if (geo_inverse<DIM, R>(G, L, xn, x2) && inside_unit<DIM, R>(x2)) {
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) x[d] = x2[d];
-      continue;
-    }
-    if (!FULL) {
-      s_left = s;
-      return kAdvLeft;
-    }
+  R x2[DIM];
+  {
     // closest vertex of the old cell seen along the velocity
     R un = R(0);
 #pragma unroll
@@ -331,7 +292,68 @@ __device__ __forceinline__ int advect_steps(int c0, R* x, R dts, int s0, int& s_
         }
       }
     }
-    if (!found) return -1;
+    return found;
+  }
+}
+
+// Sub-steps s0 .. S-1 of the S forward-Euler sub-steps of one particle with
+// the Q1-interpolated mesh velocity (move_particles,
+// TurekBenchmark/pfem2particle.cpp:813-856), starting in cell c0 at
+// reference coordinates x (updated). After a sub-step
+// the point is first tried in the current cell; if it left, FULL runs the
+// reference's search (sort_particles_into_subdomains_and_cells: the vertex
+// of the old cell best aligned with the velocity, then that vertex's cells
+// ordered by alignment with the directions to their centres, :276-507) and
+// returns the new cell, or -1 when no cell of the patch contains the point
+// (the particle is deleted); without FULL it returns kAdvLeft at the first
+// sub-step that leaves the cell, with x still at the start of that
+// sub-step and its index in s_left. Otherwise it returns the cell.
+template <int DIM, typename R, bool FULL>
+__device__ __forceinline__ int advect_steps(int c0, R* x, R dts, int s0, int& s_left, int S,
+                                            const CellGeo<DIM, R>* __restrict__ geo,
+                                            const int* __restrict__ cv, const R* __restrict__ Vr, int nv,
+                                            const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
+                                            const R* __restrict__ v2c_dir) {
+  constexpr int NV = Dims<DIM>::NV;
+  int c = c0;
+  // vertex ids and velocities of the current cell, reloaded only when the
+  // particle changes cell
+  int gvx[NV];
+  R vv[NV][DIM], N[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
+  CellGeo<DIM, R> G = geo[c];
+  LocalCell<DIM, R> L;
+  double x0[DIM];
+  geo_to_local<DIM, R>(G, L, x0);
+  for (int s = s0; s < S; ++s) {
+    shape_values<DIM, R>(x, N);
+    R uf[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) uf[d] = R(0);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) uf[d] = uf[d] + N[v] * vv[v][d];
+    }
+    R xo[DIM], xn[DIM], x2[DIM];
+    local_map<DIM, R>(L, x, xo);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xn[d] = xo[d] + uf[d] * dts;
+    if (geo_inverse<DIM, R>(G, L, xn, x2) && inside_unit<DIM, R>(x2)) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) x[d] = x2[d];
+      continue;
+    }
+    if (!FULL) {
+      s_left = s;
+      return kAdvLeft;
+    }
+    if (!locate_from<DIM, R>(c, G, L, x0, xo, xn, uf, x, gvx, geo, v2c_ptr, v2c_cell, v2c_dir)) return -1;
 #pragma unroll
     for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c * NV + v);
 #pragma unroll
@@ -527,6 +549,184 @@ __global__ void __launch_bounds__(256, (DIM == 2 && sizeof(R) == 4) ? 4 : 1) k_a
   }
 }
 
+__global__ void k_far_sort(unsigned long long* keys, const int* __restrict__ counters, int cap);
+
+// ------------------------------------------------------------ moving mesh
+// physical position of every particle (FP64) from its cell record, before
+// the mesh moves
+template <int DIM, typename R>
+__global__ void k_particle_positions(const int* __restrict__ cell, const R* __restrict__ xi, size_t cap,
+                                     const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo,
+                                     double* __restrict__ out) {
+  const int n = min(*d_np, (int)cap);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const CellGeo<DIM, R> G = geo[cell[p]];
+    LocalCell<DIM, R> L;
+    double x0[DIM];
+    geo_to_local<DIM, R>(G, L, x0);
+    R x[DIM], xl[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) x[d] = xi[d * cap + p];
+    local_map<DIM, R>(L, x, xl);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) out[d * cap + p] = x0[d] + (double)xl[d];
+  }
+}
+
+// sort_particles_into_subdomains_and_cells after transform_grid: every
+// particle keeps its physical position xphys and is located in the moved
+// mesh: its cell first, else the reference's vertex-patch search from its
+// cell along the direction it moved relative to the mesh (from where its
+// old reference coordinates now map to); the new cell (-1: deleted) goes
+// to newcell with the moves recorded for the re-sort like the advection's
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_relocate(
+    const int* __restrict__ cell, R* __restrict__ xi, int* __restrict__ newcell, size_t cap,
+    const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
+    const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell, const R* __restrict__ v2c_dir,
+    const double* __restrict__ xphys, const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell,
+    unsigned long long* __restrict__ far_keys, int far_cap, int* __restrict__ counters,
+    unsigned* __restrict__ dest_mask) {
+  constexpr int NV = Dims<DIM>::NV;
+  const int n = min(*d_np, (int)cap);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int c0 = cell[p];
+    int c = c0;
+    CellGeo<DIM, R> G = geo[c0];
+    LocalCell<DIM, R> L;
+    double x0[DIM];
+    geo_to_local<DIM, R>(G, L, x0);
+    R x[DIM], xo[DIM], xn[DIM], uf[DIM], x2[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) x[d] = xi[d * cap + p];
+    local_map<DIM, R>(L, x, xo);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      xn[d] = R(xphys[d * cap + p] - x0[d]);
+      uf[d] = xn[d] - xo[d];
+    }
+    if (geo_inverse<DIM, R>(G, L, xn, x2) && inside_unit<DIM, R>(x2)) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) x[d] = x2[d];
+    } else {
+      int gvx[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) gvx[v] = __ldg(cv + (size_t)c0 * NV + v);
+      if (!locate_from<DIM, R>(c, G, L, x0, xo, xn, uf, x, gvx, geo, v2c_ptr, v2c_cell, v2c_dir)) c = -1;
+    }
+    advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters, dest_mask);
+    newcell[p] = c;
+    if (c >= 0)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
+  }
+}
+
+// per-cell records of the particle kernels rebuilt from the vertices on the
+// device (the same arithmetic as at setup); *flag = 1 if a cell has a
+// non-positive Jacobian at its centre
+template <int DIM, typename R>
+__global__ void k_cell_geo(int nc, const double* __restrict__ X, const int* __restrict__ cv,
+                           CellGeo<DIM, R>* __restrict__ geo, int* __restrict__ flag) {
+  constexpr int NV = Dims<DIM>::NV;
+  for (int ce = blockIdx.x * blockDim.x + threadIdx.x; ce < nc; ce += gridDim.x * blockDim.x) {
+    CellGeo<DIM, R> g;
+    double D[NV][DIM];
+    const int g0 = cv[(size_t)ce * NV];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) g.x0[a] = X[(size_t)g0 * DIM + a];
+    double scale = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        D[v][a] = X[(size_t)cv[(size_t)ce * NV + v] * DIM + a] - g.x0[a];
+        scale = fmax(scale, fabs(D[v][a]));
+        if (v > 0) g.D[v - 1][a] = (R)D[v][a];
+      }
+    double J[DIM * DIM];
+#pragma unroll
+    for (int k = 0; k < DIM * DIM; ++k) J[k] = 0.0;
+    const double w0 = DIM == 2 ? 0.5 : 0.25;
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        const double w = ((v >> b) & 1) ? w0 : -w0;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) J[a * DIM + b] += D[v][a] * w;
+      }
+    double Ji[DIM * DIM];
+    const double det = det_inv<DIM, double>(J, Ji);
+    if (!(det > 0.0)) atomicExch(flag, 1);
+#pragma unroll
+    for (int k = 0; k < DIM * DIM; ++k) g.Ji[k] = (R)Ji[k];
+    bool aff = true;
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < DIM; ++b)
+          if ((v >> b) & 1) s += D[1 << b][a];
+        if (fabs(D[v][a] - s) > 1e-13 * scale) aff = false;
+      }
+    g.affine = aff ? 1 : 0;
+    geo[ce] = g;
+  }
+}
+
+template <int DIM, typename R>
+static pfem2_status positions_impl(Ctx& c, double* out) {
+  const int b = c.cur;
+  k_particle_positions<DIM, R><<<grid_for(c, c.pcap, 256, 8), 256, 0, c.stream>>>(
+      c.pcell[b], (const R*)c.pxi[b], (size_t)c.pcap, c.d_np + b, (const CellGeo<DIM, R>*)c.cell_geo, out);
+  c.launches++;
+  return PFEM2_OK;
+}
+
+pfem2_status launch_particle_positions(Ctx& c, double* out) {
+  if (c.dim == 2) return c.pmixed ? positions_impl<2, float>(c, out) : positions_impl<2, double>(c, out);
+  return c.pmixed ? positions_impl<3, float>(c, out) : positions_impl<3, double>(c, out);
+}
+
+template <int DIM, typename R>
+static pfem2_status relocate_impl(Ctx& c, const double* xphys) {
+  const int b = c.cur;
+  PFEM2_CUDA(cudaMemsetAsync(c.d_counters, 0, sizeof(int) * CNT_N_STATS, c.stream));
+  PFEM2_CUDA(cudaMemsetAsync(c.dest_mask, 0, sizeof(unsigned) * c.nc, c.stream));
+  k_relocate<DIM, R><<<grid_for(c, c.pcap, 256, 8), 256, 0, c.stream>>>(
+      c.pcell[b], (R*)c.pxi[b], c.newcell, (size_t)c.pcap, c.d_np + b, (const CellGeo<DIM, R>*)c.cell_geo, c.cv,
+      c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, xphys, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap,
+      c.d_counters, c.dest_mask);
+  k_far_sort<<<1, 1024, sizeof(unsigned long long) * c.far_cap, c.stream>>>(c.far_keys, c.d_counters, c.far_cap);
+  c.launches += 2;
+  return PFEM2_OK;
+}
+
+pfem2_status launch_relocate(Ctx& c, const double* xphys) {
+  const pfem2_status s = c.dim == 2 ? (c.pmixed ? relocate_impl<2, float>(c, xphys) : relocate_impl<2, double>(c, xphys))
+                                    : (c.pmixed ? relocate_impl<3, float>(c, xphys) : relocate_impl<3, double>(c, xphys));
+  if (s != PFEM2_OK) return s;
+  // the re-sort into the moved cells with check_empty_cells
+  return launch_rebin(c, true, false, true);
+}
+
+pfem2_status launch_cell_geo(Ctx& c, int* flag) {
+  const int grid = grid_for(c, c.nc, 128, 8);
+  if (c.dim == 2) {
+    if (c.pmixed) k_cell_geo<2, float><<<grid, 128, 0, c.stream>>>(c.nc, c.X, c.cv, (CellGeo<2, float>*)c.cell_geo, flag);
+    else k_cell_geo<2, double><<<grid, 128, 0, c.stream>>>(c.nc, c.X, c.cv, (CellGeo<2, double>*)c.cell_geo, flag);
+  } else {
+    if (c.pmixed) k_cell_geo<3, float><<<grid, 128, 0, c.stream>>>(c.nc, c.X, c.cv, (CellGeo<3, float>*)c.cell_geo, flag);
+    else k_cell_geo<3, double><<<grid, 128, 0, c.stream>>>(c.nc, c.X, c.cv, (CellGeo<3, double>*)c.cell_geo, flag);
+  }
+  c.launches++;
+  PFEM2_CUDA(cudaGetLastError());
+  return PFEM2_OK;
+}
+
 // single-CTA bitonic sort of the (cell, particle) keys of the far movers
 __global__ void k_far_sort(unsigned long long* keys, const int* __restrict__ counters, int cap) {
   extern __shared__ unsigned long long sk[];
@@ -550,6 +750,13 @@ __global__ void k_far_sort(unsigned long long* keys, const int* __restrict__ cou
       __syncthreads();
     }
   for (int i = threadIdx.x; i < n; i += blockDim.x) keys[i] = sk[i];
+}
+
+// the far-mover sort's shared memory beyond the 48 KB default
+pfem2_status far_sort_setup(Ctx& c) {
+  PFEM2_CUDA(cudaFuncSetAttribute((const void*)k_far_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(unsigned long long) * c.far_cap)));
+  return PFEM2_OK;
 }
 
 template <int DIM, typename R>

@@ -38,6 +38,7 @@ EXPORTS = [
     "pfem2_launch_count", "pfem2_stage_times", "pfem2_enable_stage_timing", "pfem2_get_stream",
     "pfem2_last_error", "pfem2_abi_version", "pfem2_project_noalloc", "pfem2_solver_sizes",
     "pfem2_calculate_vorticity", "pfem2_set_tuning", "pfem2_get_tuning", "pfem2_tuning_key",
+    "pfem2_mesh_elasticity", "pfem2_move_mesh", "pfem2_get_vertices",
 ]
 
 
@@ -80,6 +81,9 @@ def load_library(path=LIB_PATH):
         "pfem2_set_tuning": [vp, C.POINTER(A.Tuning)],
         "pfem2_get_tuning": [vp, C.POINTER(A.Tuning)],
         "pfem2_tuning_key": [vp, C.c_char_p, C.c_int32],
+        "pfem2_mesh_elasticity": [vp, C.c_int32, C.POINTER(A.Elasticity), dp, ip, dp],
+        "pfem2_move_mesh": [vp],
+        "pfem2_get_vertices": [vp, C.c_int32, dp],
     }
     sig["pfem2_project_noalloc"] = [C.c_int32, C.c_int32, C.c_int32] + [vp] * 9 + [vp]
     for name, args in sig.items():
@@ -106,7 +110,7 @@ class Solver:
 
     def __init__(self, specs, precision=A.PREC_MIXED, device=0, movement_steps=None, max_per_part=None,
                  use_graph=True, capacity_factor=2.0, per_cell_max=0, particles_only=False, fp32_stages=0,
-                 far_capacity=0, tuning=None):
+                 far_capacity=0, tuning=None, moving_mesh=False):
         """tuning: a dict of pfem2_tuning fields (launch shapes) set before
         setup; unset or 0 fields come from the tuning cache named by
         PFEM2_TUNING_CACHE, else from the sizes"""
@@ -127,6 +131,7 @@ class Solver:
         cfg.use_graph = 1 if use_graph else 0
         cfg.particles_only = 1 if particles_only else 0
         cfg.fp32_stages = fp32_stages
+        cfg.moving_mesh = 1 if moving_mesh else 0
         self.cfg = cfg
         h = C.c_void_p()
         self._check(self.L.pfem2_create(C.byref(cfg), C.byref(h)))
@@ -201,6 +206,28 @@ class Solver:
     def step(self):
         self._check(self.L.pfem2_step(self.h))
 
+    # ---- moving mesh (cylinderDyM)
+    def problem_of_elasticity(self, lam, mu, fixed_ids, body_id, disp, tol=0.0, rtol=1e-12, max_iter=10000):
+        """problem_of_elasticity + solveU (cylinderDyM/cylinderDyM.cc:926-976,
+        886-903): the mesh displacement into FIELD_DISP_*; returns
+        (iterations, residual)"""
+        e = A.Elasticity()
+        e.lam, e.mu, e.body_id, e.tol, e.rtol, e.max_iter = lam, mu, body_id, tol, rtol, max_iter
+        mask = 0
+        for b in fixed_ids:
+            mask |= 1 << b
+        e.fixed_mask = mask
+        d = np.zeros(3)
+        d[:len(disp)] = disp
+        it, res = C.c_int32(), C.c_double()
+        self._check(self.L.pfem2_mesh_elasticity(self.h, 0, C.byref(e), _dptr(d), C.byref(it), C.byref(res)))
+        return it.value, res.value
+
+    def move_mesh(self):
+        """reinterpolate_fields, transform_grid, sort_particles_into_subdomains_and_cells
+        and check_empty_cells (cylinderDyM/cylinderDyM.cc:1157-1160)"""
+        self._check(self.L.pfem2_move_mesh(self.h))
+
     def step_and_read(self, fields=(A.FIELD_VX, A.FIELD_VY, A.FIELD_P), loads=None, out=None):
         n_inst = len(self.specs)
         if loads is None:
@@ -220,6 +247,12 @@ class Solver:
     def set_field(self, f, values, instance=0):
         v = np.ascontiguousarray(values, np.float64)
         self._check(self.L.pfem2_set_field(self.h, instance, f, _dptr(v)))
+
+    def vertices(self, instance=0):
+        """vertex coordinates [n_vertices, dim] (moved by move_mesh)"""
+        out = np.zeros(self.specs[instance].mesh.n_vertices * self.dim)
+        self._check(self.L.pfem2_get_vertices(self.h, instance, _dptr(out)))
+        return out.reshape(-1, self.dim)
 
     def n_particles(self, instance=0):
         n = C.c_int32()

@@ -25,8 +25,9 @@ STRUCTS = {
     "pfem2_mesh_view": (A.MeshView, ["n_vertices", "n_cells", "vertices", "cells", "face_boundary_id"]),
     "pfem2_config": (A.Config, ["dim", "precision", "device", "movement_steps", "max_particles_per_cell_part",
                                 "particles_per_cell_max", "particle_capacity_factor", "far_mover_capacity",
-                                "use_graph", "particles_only", "fp32_stages"]),
+                                "use_graph", "particles_only", "fp32_stages", "moving_mesh"]),
     "pfem2_tuning": (A.Tuning, A.TUNING_FIELDS),
+    "pfem2_elasticity": (A.Elasticity, ["lambda", "mu", "fixed_mask", "body_id", "tol", "rtol", "max_iter"]),
     "pfem2_stats": (A.Stats, ["n_particles", "n_deleted_last_move", "n_removed_last_check",
                               "n_reseeded_last_check", "n_far_movers_last_move", "iters", "residual",
                               "refinements_p"]),
@@ -54,7 +55,8 @@ def test_struct_layout_matches_header():
     for cname, (cls, fields) in STRUCTS.items():
         assert got[(cname, "sizeof")] == C.sizeof(cls), cname
         for f in fields:
-            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)
+            py = {"lambda": "lam"}.get(f, f)
+            assert got[(cname, f)] == getattr(cls, py).offset, (cname, f)
 
 
 def declared_entry_points():
