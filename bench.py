@@ -403,15 +403,18 @@ def channel_leg(args, local, flush, prec, stages):
     s.synchronize()
     s.enable_stage_timing(True)
     s.stage_times(reset=True)
-    ms, iters = 0.0, []
+    ms, iters, viters = 0.0, [], []
     for _ in range(args.steps):
         ms += timed_steps(s, stream, flush, 1)
-        iters.append(s.stats()["iters"][3])
+        st = s.stats()
+        iters.append(st["iters"][3])
+        viters.append([st["iters"][k] for k in (0, 1, 4, 5)])
     stages_ms = s.stage_times()
     out = {"timesteps_per_s": args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
            "fp32_stages": s.fp32_stages(),
            "stage_ms_per_step": {n: stages_ms[i] / args.steps for i, n in enumerate(STAGE_NAMES)},
-           "pressure_cg_iters_per_step": iters}
+           "pressure_cg_iters_per_step": iters,
+           "velocity_iters_per_step": viters}
     s.close()
     return out
 

@@ -76,6 +76,16 @@ def tune(specs, space=None, steps=5, warmup=2, cache=None, rounds=1, prepare=Non
     the automatic shapes. Returns {"key", "tuning", "ms_per_step",
     "baseline_ms", "trials"}; with `cache` the best entry is appended there."""
     space = DEFAULT_SPACE if space is None else space
+    # the candidates are timed without an existing cache's entries
+    saved = os.environ.pop("PFEM2_TUNING_CACHE", None)
+    try:
+        return _tune(specs, space, steps, warmup, cache, rounds, prepare, solver_kw)
+    finally:
+        if saved is not None:
+            os.environ["PFEM2_TUNING_CACHE"] = saved
+
+
+def _tune(specs, space, steps, warmup, cache, rounds, prepare, solver_kw):
     t0, best = measure(specs, None, steps, warmup, prepare=prepare, **solver_kw)
     if t0 is None:
         raise RuntimeError("the automatic launch shapes failed")
@@ -118,3 +128,57 @@ def read_cache(path):
         ms = float(parts[10]) if len(parts) > 10 else None
         out[key] = (dict(zip(A.TUNING_FIELDS, vals)), ms)
     return out
+
+
+def main(argv=None):
+    """Tunes the launch shapes of named workloads and appends them to a
+    cache file:  python -m pfem2_b200.autotune --cache FILE [--workloads ...]"""
+    import argparse
+
+    from . import cases
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--cache", required=True)
+    ap.add_argument("--workloads", nargs="+", default=["channel_mixed", "channel_fp64"],
+                    choices=["channel_mixed", "channel_fp64", "stress", "pipe_mixed", "ensemble"])
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    args = ap.parse_args(argv)
+
+    def tight(sp, rtol):
+        sp.case.vel_tol = sp.case.p_tol = 0.0
+        sp.case.vel_rtol = sp.case.p_rtol = rtol
+        return sp
+
+    particle_space = {k: DEFAULT_SPACE[k] for k in ("advect_blocks_per_sm", "advect_split", "rebin_blocks_per_sm")}
+    for w in args.workloads:
+        prepare = None
+        if w.startswith("channel"):
+            specs = [tight(cases.channel_disk(), args.rtol)]
+            kw = {"precision": A.PREC_MIXED if w == "channel_mixed" else A.PREC_FP64}
+            space = DEFAULT_SPACE
+        elif w == "pipe_mixed":
+            specs = [tight(cases.pipe_3d(), 1e-11)]
+            kw = {"precision": A.PREC_MIXED}
+            space = DEFAULT_SPACE
+        elif w == "ensemble":
+            specs = [tight(sp, args.rtol) for sp in cases.ensemble()]
+            kw = {"precision": A.PREC_MIXED}
+            space = {k: v for k, v in DEFAULT_SPACE.items() if k != "p_blocks_per_sm"}
+        else:
+            sp = cases.stress_2d()
+            specs = [sp]
+            kw = {"precision": A.PREC_MIXED, "fp32_stages": A.FP32_ALL, "particles_only": True,
+                  "capacity_factor": 3.0}
+            space = particle_space
+
+            def prepare(s, sp=sp):
+                for f, v in ((A.FIELD_VX, sp.meta["ux"]), (A.FIELD_VY, sp.meta["uy"]),
+                             (A.FIELD_PRED_VX, sp.meta["ux"]), (A.FIELD_PRED_VY, sp.meta["uy"])):
+                    s.set_field(f, v)
+        res = tune(specs, space=space, steps=args.steps, warmup=2, cache=args.cache, prepare=prepare, **kw)
+        print(w, res["key"], res["tuning"], f"{res['baseline_ms']:.4f} -> {res['ms_per_step']:.4f} ms", flush=True)
+
+
+if __name__ == "__main__":
+    main()
