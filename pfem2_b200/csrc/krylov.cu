@@ -58,12 +58,14 @@ constexpr int kSolveThreads = 384;  // 12 warps
 constexpr int kWarps = kSolveThreads / 32;
 constexpr int kMaxLocalSys = 16;
 
-enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_UZ = 5, S_B2 = 6 };
+enum { S_OUT_A = 0, S_OUT_B = 1, S_A = 2, S_B = 3, S_DONE = 4, S_UZ = 5, S_B2 = 6, S_C0 = 7, S_C1 = 8 };
 enum {
   ACT_NONE = 0, ACT_OUT_A = 1, ACT_OUT_B = 2, ACT_OUT_DONE = 3, ACT_A = 4, ACT_B = 5, ACT_UZ = 6, ACT_B2 = 7,
   ACT_P1 = 8,   // BiCGStab: finish the previous step, y = K^-1 p, v = A y
   ACT_P2 = 9,   // BiCGStab: e += alpha y, s = r - alpha v, t = A K^-1 s
-  ACT_BF = 10   // BiCGStab: e += omega K^-1 s before a reliable update
+  ACT_BF = 10,  // BiCGStab: e += omega K^-1 s before a reliable update
+  ACT_C0 = 11,  // Jacobi CG: w = A u after a restart
+  ACT_C1 = 12   // Jacobi CG: one iteration in one phase (single reduction)
 };
 // partial sums per tile: CG uses 2, BiCGStab 5 (and the FP64 residual
 // phase |r|^2 and |b|^2)
@@ -145,6 +147,10 @@ template <typename R> struct SolveArgs {
   // w = K^-1 v double buffered (parity L.par; y in p), the shadow residual
   // rh, s, t and kt = K^-1 t; v in q, r in r's first buffer
   R *bz, *bw, *rh, *bs, *bt, *bkt;
+  // Jacobi CG with one reduction per iteration: u = D^-1 r, wh = D^-1 w and
+  // sh = D^-1 s double buffered (parity L.par), w = A u and s = A p on the
+  // own rows only; p in p's first buffer, r in r's first buffer
+  R *cu, *cwh, *csh, *cw, *cs;
   // workspace per component slot, nv entries each; r and p: 2 buffers
   R *e, *r, *z, *p, *q;
   double* r64;
@@ -461,7 +467,6 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
       if (threadIdx.x == 0) atomicCAS(a.gb.err, 0, 2);
       break;
     }
-    const bool phaseA = (iter & 1) == 0;
     const double* prev = a.part + (size_t)((iter + 1) & 1) * a.ntiles * NS;
     // ---- wait for the previous phase of the block's running systems: every
     // tile adds 1 to its system's counter with a release add once its phase
@@ -613,25 +618,18 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
               break;
           }
         } else if (!MG) {
-          if (phaseA) {
-            if (L.state == S_OUT_A) {
+          // Jacobi CG with one reduction per iteration (Chronopoulos and
+          // Gear 1989): u = D^-1 r, w = A u, gamma = (r, u), delta = (w, u);
+          // beta = gamma / gamma_old, alpha = gamma / (delta - beta gamma /
+          // alpha_old); p = u + beta p, s = w + beta s (= A p), x += alpha p,
+          // r -= alpha s. One phase per iteration (C1), the w = A u of a
+          // restart in a phase of its own (C0).
+          switch (L.state) {
+            case S_OUT_A:
               act = ACT_OUT_A;
               L.state = S_OUT_B;
-            } else if (L.state == S_A) {
-              const double rz = L.sum[0], rr = sqrt(L.sum[1]);
-              if (rr <= L.intol || L.it >= L.maxit || !(rr == rr)) {
-                act = ACT_OUT_A;  // reliable update in FP64
-                L.state = S_OUT_B;
-              } else {
-                L.beta = L.first ? 0.0 : (L.rz_prev != 0.0 ? rz / L.rz_prev : 0.0);
-                L.rz_prev = rz;
-                L.first = 0;
-                act = ACT_A;
-                L.state = S_B;
-              }
-            }
-          } else {
-            if (L.state == S_OUT_B) {
+              break;
+            case S_OUT_B:
               L.res = sqrt(L.sum[0]);
               L.outer += 1;
               if (L.res <= L.tol || L.it >= L.maxit || !(L.res == L.res)) {
@@ -639,16 +637,41 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
                 L.state = S_DONE;
               } else {
                 L.intol = fmax(a.eta * L.res, 0.5 * L.tol);
-                L.first = 1;  // CG restarts from the true residual
+                L.chk = 0;
                 act = ACT_OUT_B;
-                L.state = S_A;
+                L.state = S_C0;
               }
-            } else if (L.state == S_B) {
-              L.alpha = L.sum[0] != 0.0 ? L.rz_prev / L.sum[0] : 0.0;
-              L.it += 1;
-              act = ACT_B;
-              L.state = S_A;
+              break;
+            case S_C0:
+              act = ACT_C0;
+              L.state = S_C1;
+              break;
+            case S_C1: {
+              // sums of the previous phase: (r, u), (w, u), (r, r)
+              const double g = L.sum[0], dl = L.sum[1], rr = sqrt(L.sum[2]);
+              if (!L.chk) {
+                L.alpha = dl != 0.0 ? g / dl : 0.0;
+                L.beta = 0.0;
+                L.rz_prev = g;
+                act = ACT_C1;
+              } else {
+                L.it += 1;
+                const double be = L.rz_prev != 0.0 ? g / L.rz_prev : 0.0;
+                const double den = dl - (L.alpha != 0.0 ? be * g / L.alpha : 0.0);
+                if (rr <= L.intol || L.it >= L.maxit || !(rr == rr) || !(den > 0.0)) {
+                  act = ACT_OUT_A;  // reliable update in FP64
+                  L.state = S_OUT_B;
+                } else {
+                  L.beta = be;
+                  L.alpha = g / den;
+                  L.rz_prev = g;
+                  act = ACT_C1;
+                }
+              }
+              break;
             }
+            default:
+              break;
           }
         } else {
           switch (L.state) {
@@ -984,13 +1007,59 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
               a.rh[k * nv + row] = rr;
               a.bz[(2 * k + L.par) * nv + row] = rr * dinv[row];
             } else if (!MG) {
-              const R zz = rr * dinv[row];
-              z[row] = zz;
-              v0 += (double)rr * (double)zz;
-              v1 += (double)rr * (double)rr;
+              a.cu[(2 * k + L.par) * nv + row] = rr * dinv[row];
             }
           }
         }
+      } else if (!MG && act == ACT_C0) {
+        // w = A u, wh = D^-1 w after a restart; (r, u), (w, u), (r, r)
+        const int row = sl * 32 + lane;
+        const R* u = a.cu + (2 * k + L.par) * nv;
+        const R* A = a.Ain[k];
+        const R w = sell_dot<R, CH>(R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; },
+                                    [&](int j) { return u[j]; });
+        a.cw[k * nv + row] = w;
+        a.cwh[(2 * k + L.par) * nv + row] = w * dinv[row];
+        const double rr = (double)r[row], uu = (double)u[row];
+        v0 += rr * uu;
+        v1 += (double)w * uu;
+        v2 += rr * rr;
+      } else if (!MG && act == ACT_C1) {
+        // p = u + beta p, s = w + beta s, sh = wh + beta sh, e += alpha p,
+        // r -= alpha s, u' = u - alpha sh (= D^-1 r'), w' = A u' with u'
+        // formed on the fly at the columns from u, wh and the old sh, wh' =
+        // D^-1 w'; (r', u'), (w', u'), (r', r'). The first iteration after a
+        // restart has p = u, s = w, sh = wh.
+        const int row = sl * 32 + lane;
+        const bool first = L.chk == 0;
+        const R al = R(L.alpha), be = R(L.beta);
+        const R* uo = a.cu + (2 * k + L.par) * nv;
+        const R* who = a.cwh + (2 * k + L.par) * nv;
+        const R* sho = a.csh + (2 * k + L.par) * nv;
+        const auto unew = [&](int j) -> R {
+          const R sh = first ? who[j] : fma_r(be, sho[j], who[j]);
+          return fma_r(-al, sh, uo[j]);
+        };
+        R* pk = a.p + (2 * k) * nv;
+        R* sk = a.cs + k * nv;
+        const R sh = first ? who[row] : fma_r(be, sho[row], who[row]);
+        const R pp = first ? uo[row] : fma_r(be, pk[row], uo[row]);
+        const R ss = first ? a.cw[k * nv + row] : fma_r(be, sk[row], a.cw[k * nv + row]);
+        pk[row] = pp;
+        sk[row] = ss;
+        e[row] = fma_r(al, pp, e[row]);
+        const R rn = fma_r(-al, ss, r[row]);
+        r[row] = rn;
+        const R un = unew(row);
+        const R* A = a.Ain[k];
+        const R w = sell_dot<R, CH>(R(0), SLc, SLp[sl], SLl[sl], lane, [&](int ei) { return A[ei]; }, unew);
+        a.csh[(2 * k + (L.par ^ 1)) * nv + row] = sh;
+        a.cu[(2 * k + (L.par ^ 1)) * nv + row] = un;
+        a.cwh[(2 * k + (L.par ^ 1)) * nv + row] = w * dinv[row];
+        a.cw[k * nv + row] = w;
+        v0 += (double)rn * (double)un;
+        v1 += (double)w * (double)un;
+        v2 += (double)rn * (double)rn;
       } else if (!MG && act == ACT_P1) {
         // y' = zr' + beta (y - omega w), zr' = zr - alpha w - omega kt the
         // preconditioned new residual (first step after a restart: y' = zr),
@@ -1116,14 +1185,11 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         spart[NS * it + 1] = v1;
       }
       if (NSMAX > 2 && NS > 2) {
-        v2 = warp_sum(v2);
-        v3 = warp_sum(v3);
-        v4 = warp_sum(v4);
-        if (lane == 0) {
-          spart[NS * it + 2] = v2;
-          spart[NS * it + 3] = v3;
-          spart[NS * it + 4] = v4;
-        }
+        const double vx[3] = {warp_sum(v2), NS > 3 ? warp_sum(v3) : 0.0, NS > 4 ? warp_sum(v4) : 0.0};
+        if (lane == 0)
+#pragma unroll
+          for (int q = 2; q < NSMAX; ++q)
+            if (q < NS) spart[NS * it + q] = vx[q - 2];
       }
     }
     __syncthreads();
@@ -1158,6 +1224,10 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
           if (MG) L.rpar ^= 1;
         }
         if (L.act == ACT_P1) L.par ^= 1;
+        if (L.act == ACT_C1) {
+          L.par ^= 1;
+          L.chk = 1;
+        }
         if (L.act == ACT_OUT_DONE && L.owner) {
           a.out_it[L.sys] = L.it;
           a.out_res[L.sys] = L.res;
@@ -1192,6 +1262,7 @@ struct KrylovWs {
   int nsum[2] = {2, 2};                            // partial sums per tile of each phase
   bool bicg[2] = {false, false};                   // phase solved by BiCGStab
   void *bz = nullptr, *bw = nullptr, *rh = nullptr, *bs = nullptr, *bt = nullptr, *bkt = nullptr;
+  void *cu = nullptr, *cwh = nullptr, *csh = nullptr, *cw = nullptr, *cs = nullptr;
   // multigrid of the pressure phase (phase 0)
   bool mg = false;
   int mg_minb = 1;  // resident blocks per SM of the pressure solve: 2 for batches (many tiles per block)
@@ -1416,7 +1487,9 @@ pfem2_status krylov_setup(Ctx& c) {
     w->ntl_max[ph] = ntl_max;
     w->items_max[ph] = items_max;
     w->bicg[ph] = ph == 0 ? c.p_bicg : c.vel_bicg;
-    w->nsum[ph] = w->bicg[ph] ? kMaxSums : 2;
+    // BiCGStab 5 sums, Jacobi CG 3 (one reduction per iteration), the
+    // multigrid CG of the pressure 2
+    w->nsum[ph] = w->bicg[ph] ? kMaxSums : (ph == 1 || !c.two_level ? 3 : 2);
     w->items_bytes[ph] =
         al16(sizeof(double) * w->nsum[ph] * (size_t)items_max) + al16(sizeof(int) * (size_t)(ntl_max + 1));
     if (ph == 0) {
@@ -1476,6 +1549,14 @@ pfem2_status krylov_setup(Ctx& c) {
   }
   PFEM2_TRY(ws_alloc(w, &w->r64, nv * dim));
   PFEM2_TRY(ws_alloc(w, &w->part, 2 * (size_t)kMaxSums * maxtiles));
+  {
+    // single-reduction Jacobi CG vectors: u, wh, sh double buffered, w, s
+    const size_t rs = c.kmixed ? sizeof(float) : sizeof(double);
+    unsigned char* b[5];
+    const size_t n[5] = {2 * nv * dim, 2 * nv * dim, 2 * nv * dim, nv * dim, nv * dim};
+    for (int k = 0; k < 5; ++k) PFEM2_TRY(ws_alloc(w, &b[k], n[k] * rs));
+    w->cu = b[0]; w->cwh = b[1]; w->csh = b[2]; w->cw = b[3]; w->cs = b[4];
+  }
   if (c.vel_bicg || c.p_bicg) {
     // BiCGStab vectors: zr and w double buffered, rh, s, t, kt
     const size_t rs = c.kmixed ? sizeof(float) : sizeof(double);
@@ -1768,6 +1849,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   a.bicg = w->bicg[ph] ? 1 : 0;
   a.nsum = mg ? 2 : w->nsum[ph];
   a.bz = (R*)w->bz; a.bw = (R*)w->bw; a.rh = (R*)w->rh; a.bs = (R*)w->bs; a.bt = (R*)w->bt; a.bkt = (R*)w->bkt;
+  a.cu = (R*)w->cu; a.cwh = (R*)w->cwh; a.csh = (R*)w->csh; a.cw = (R*)w->cw; a.cs = (R*)w->cs;
   a.maxit_i = c.d_sysinfo;
   a.e = (R*)w->e; a.r = (R*)w->r; a.z = (R*)w->z; a.q = (R*)w->q; a.p = (R*)w->p;
   a.r64 = w->r64;
@@ -1782,7 +1864,7 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   int mx = 0;
   for (auto& in : c.inst) mx = std::max(mx, in.cs.max_iter > 0 ? in.cs.max_iter : 10000);
   // phases per iteration, and BiCGStab's restarts (three phases each, at most max_iter)
-  a.iter_cap = (mg ? (w->split ? 4 : 3) : (a.bicg ? 5 : 2)) * mx + 256;
+  a.iter_cap = (mg ? (w->split ? 4 : 3) : (a.bicg ? 5 : 4)) * mx + 256;
   a.gb.count = c.barrier;
   a.gb.gen = c.barrier + 1;
   a.gb.err = c.d_err;
