@@ -667,7 +667,7 @@ def ensemble_leg(args, rank, world, local, flush, fp64_single):
 
     from pfem2_b200 import _abi as A
     from pfem2_b200 import cases, sharding
-    from pfem2_b200.solver import Solver
+    from pfem2_b200.solver import STAGE_NAMES, Solver
 
     all_specs = [tight(sp, args.rtol) for sp in cases.ensemble(n=args.ensemble_n)]
     specs = all_specs
@@ -679,7 +679,10 @@ def ensemble_leg(args, rank, world, local, flush, fp64_single):
     for _ in range(3):
         s.step()
     s.synchronize()
+    s.enable_stage_timing(True)
+    s.stage_times(reset=True)
     ms = timed_steps(s, stream, flush, args.extra_steps)
+    stages = s.stage_times()
     if world > 1:
         ms = sharding.max_over_ranks(ms)
     st = s.stats()
@@ -693,6 +696,7 @@ def ensemble_leg(args, rank, world, local, flush, fp64_single):
         "ms_per_batch_step": ms / args.extra_steps, "instance_timesteps_per_s": inst_steps,
         "cell_updates_per_s": cells * args.extra_steps / (ms / 1e3),
         "max_pressure_cg_iters": st["iters"][3], "far_movers_last_step": st["far"],
+        "stage_ms_per_step": {n: stages[i] / args.extra_steps for i, n in enumerate(STAGE_NAMES)},
     }
     s.close()
     return out

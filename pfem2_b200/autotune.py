@@ -160,7 +160,8 @@ def main(argv=None):
         elif w == "pipe_mixed":
             specs = [tight(cases.pipe_3d(), 1e-11)]
             kw = {"precision": A.PREC_MIXED}
-            space = DEFAULT_SPACE
+            space = {"p_blocks_per_sm": [1, 2], "vel_tile_slices": [8, 16, 32], "advect_blocks_per_sm": [8, 16],
+                     "rebin_blocks_per_sm": [4, 8]}
         elif w == "ensemble":
             specs = [tight(sp, args.rtol) for sp in cases.ensemble()]
             kw = {"precision": A.PREC_MIXED}

@@ -1370,8 +1370,9 @@ pfem2_status krylov_setup(Ctx& c) {
   // warps bring); a batch, or one system from mg_wide_min rows on (where the
   // solve is bound by memory parallelism, not by latency): two
   w->mg_minb = (c.inst.size() > 1 || (long long)c.nv >= c.mg_wide_min) ? 2 : 1;
-  // a single system below the wide size may be tuned to two blocks per SM
-  if (c.inst.size() == 1 && (long long)c.nv < c.mg_wide_min && c.tune.p_blocks_per_sm) w->mg_minb = c.tune.p_blocks_per_sm;
+  // a single system may be tuned to one or two blocks per SM (one block has
+  // the registers of the whole SM share, two hide more latency)
+  if (c.inst.size() == 1 && c.tune.p_blocks_per_sm) w->mg_minb = c.tune.p_blocks_per_sm;
   c.tune.p_blocks_per_sm = w->mg_minb;
   const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
