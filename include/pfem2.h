@@ -348,15 +348,16 @@ int32_t pfem2_abi_version(void);
  * No counterpart in the reference (its kernels have fixed launch shapes).
  * Each field 0 = automatic. None of them changes the particle kernels'
  * arithmetic (their results are bitwise the same under every setting); the
- * velocity tile size changes the order of the solver's partial sums and the
- * pressure width its preconditioner, both within the solver tolerance. */
+ * velocity tile size and blocks per SM change the order of the solver's
+ * partial sums and the pressure width its preconditioner, all within the
+ * solver tolerance. */
 typedef struct {
   int32_t advect_blocks_per_sm;  /* advection grid in 256-thread blocks per SM (sets particles per block) */
-  int32_t advect_split;          /* 1: one advection kernel, 2: stayers then leavers in two kernels */
+  int32_t advect_split;          /* 1: one advection pass, 2: stayers, then each block's queued leavers */
   int32_t rebin_blocks_per_sm;   /* re-sort grid in 256-thread blocks per SM (tiles of 8 cells) */
   int32_t vel_tile_slices;       /* velocity solves: SELL slices of 32 rows per Krylov tile */
   int32_t p_blocks_per_sm;       /* pressure multigrid of a single system: 1 or 2 blocks per SM */
-  int32_t pad_;
+  int32_t vel_blocks_per_sm;     /* velocity solves: 1 or 2 blocks per SM */
 } pfem2_tuning;
 /* Sets the launch shapes (before pfem2_setup). Fields left at 0 are taken
  * from the tuning cache named by the environment variable PFEM2_TUNING_CACHE

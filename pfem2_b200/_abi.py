@@ -91,11 +91,12 @@ class Tuning(C.Structure):
     _fields_ = [
         ("advect_blocks_per_sm", C.c_int32), ("advect_split", C.c_int32),
         ("rebin_blocks_per_sm", C.c_int32), ("vel_tile_slices", C.c_int32),
-        ("p_blocks_per_sm", C.c_int32), ("pad_", C.c_int32),
+        ("p_blocks_per_sm", C.c_int32), ("vel_blocks_per_sm", C.c_int32),
     ]
 
 
-TUNING_FIELDS = ["advect_blocks_per_sm", "advect_split", "rebin_blocks_per_sm", "vel_tile_slices", "p_blocks_per_sm"]
+TUNING_FIELDS = ["advect_blocks_per_sm", "advect_split", "rebin_blocks_per_sm", "vel_tile_slices", "p_blocks_per_sm",
+                 "vel_blocks_per_sm"]
 
 
 class Elasticity(C.Structure):

@@ -2,10 +2,11 @@
 
 The particle kernels and the persistent Krylov solver have shapes that the
 best choice of depends on the GPU and the mesh size: the advection grid
-(particles per block) and whether advection runs as one kernel or as two
-(stayers, then leavers), the re-sort grid, the velocity solver's tile size
-(SELL slices per tile) and the blocks per SM of a single pressure system's
-multigrid solve. `tune` times whole steps (the device time of every stage,
+(particles per block) and whether advection runs in one pass or in two
+phases (stayers, then queued leavers), the re-sort grid, the velocity
+solves' tile size (SELL slices per tile) and blocks per SM, and the blocks
+per SM of a single pressure system's multigrid solve. `tune` times whole
+steps (the device time of every stage,
 CUDA events inside the library) for candidate shapes by coordinate descent
 and appends the fastest to a cache file under the context's key: device
 name, dim, FP32 stages, log2 cells, log2 instances (pfem2_tuning_key). A
@@ -33,6 +34,7 @@ DEFAULT_SPACE = {
     "rebin_blocks_per_sm": [2, 4, 6, 8, 12],
     "vel_tile_slices": [4, 8, 16, 32],
     "p_blocks_per_sm": [1, 2],
+    "vel_blocks_per_sm": [1, 2],
 }
 
 
@@ -124,8 +126,14 @@ def read_cache(path):
         if len(parts) < 10:
             continue
         key = " ".join(parts[:5])
-        vals = [int(x) for x in parts[5:10]]
-        ms = float(parts[10]) if len(parts) > 10 else None
+        vals, ms = [], None
+        for x in parts[5:]:
+            if "." in x:
+                ms = float(x)
+                break
+            if len(vals) < len(A.TUNING_FIELDS):
+                vals.append(int(x))
+        vals += [0] * (len(A.TUNING_FIELDS) - len(vals))
         out[key] = (dict(zip(A.TUNING_FIELDS, vals)), ms)
     return out
 
@@ -160,8 +168,8 @@ def main(argv=None):
         elif w == "pipe_mixed":
             specs = [tight(cases.pipe_3d(), 1e-11)]
             kw = {"precision": A.PREC_MIXED}
-            space = {"p_blocks_per_sm": [1, 2], "vel_tile_slices": [8, 16, 32], "advect_blocks_per_sm": [8, 16],
-                     "rebin_blocks_per_sm": [4, 8]}
+            space = {"p_blocks_per_sm": [1, 2], "vel_tile_slices": [8, 16, 32], "vel_blocks_per_sm": [1, 2],
+                     "advect_blocks_per_sm": [8, 16], "rebin_blocks_per_sm": [4, 8]}
         elif w == "ensemble":
             specs = [tight(sp, args.rtol) for sp in cases.ensemble()]
             kw = {"precision": A.PREC_MIXED}

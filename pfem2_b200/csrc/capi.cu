@@ -142,9 +142,12 @@ static std::string tuning_key(const Ctx& c) {
 
 // The tuning cache (PFEM2_TUNING_CACHE): one entry per line,
 //   <device> <dim> <stages> <log2 cells> <log2 instances>
-//   <advect bps> <advect split> <rebin bps> <vel tile slices> <p bps> [ms per step]
-// '#' starts a comment; the last entry with this context's key wins. Its
-// values fill the fields the caller left at 0.
+//   <advect bps> <advect split> <rebin bps> <vel tile slices> <p bps> [<vel bps>] [ms per step]
+// (the launch-shape values are integers, the time has a decimal point; a
+// missing value is automatic). '#' starts a comment; the last entry with
+// this context's key wins. Its values fill the fields the caller left at 0.
+constexpr int kTuneVals = 6;
+
 static void apply_tuning_cache(Ctx& c) {
   c.tune = c.tune_req;
   c.tune_source = "caller";
@@ -154,26 +157,39 @@ static void apply_tuning_cache(Ctx& c) {
   if (!f) return;
   const std::string key = tuning_key(c);
   char line[512];
-  int best[5] = {0, 0, 0, 0, 0};
+  int best[kTuneVals] = {};
   bool found = false;
   while (fgets(line, sizeof(line), f)) {
     if (line[0] == '#') continue;
-    char dev[256];
-    int dim, st, lc, li, v[5];
-    if (sscanf(line, "%255s %d %d %d %d %d %d %d %d %d", dev, &dim, &st, &lc, &li, &v[0], &v[1], &v[2], &v[3],
-               &v[4]) != 10)
-      continue;
-    char k[320];
-    snprintf(k, sizeof(k), "%s %d %d %d %d", dev, dim, st, lc, li);
+    std::vector<std::string> tok;
+    char* save = nullptr;
+    for (char* t = strtok_r(line, " \t\r\n", &save); t; t = strtok_r(nullptr, " \t\r\n", &save))
+      tok.emplace_back(t);
+    if (tok.size() < 5 + 5) continue;
+    const std::string k = tok[0] + " " + tok[1] + " " + tok[2] + " " + tok[3] + " " + tok[4];
     if (key != k) continue;
-    std::copy(v, v + 5, best);
+    int v[kTuneVals] = {};
+    bool ok = true;
+    int nv = 0;
+    for (size_t q = 5; q < tok.size() && nv < kTuneVals; ++q) {
+      if (tok[q].find('.') != std::string::npos) break;  // the time
+      char* end = nullptr;
+      const long x = strtol(tok[q].c_str(), &end, 10);
+      if (!end || *end) {
+        ok = false;
+        break;
+      }
+      v[nv++] = (int)x;
+    }
+    if (!ok || nv < 5) continue;
+    std::copy(v, v + kTuneVals, best);
     found = true;
   }
   fclose(f);
   if (!found) return;
-  int32_t* dst[5] = {&c.tune.advect_blocks_per_sm, &c.tune.advect_split, &c.tune.rebin_blocks_per_sm,
-                     &c.tune.vel_tile_slices, &c.tune.p_blocks_per_sm};
-  for (int i = 0; i < 5; ++i)
+  int32_t* dst[kTuneVals] = {&c.tune.advect_blocks_per_sm, &c.tune.advect_split, &c.tune.rebin_blocks_per_sm,
+                             &c.tune.vel_tile_slices, &c.tune.p_blocks_per_sm, &c.tune.vel_blocks_per_sm};
+  for (int i = 0; i < kTuneVals; ++i)
     if (*dst[i] == 0 && best[i] > 0) *dst[i] = best[i];
   c.tune_source = "cache";
 }
@@ -181,7 +197,7 @@ static void apply_tuning_cache(Ctx& c) {
 static pfem2_status check_tuning(const pfem2_tuning& t) {
   if (t.advect_blocks_per_sm < 0 || t.advect_blocks_per_sm > 32 || t.advect_split < 0 || t.advect_split > 2 ||
       t.rebin_blocks_per_sm < 0 || t.rebin_blocks_per_sm > 32 || t.vel_tile_slices < 0 || t.vel_tile_slices > 4096 ||
-      t.p_blocks_per_sm < 0 || t.p_blocks_per_sm > 2) {
+      t.p_blocks_per_sm < 0 || t.p_blocks_per_sm > 2 || t.vel_blocks_per_sm < 0 || t.vel_blocks_per_sm > 2) {
     set_error("tuning: a field is out of range");
     return PFEM2_INVALID_ARG;
   }
@@ -555,14 +571,6 @@ static pfem2_status alloc_particles(Ctx& c, size_t seeded) {
   }
   if (c.newcell) cudaFree(c.newcell);
   PFEM2_CUDA(cudaMalloc(&c.newcell, sizeof(int) * cap));
-  // the advection queue: one region per warp of the fast kernel's grid
-  c.adv_grid = grid_for(c, (long long)cap, 256, c.tune.advect_blocks_per_sm);
-  if (c.adv_queue) cudaFree(c.adv_queue);
-  if (c.adv_wcount) cudaFree(c.adv_wcount);
-  if (c.adv_qstep) cudaFree(c.adv_qstep);
-  PFEM2_CUDA(cudaMalloc(&c.adv_qstep, (cap + (size_t)c.adv_grid * 257)));
-  PFEM2_CUDA(cudaMalloc(&c.adv_queue, sizeof(int) * (cap + (size_t)c.adv_grid * 257)));
-  PFEM2_CUDA(cudaMalloc(&c.adv_wcount, sizeof(int) * (size_t)c.adv_grid * 8));
   c.pcap = (int)cap;
   c.graph_valid = false;
   return PFEM2_OK;
@@ -776,7 +784,7 @@ pfem2_status pfem2_destroy(pfem2_ctx* x) {
                   c.ring_ptr, c.ring_cell, c.sl_ptr, c.sl_len, c.sl_col, c.inc_slot, c.zero_flag, c.wall_dv,
                   c.wall_cells, c.ring_rev, c.dest_mask, c.d_inst,
                   c.sys_scalars, c.d_sysinfo, c.Vr, c.dVr, c.partial, c.rebin_tiles, c.d_np, c.d_counters,
-                  c.far_keys, c.barrier, c.d_err, c.d_err_sticky, c.newcell, c.adv_queue, c.adv_wcount, c.adv_qstep};
+                  c.far_keys, c.barrier, c.d_err, c.d_err_sticky, c.newcell};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c.pmixed && c.v2c_dir_r) cudaFree(c.v2c_dir_r);
@@ -1236,7 +1244,6 @@ pfem2_status pfem2_set_tuning(pfem2_ctx* x, const pfem2_tuning* t) {
   if (x->c.setup_done) { set_error("pfem2_set_tuning: call it before pfem2_setup"); return PFEM2_BAD_STATE; }
   PFEM2_TRY(check_tuning(*t));
   x->c.tune_req = *t;
-  x->c.tune_req.pad_ = 0;
   return PFEM2_OK;
 }
 

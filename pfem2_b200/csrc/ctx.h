@@ -137,16 +137,10 @@ struct Ctx {
   void* pu[2] = {};
   int cur = 0;
   int* newcell = nullptr;
-  // particles that leave their cell during the advection sub-steps: the
-  // fast advection kernel's warp w of block b appends them to region
-  // (b * kAdvWarps + w) of adv_queue and stores the count in adv_wcount
-  int* adv_queue = nullptr;
-  unsigned char* adv_qstep = nullptr;  // the sub-step each queued particle left in
-  int* adv_wcount = nullptr;
-  int adv_grid = 0;
-  // particle capacity from which the advection runs as two kernels (the
-  // second pass does not pay for itself on small particle sets); the
-  // environment variable PFEM2_ADVECT_SPLIT_MIN overrides it at creation
+  // particle capacity from which the advection runs in two phases per
+  // block (stayers, then the block's queued leavers; on small particle sets
+  // the one-pass kernel is as fast); the environment variable
+  // PFEM2_ADVECT_SPLIT_MIN overrides it at creation
   long long adv_split_min = 1LL << 23;
   int* cell_start[2] = {};
   unsigned long long* rebin_tiles = nullptr;  // ticket + status words of the rebin's single-pass scan

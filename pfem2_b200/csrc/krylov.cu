@@ -471,11 +471,10 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
     // ---- wait for the previous phase of the block's running systems: every
     // tile adds 1 to its system's counter with a release add once its phase
     // is written, so iter x (tiles of the system) means that every tile of
-    // the system has finished phase iter - 1; lane k polls local system k,
-    // then an acquire fence (and the block barrier) orders everything those
-    // blocks wrote before this phase's reads. Blocks of other systems are
-    // not waited for. Then the sums of the previous phase's partials (warp
-    // 0, fixed order).
+    // the system has finished phase iter - 1; lane k of warp 0 polls local
+    // system k, then an acquire fence (and the block barrier) orders
+    // everything those blocks wrote before this phase's reads. Blocks of
+    // other systems are not waited for.
     if (warp == 0) {
       bool stop = true;
       for (int k = 0; k < nls; ++k) stop &= ls[k].state == S_DONE;
@@ -499,53 +498,35 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) 
         }
       }
       if (lane == 0) s_stop = stop;
-      for (int k = 0; k < nls && !stop; ++k) {
-        const int st = ls[k].state;
-        if (st == S_DONE || st == S_OUT_A || (st == S_UZ && (!ls[k].chk || a.split))) continue;
-        const int t0 = ls[k].t0, t1 = ls[k].t1;
-        double s0 = 0.0, s1 = 0.0;
-        for (int tb = t0; tb < t1; tb += 256) {
-          double v0[8], v1[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int t = tb + u * 32 + lane;
-            v0[u] = t < t1 ? __ldcg(prev + t) : 0.0;
-            v1[u] = t < t1 ? __ldcg(prev + a.ntiles + t) : 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            s0 += v0[u];
-            s1 += v1[u];
-          }
-        }
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        if (lane == 0) {
-          ls[k].sum[0] = s0;
-          ls[k].sum[1] = s1;
-        }
-        // BiCGStab's further sums, in the same fixed order
-#pragma unroll
-        for (int q = 2; q < NSMAX; ++q) {
-          if (q >= NS) break;
-          double sq = 0.0;
-          for (int tb = t0; tb < t1; tb += 256) {
-            double vq[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              const int t = tb + u * 32 + lane;
-              vq[u] = t < t1 ? __ldcg(prev + (size_t)q * a.ntiles + t) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) sq += vq[u];
-          }
-          sq = warp_sum(sq);
-          if (lane == 0) ls[k].sum[q] = sq;
-        }
-      }
     }
     __syncthreads();
     if (s_stop) break;
+    // the sums of the previous phase's partials: warp q sums partial q of
+    // every local system over its tiles in a fixed order (lane l adds tiles
+    // l, l + 32, ..., then the warp sum), all sums in one round of loads
+    if (warp < NS) {
+      const int q = warp;
+      for (int k = 0; k < nls; ++k) {
+        const int st = ls[k].state;
+        if (st == S_DONE || st == S_OUT_A || (st == S_UZ && (!ls[k].chk || a.split))) continue;
+        const int t0 = ls[k].t0, t1 = ls[k].t1;
+        const double* pq = prev + (size_t)q * a.ntiles;
+        double sq = 0.0;
+        for (int tb = t0; tb < t1; tb += 256) {
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int t = tb + u * 32 + lane;
+            v[u] = t < t1 ? __ldcg(pq + t) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) sq += v[u];
+        }
+        sq = warp_sum(sq);
+        if (lane == 0) ls[k].sum[q] = sq;
+      }
+    }
+    __syncthreads();
     // ---- decisions (thread 0; identical in every block owning the system)
     if (threadIdx.x == 0) {
       for (int k = 0; k < nls; ++k) {
@@ -1266,6 +1247,7 @@ struct KrylovWs {
   // multigrid of the pressure phase (phase 0)
   bool mg = false;
   int mg_minb = 1;  // resident blocks per SM of the pressure solve: 2 for batches (many tiles per block)
+  int vel_minb = 2;  // resident blocks per SM of the velocity solves
   int nls0 = 1;
   int dmax = 1, s1max = 0, s2max = 0, s3max = 0, b2max = 0, o2max = 0, emax = 0;
   int n1 = 0, n2 = 0, n3 = 0;
@@ -1374,6 +1356,10 @@ pfem2_status krylov_setup(Ctx& c) {
   // the registers of the whole SM share, two hide more latency)
   if (c.inst.size() == 1 && c.tune.p_blocks_per_sm) w->mg_minb = c.tune.p_blocks_per_sm;
   c.tune.p_blocks_per_sm = w->mg_minb;
+  // the velocity solves: two blocks per SM hide more latency, one has fewer
+  // blocks to wait for at every phase and the registers of the SM share
+  w->vel_minb = c.tune.vel_blocks_per_sm ? c.tune.vel_blocks_per_sm : 2;
+  c.tune.vel_blocks_per_sm = w->vel_minb;
   const int dim = c.dim, ni = (int)c.inst.size();
   const size_t nv = c.nv;
   const int bps = std::max(1, c.solve_blocks_per_sm);
@@ -1421,7 +1407,7 @@ pfem2_status krylov_setup(Ctx& c) {
     // the multigrid grid is sized before its shared memory is known
     // (mg_minb blocks per SM); krylov_setup_precond checks residency
     // afterwards. The Jacobi kernel runs two blocks per SM.
-    const int occ = ph == 0 ? w->mg_minb : std::min(2, occupancy_any<false>(c.kmixed, 2, 0));
+    const int occ = ph == 0 ? w->mg_minb : std::min(w->vel_minb, occupancy_any<false>(c.kmixed, w->vel_minb, 0));
     if (occ < 1) {
       set_error("krylov: the solver kernel cannot be resident");
       return PFEM2_CUDA_ERROR;
@@ -1503,15 +1489,15 @@ pfem2_status krylov_setup(Ctx& c) {
     if (ph == 1) {
       w->stage[1] = 0;
       w->smem[1] = w->items_bytes[1];
-      if (w->smem[1] + meta <= smem_budget(2)) {
+      if (w->smem[1] + meta <= smem_budget(w->vel_minb)) {
         w->stage[1] |= ST_L0META;
         w->smem[1] += meta;
       }
-      if (w->smem[1] + col <= smem_budget(2)) {
+      if (w->smem[1] + col <= smem_budget(w->vel_minb)) {
         w->stage[1] |= ST_L0COL;
         w->smem[1] += col;
       }
-      const int occ2 = occupancy_any<false>(c.kmixed, 2, w->smem[1]);
+      const int occ2 = occupancy_any<false>(c.kmixed, w->vel_minb, w->smem[1]);
       if (occ2 * c.num_sms < G) {
         w->stage[1] = 0;
         w->smem[1] = w->items_bytes[1];
@@ -1875,12 +1861,11 @@ static pfem2_status solve_impl(Ctx& c, int which) {
   c.launches++;
   void* args[] = {&a};
   const void* kmg = w->mg_minb == 1 ? (const void*)k_krylov<R, true, 1> : (const void*)k_krylov<R, true, 2>;
-  if (mg)
-    PFEM2_CUDA(cudaLaunchCooperativeKernel(kmg, dim3(w->grid[ph]), dim3(kSolveThreads),
-                                           args, w->smem[ph], c.stream));
-  else
-    PFEM2_CUDA(cudaLaunchCooperativeKernel((const void*)k_krylov<R, false, 2>, dim3(w->grid[ph]), dim3(kSolveThreads),
-                                           args, w->smem[ph], c.stream));
+  // the Jacobi kernel: the velocity solves at vel_minb blocks per SM, a
+  // pressure solve without multigrid at two
+  const void* kj = (ph == 1 && w->vel_minb == 1) ? (const void*)k_krylov<R, false, 1> : (const void*)k_krylov<R, false, 2>;
+  PFEM2_CUDA(cudaLaunchCooperativeKernel(mg ? kmg : kj, dim3(w->grid[ph]), dim3(kSolveThreads), args, w->smem[ph],
+                                         c.stream));
   c.launches++;
   return PFEM2_OK;
 }

@@ -198,9 +198,12 @@ struct AdvectMinBlocks {
   static constexpr int value = DIM == 2 ? (sizeof(R) == 4 ? 4 : 2) : (sizeof(R) == 4 ? 2 : 1);
 };
 
-constexpr int kAdvWarps = 8;  // warps per block of the advection kernels (256 threads)
 
 constexpr int kAdvLeft = -2;  // advect_steps<.., false>: the particle left its cell
+
+// patches of at most this many cells are searched without the sort's
+// local-memory arrays
+constexpr int kSmallPatch = 8;
 
 // The reference's search for a point xn (cell-local frame of cell c, whose
 // record is G / L / x0) that left cell c (sort_particles_into_subdomains_and_
@@ -254,25 +257,10 @@ __device__ __forceinline__ bool locate_from(int& c, CellGeo<DIM, R>& G, LocalCel
     const int k0 = __ldg(v2c_ptr + gv);
     int nk = __ldg(v2c_ptr + gv + 1) - k0;
     if (nk > kMaxPatch) nk = kMaxPatch;
-    R key[kMaxPatch];
-    int perm[kMaxPatch];
-    for (int i = 0; i < nk; ++i) {
-      R sdot = R(0);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) sdot += __ldg(v2c_dir + (size_t)(k0 + i) * DIM + d) * vp[d];
-      key[i] = sdot;
-      // stable insertion by descending alignment (std::sort is an
-      // insertion sort, hence stable, for patches of <= 16 cells)
-      int j = i - 1;
-      while (j >= 0 && sdot > key[perm[j]]) {
-        perm[j + 1] = perm[j];
-        --j;
-      }
-      perm[j + 1] = i;
-    }
     bool found = false;
-    for (int i = 0; i < nk && !found; ++i) {
-      const int cc = __ldg(v2c_cell + k0 + perm[i]);
+    // the point in patch cell i (i in v2c order): on success the new cell
+    auto try_cell = [&](int i) {
+      const int cc = __ldg(v2c_cell + k0 + i);
       const CellGeo<DIM, R> Gc = geo[cc];
       LocalCell<DIM, R> Lc;
       double xc[DIM];
@@ -291,7 +279,51 @@ __device__ __forceinline__ bool locate_from(int& c, CellGeo<DIM, R>& G, LocalCel
           x[d] = x2[d];
         }
       }
+    };
+    auto align = [&](int i) {
+      R sdot = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) sdot += __ldg(v2c_dir + (size_t)(k0 + i) * DIM + d) * vp[d];
+      return sdot;
+    };
+    if (nk <= kSmallPatch) {
+      // small patches: the cells are tried in order by repeated selection of
+      // the best aligned remaining one (the lowest index among equal
+      // alignments), which is the order of the stable sort below without
+      // its local-memory arrays; the alignments are recomputed per round
+      // from cached loads, and usually the first cell tried holds the point
+      unsigned left = (1u << nk) - 1u;
+      while (left && !found) {
+        int bi = -1;
+        R bk = R(0);
+        for (int i = 0; i < nk; ++i) {
+          if (!((left >> i) & 1u)) continue;
+          const R k = align(i);
+          if (bi < 0 || k > bk) {
+            bi = i;
+            bk = k;
+          }
+        }
+        left &= ~(1u << bi);
+        try_cell(bi);
+      }
+      return found;
     }
+    R key[kMaxPatch];
+    int perm[kMaxPatch];
+    for (int i = 0; i < nk; ++i) {
+      const R sdot = align(i);
+      key[i] = sdot;
+      // stable insertion by descending alignment (std::sort is an
+      // insertion sort, hence stable, for patches of <= 16 cells)
+      int j = i - 1;
+      while (j >= 0 && sdot > key[perm[j]]) {
+        perm[j + 1] = perm[j];
+        --j;
+      }
+      perm[j + 1] = i;
+    }
+    for (int i = 0; i < nk && !found; ++i) try_cell(perm[i]);
     return found;
   }
 }
@@ -362,75 +394,6 @@ __device__ __forceinline__ int advect_steps(int c0, R* x, R dts, int s0, int& s_
       for (int d = 0; d < DIM; ++d) vv[v][d] = __ldg(Vr + (size_t)d * nv + gvx[v]);
   }
   return c;
-}
-
-// Advection, first kernel: the particles of a contiguous chunk per block;
-// with FUSE the FLIP correction (correct_particles_velocities) is applied
-// and stored for every particle. A particle that stays in its cell for all
-// sub-steps is finished here; one that leaves is appended, unfinished, to
-// its warp's region of the queue with the sub-step it left in, its
-// reference coordinates stored as they were before that sub-step (the second
-// kernel resumes there with the same arithmetic, so the result does not
-// depend on this split). Warps whose lanes all stay never run the patch
-// search.
-template <int DIM, typename R, bool FUSE>
-__global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect(
-    const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
-    const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
-    const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
-    const int* __restrict__ cell_inst, int* __restrict__ queue, unsigned char* __restrict__ qstep,
-    int* __restrict__ wcount) {
-  constexpr int NV = Dims<DIM>::NV;
-  const int n = min(*d_np, (int)cap);
-  const int chunk = (n + gridDim.x - 1) / gridDim.x;
-  const int wcap = ((chunk + 255) / 256) * 32;  // particles one warp handles at most
-  const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int* wq = queue + ((size_t)blockIdx.x * kAdvWarps + warp) * wcap;
-  int nq = 0;
-  for (int base = lo; base < hi; base += 256) {
-    const int p = base + threadIdx.x;
-    bool leave = false;
-    int s_left = 0;
-    if (p < hi) {
-      const int c0 = cell[p];
-      R x[DIM], up[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        x[d] = xi[d * cap + p];
-        up[d] = u[d * cap + p];
-      }
-      if (FUSE) {
-        R N[NV];
-        shape_values<DIM, R>(x, N);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const int g = __ldg(cv + (size_t)c0 * NV + v);
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
-        }
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) u[d * cap + p] = up[d];
-      }
-      const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
-      const int c = advect_steps<DIM, R, false>(c0, x, dts, 0, s_left, S, geo, cv, Vr, nv, nullptr, nullptr, nullptr);
-      if (c == kAdvLeft) {
-        leave = true;
-      } else {
-        newcell[p] = c;
-      }
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
-    }
-    const unsigned m = __ballot_sync(PFEM2_FULL_MASK, leave);
-    if (leave) {
-      const size_t q = (size_t)(wq - queue) + nq + __popc(m & lanemask_lt());
-      queue[q] = p;
-      qstep[q] = (unsigned char)s_left;
-    }
-    nq += __popc(m);
-  }
-  if (lane == 0) wcount[(size_t)blockIdx.x * kAdvWarps + warp] = nq;
 }
 
 // deletion count and far movers of one advected particle (c: its new cell,
@@ -505,47 +468,107 @@ __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_
   }
 }
 
-// Advection, second kernel: the queued particles (a warp per queue region),
-// sub-steps redone from their start with the full point location; deletion
-// count and far movers (left the 1-ring of the old cell) recorded here.
-// In 2D FP32 the registers are capped for four resident blocks (its point
-// location is bound by dependent loads: 5% faster than the three blocks 78
-// registers allowed); the 3D and FP64 forms keep their registers.
-template <int DIM, typename R>
-__global__ void __launch_bounds__(256, (DIM == 2 && sizeof(R) == 4) ? 4 : 1) k_advect_left(
-    const int* __restrict__ cell, R* __restrict__ xi, int* __restrict__ newcell, size_t cap,
-    const int* __restrict__ d_np, int fast_grid, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
-    const R* __restrict__ Vr, int nv, int S, const DevInst* __restrict__ inst, const int* __restrict__ cell_inst,
-    const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell, const R* __restrict__ v2c_dir,
-    const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell, const int* __restrict__ queue,
-    const unsigned char* __restrict__ qstep, const int* __restrict__ wcount,
-    unsigned long long* __restrict__ far_keys, int far_cap,
-    int* __restrict__ counters, unsigned* __restrict__ dest_mask) {
+// Advection in two phases per warp (large particle sets): a warp walks its
+// 32-particle slices of the block's contiguous chunk; every particle is
+// corrected (FUSE) and takes the lean sub-steps while it stays in its cell,
+// and one that leaves is appended to the warp's queue in shared memory with
+// its state (slot, old cell, the sub-step it left in, its reference
+// coordinates at the start of that sub-step). Whenever the queue holds 32
+// particles the warp resumes them with the full point location, so that the
+// divergent patch search runs on full warps, the leavers' state never goes
+// back to memory and the warps stay independent of each other (no block
+// barrier). The arithmetic is that of k_advect_one (bitwise equal results).
+constexpr int kAdvThreads = 256;
+
+template <int DIM, typename R, bool FUSE>
+__global__ void __launch_bounds__(kAdvThreads, AdvectMinBlocks<DIM, R>::value) k_advect_q(
+    const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,
+    const int* __restrict__ d_np, const CellGeo<DIM, R>* __restrict__ geo, const int* __restrict__ cv,
+    const R* __restrict__ Vr, const R* __restrict__ dVr, int nv, int S, const DevInst* __restrict__ inst,
+    const int* __restrict__ cell_inst, const int* __restrict__ v2c_ptr, const int* __restrict__ v2c_cell,
+    const R* __restrict__ v2c_dir, const int* __restrict__ ring_ptr, const int* __restrict__ ring_cell,
+    unsigned long long* __restrict__ far_keys, int far_cap, int* __restrict__ counters, unsigned* __restrict__ dest_mask) {
+  constexpr int NV = Dims<DIM>::NV;
+  constexpr int NW = kAdvThreads / 32;
+  constexpr int QN = 64;  // below 32 left over + 32 appended
+  __shared__ int q_p[NW][QN], q_c[NW][QN];
+  __shared__ R q_x[NW][DIM][QN];
+  __shared__ unsigned char q_s[NW][QN];
   const int n = min(*d_np, (int)cap);
-  const int chunk = (n + fast_grid - 1) / fast_grid;
-  const int wcap = ((chunk + 255) / 256) * 32;
-  const int lane = threadIdx.x & 31;
-  const int nreg = fast_grid * kAdvWarps;
-  for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < nreg;
-       r += (int)((gridDim.x * blockDim.x) >> 5)) {
-    const int cnt = wcount[r];
-    for (int i = lane; i < cnt; i += 32) {
-      const size_t q = (size_t)r * wcap + i;
-      const int p = queue[q];
-      const int s0 = qstep[q];
-      const int c0 = cell[p];
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int nq = 0;  // the warp's queued particles (uniform over the warp)
+  for (int base = lo + warp * 32;; base += kAdvThreads) {
+    const bool more = base < hi;  // uniform over the warp
+    if (more) {
+      const int p = base + lane;
+      bool leave = false;
+      int s_left = 0, c0 = 0;
       R x[DIM];
+      if (p < hi) {
+        c0 = cell[p];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) x[d] = xi[d * cap + p];
-      const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
-      int s_left = 0;
-      int c = advect_steps<DIM, R, true>(c0, x, dts, s0, s_left, S, geo, cv, Vr, nv, v2c_ptr, v2c_cell, v2c_dir);
-      if (c < 0) c = -1;
-      advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters, dest_mask);
-      newcell[p] = c;
+        for (int d = 0; d < DIM; ++d) x[d] = xi[d * cap + p];
+        if (FUSE) {
+          R N[NV], up[DIM];
+          shape_values<DIM, R>(x, N);
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
+          for (int d = 0; d < DIM; ++d) up[d] = u[d * cap + p];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            const int g = __ldg(cv + (size_t)c0 * NV + v);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) up[d] = up[d] + N[v] * __ldg(dVr + (size_t)d * nv + g);
+          }
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) u[d * cap + p] = up[d];
+        }
+        const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
+        const int c = advect_steps<DIM, R, false>(c0, x, dts, 0, s_left, S, geo, cv, Vr, nv, nullptr, nullptr, nullptr);
+        if (c == kAdvLeft) {
+          leave = true;
+        } else {
+          newcell[p] = c;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
+        }
+      }
+      const unsigned m = __ballot_sync(PFEM2_FULL_MASK, leave);
+      if (leave) {
+        const int k = nq + __popc(m & lanemask_lt());
+        q_p[warp][k] = p;
+        q_c[warp][k] = c0;
+        q_s[warp][k] = (unsigned char)s_left;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) q_x[warp][d][k] = x[d];
+      }
+      nq += __popc(m);
     }
+    __syncwarp();
+    // resume 32 queued particles at a time (after the last slice: all),
+    // from the top of the queue; the order does not change any result
+    while (nq >= 32 || (!more && nq > 0)) {
+      const int k = nq - 32 + lane;
+      if (k >= 0) {
+        const int p = q_p[warp][k], c0 = q_c[warp][k];
+        R x[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) x[d] = q_x[warp][d][k];
+        const R dts = R(inst[__ldg(cell_inst + c0)].dt_sub);
+        int s_left = 0;
+        int c = advect_steps<DIM, R, true>(c0, x, dts, (int)q_s[warp][k], s_left, S, geo, cv, Vr, nv, v2c_ptr,
+                                           v2c_cell, v2c_dir);
+        if (c < 0) c = -1;
+        advect_record(p, c0, c, ring_ptr, ring_cell, far_keys, far_cap, counters, dest_mask);
+        newcell[p] = c;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xi[d * cap + p] = x[d];
+      }
+      nq = nq > 32 ? nq - 32 : 0;
+      __syncwarp();  // the resumed entries are read before the next slice appends over them
+    }
+    if (!more) break;
   }
 }
 
@@ -762,7 +785,6 @@ pfem2_status far_sort_setup(Ctx& c) {
 template <int DIM, typename R>
 static pfem2_status advect_impl(Ctx& c, bool fuse) {
   int b = c.cur;
-  const int G = c.adv_grid;
   int S = c.cfg.movement_steps;
   const bool split = c.tune.advect_split ? c.tune.advect_split == 2 : (long long)c.pcap >= c.adv_split_min;
   if (!split) {
@@ -781,22 +803,21 @@ static pfem2_status advect_impl(Ctx& c, bool fuse) {
           c.dest_mask);
     c.launches++;
   } else {
-  if (fuse)
-    k_advect<DIM, R, true><<<G, 256, 0, c.stream>>>(
-        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
-        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
-        c.adv_queue, c.adv_qstep, c.adv_wcount);
-  else
-    k_advect<DIM, R, false><<<G, 256, 0, c.stream>>>(
-        c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
-        (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
-        c.adv_queue, c.adv_qstep, c.adv_wcount);
-  c.launches++;
-  k_advect_left<DIM, R><<<G, 256, 0, c.stream>>>(
-      c.pcell[b], (R*)c.pxi[b], c.newcell, (size_t)c.pcap, c.d_np + b, G, (const CellGeo<DIM, R>*)c.cell_geo, c.cv,
-      (const R*)c.Vr, c.nv, S, c.d_inst, c.cell_inst, c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr,
-      c.ring_cell, c.adv_queue, c.adv_qstep, c.adv_wcount, c.far_keys, c.far_cap, c.d_counters, c.dest_mask);
-  c.launches++;
+    // the queue kernel's blocks walk contiguous chunks
+    const int grid = grid_for(c, c.pcap, kAdvThreads, c.tune.advect_blocks_per_sm);
+    if (fuse)
+      k_advect_q<DIM, R, true><<<grid, kAdvThreads, 0, c.stream>>>(
+          c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
+          (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
+          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters,
+          c.dest_mask);
+    else
+      k_advect_q<DIM, R, false><<<grid, kAdvThreads, 0, c.stream>>>(
+          c.pcell[b], (R*)c.pxi[b], (R*)c.pu[b], c.newcell, (size_t)c.pcap, c.d_np + b,
+          (const CellGeo<DIM, R>*)c.cell_geo, c.cv, (const R*)c.Vr, (const R*)c.dVr, c.nv, S, c.d_inst, c.cell_inst,
+          c.v2c_ptr, c.v2c_cell, (const R*)c.v2c_dir_r, c.ring_ptr, c.ring_cell, c.far_keys, c.far_cap, c.d_counters,
+          c.dest_mask);
+    c.launches++;
   }
   k_far_sort<<<1, 1024, sizeof(unsigned long long) * c.far_cap, c.stream>>>(c.far_keys, c.d_counters, c.far_cap);
   c.launches++;
@@ -889,7 +910,7 @@ __device__ __forceinline__ void proj_store(ProjAcc<DIM, R>& acc, R* __restrict__
 // For FP32 coordinates xi * q is exact in FP64, so that happens only when
 // it is an integer; for FP64 coordinates a relative 1e-12 decides.
 template <typename R>
-__device__ __forceinline__ int sub_bucket(R xr, double h, int q) {
+__device__ __forceinline__ int sub_bucket_fp64(R xr, double h, int q) {
   const double xi = (double)xr;
   double t = xi * (double)q;
   if (sizeof(R) == 4) {
@@ -900,6 +921,34 @@ __device__ __forceinline__ int sub_bucket(R xr, double h, int q) {
   if (!(t >= 0.0)) t = 0.0;
   if (t > (double)q) t = (double)q;
   return (int)(unsigned)t;
+}
+
+template <typename R>
+__device__ __forceinline__ int sub_bucket(R xr, double h, int q) {
+  return sub_bucket_fp64<R>(xr, h, q);
+}
+
+// FP32 coordinates: for 0 < xi < 1, xi = m 2^-s with the 24-bit significand
+// m and s = 150 - (biased exponent) >= 24, so xi q = (m q) 2^-s exactly in
+// 64-bit integers (q < 2^16): its integer part is the bucket unless xi q
+// is itself an integer, where the quotient xi / h decides (the FP64 form,
+// as for 0, 1 and anything outside (0, 1)). Same results as the FP64 form,
+// with integer instructions only.
+template <>
+__device__ __forceinline__ int sub_bucket<float>(float xr, double h, int q) {
+  const unsigned b = __float_as_uint(xr);
+  if (b - 1u < 0x3f7fffffu) {  // 0 < xi < 1 (positive, below the bits of 1.0f)
+    const int e = (int)(b >> 23);
+    if (e == 0) return 0;  // subnormal: 0 < xi q < 1
+    const int sh = 150 - e;
+    if (sh < 64) {
+      const unsigned long long prod = (unsigned long long)((b & 0x7fffffu) | 0x800000u) * (unsigned)q;
+      if (prod & ((1ull << sh) - 1ull)) return (int)(prod >> sh);
+    } else {
+      return 0;  // xi < 2^-40: 0 < xi q < 1
+    }
+  }
+  return sub_bucket_fp64<float>(xr, h, q);
 }
 
 // t / q for t, q < 2^16 with qm = ceil(2^32 / q)

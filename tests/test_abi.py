@@ -128,3 +128,19 @@ def test_cpp_shim_compiles_and_links():
 def test_abi_version_mirror_matches_header():
     hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pfem2.h")).read()
     assert int(re.search(r"#define PFEM2_ABI_VERSION (\d+)", hdr).group(1)) == A.ABI_VERSION
+
+
+def test_tuning_cache_reader_accepts_both_line_forms(tmp_path):
+    """cache lines with five launch-shape values (no velocity blocks per SM)
+    and with six read back the same way; the time is recognised by its
+    decimal point"""
+    from pfem2_b200 import autotune
+    p = tmp_path / "c.txt"
+    p.write_text("# comment\n"
+                 "DEV 2 4 15 0 16 2 8 16 1 2.5656\n"
+                 "DEV 2 -1 15 0 16 2 6 16 1 1 2.6834\n"
+                 "DEV 3 4 20 0 8 1 4 8 2\n")
+    c = autotune.read_cache(str(p))
+    assert c["DEV 2 4 15 0"] == (dict(zip(A.TUNING_FIELDS, [16, 2, 8, 16, 1, 0])), 2.5656)
+    assert c["DEV 2 -1 15 0"] == (dict(zip(A.TUNING_FIELDS, [16, 2, 6, 16, 1, 1])), 2.6834)
+    assert c["DEV 3 4 20 0"] == (dict(zip(A.TUNING_FIELDS, [8, 1, 4, 8, 2, 0])), None)

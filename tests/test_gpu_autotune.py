@@ -66,17 +66,19 @@ def test_particle_shapes_do_not_change_results():
 
 
 def test_solver_shapes_within_tolerance():
-    """velocity tile size and pressure blocks per SM: same solution to the
-    solver tolerance (1e-13 / 1e-12 absolute in this spec)"""
+    """velocity tile size and blocks per SM, pressure blocks per SM: same
+    solution to the solver tolerance (1e-13 / 1e-12 absolute in this spec)"""
     sp = spec_2d(dt=0.01)
-    a = run(sp, {"vel_tile_slices": 1, "p_blocks_per_sm": 1})
-    b = run(sp, {"vel_tile_slices": 8, "p_blocks_per_sm": 2})
+    a = run(sp, {"vel_tile_slices": 1, "p_blocks_per_sm": 1, "vel_blocks_per_sm": 1})
+    b = run(sp, {"vel_tile_slices": 8, "p_blocks_per_sm": 2, "vel_blocks_per_sm": 2})
     assert a[2]["vel_tile_slices"] == 1 and b[2]["p_blocks_per_sm"] == 2
+    assert a[2]["vel_blocks_per_sm"] == 1 and b[2]["vel_blocks_per_sm"] == 2
     for x, y in zip(a[0], b[0]):
         assert rel_l2(x, y) <= 1e-9
 
 
 def test_bad_tuning_rejected():
     sp = spec_2d()
-    with pytest.raises(Exception):
-        Solver(sp, tuning={"p_blocks_per_sm": 3})
+    for bad in ({"p_blocks_per_sm": 3}, {"vel_blocks_per_sm": 3}, {"advect_split": 5}):
+        with pytest.raises(Exception):
+            Solver(sp, tuning=bad)
