@@ -8,7 +8,8 @@ solves' tile size (SELL slices per tile) and blocks per SM, and the blocks
 per SM of a single pressure system's multigrid solve. `tune` times whole
 steps (the device time of every stage,
 CUDA events inside the library) for candidate shapes by coordinate descent
-and appends the fastest to a cache file under the context's key: device
+(coupled knobs, such as the advection grid and its one- or two-phase form,
+over all their combinations) and appends the fastest to a cache file under the context's key: device
 name, dim, FP32 stages, log2 cells, log2 instances (pfem2_tuning_key). A
 later context with the same key reads the entry at pfem2_setup when the
 environment variable PFEM2_TUNING_CACHE names the file; fields the caller
@@ -87,7 +88,25 @@ def tune(specs, space=None, steps=5, warmup=2, cache=None, rounds=1, prepare=Non
             os.environ["PFEM2_TUNING_CACHE"] = saved
 
 
+# knobs whose best values depend on each other are searched together (every
+# combination), the others one at a time
+COUPLED = [("advect_blocks_per_sm", "advect_split"), ("vel_tile_slices", "vel_blocks_per_sm")]
+
+
+def _groups(space):
+    groups, done = [], set()
+    for grp in COUPLED:
+        g = tuple(k for k in grp if k in space)
+        if g:
+            groups.append(g)
+            done.update(g)
+    groups += [(k,) for k in space if k not in done]
+    return groups
+
+
 def _tune(specs, space, steps, warmup, cache, rounds, prepare, solver_kw):
+    import itertools
+
     t0, best = measure(specs, None, steps, warmup, prepare=prepare, **solver_kw)
     if t0 is None:
         raise RuntimeError("the automatic launch shapes failed")
@@ -98,11 +117,11 @@ def _tune(specs, space, steps, warmup, cache, rounds, prepare, solver_kw):
     best_t = t0
     trials = [({k: best[k] for k in best}, t0)]
     for _ in range(rounds):
-        for knob, values in space.items():
-            for v in values:
-                if best.get(knob) == v:
+        for grp in _groups(space):
+            for combo in itertools.product(*(space[k] for k in grp)):
+                if all(best.get(k) == v for k, v in zip(grp, combo)):
                     continue
-                cand = dict(best, **{knob: v})
+                cand = dict(best, **dict(zip(grp, combo)))
                 t, resolved = measure(specs, cand, steps, warmup, prepare=prepare, **solver_kw)
                 trials.append((cand, t))
                 if t is not None and t < best_t:

@@ -207,7 +207,7 @@ static pfem2_status check_tuning(const pfem2_tuning& t) {
 // --------------------------------------------------------------- setup
 static pfem2_status do_setup(Ctx& c) {
   apply_tuning_cache(c);
-  if (!c.tune.advect_blocks_per_sm) c.tune.advect_blocks_per_sm = 8;
+  if (!c.tune.advect_blocks_per_sm) c.tune.advect_blocks_per_sm = 16;
   if (!c.tune.rebin_blocks_per_sm) c.tune.rebin_blocks_per_sm = 8;
   const int dim = c.dim, NV = 1 << dim, NF = 2 * dim;
   // offsets

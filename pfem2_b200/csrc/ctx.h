@@ -137,11 +137,11 @@ struct Ctx {
   void* pu[2] = {};
   int cur = 0;
   int* newcell = nullptr;
-  // particle capacity from which the advection runs in two phases per
-  // block (stayers, then the block's queued leavers; on small particle sets
-  // the one-pass kernel is as fast); the environment variable
-  // PFEM2_ADVECT_SPLIT_MIN overrides it at creation
-  long long adv_split_min = 1LL << 23;
+  // particle capacity from which the advection runs in two phases per warp
+  // (stayers, then the warp's queued leavers; measured faster than the
+  // one-pass kernel on every bench workload, the smallest 1.3M particles);
+  // the environment variable PFEM2_ADVECT_SPLIT_MIN overrides it at creation
+  long long adv_split_min = 0;
   int* cell_start[2] = {};
   unsigned long long* rebin_tiles = nullptr;  // ticket + status words of the rebin's single-pass scan
   int* d_np = nullptr;       // [2] particle count of buffer 0/1

@@ -50,7 +50,7 @@ def test_tuner_writes_and_library_reads_cache(tmp_path, monkeypatch):
     s.close()
     # another key (FP64) finds no entry: automatic shapes
     s = Solver(sp, precision=A.PREC_FP64)
-    assert s.tuning_key() != res["key"] and s.tuning()["advect_blocks_per_sm"] == 8
+    assert s.tuning_key() != res["key"] and s.tuning()["advect_blocks_per_sm"] == 16
     s.close()
 
 

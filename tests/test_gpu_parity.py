@@ -319,9 +319,9 @@ def test_ensemble_batch_matches_oracle():
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_advect_split_equals_one_kernel(monkeypatch, prec):
-    """the two-kernel advection (used from ~8M particle slots: fast sub-steps,
-    then the particles that left their cell) equals the one-kernel form bit
-    for bit; forced here on a small case through PFEM2_ADVECT_SPLIT_MIN"""
+    """the two-phase advection (the default: lean sub-steps, then each warp's
+    queued particles that left their cell) equals the one-pass form bit for
+    bit; both chosen here through PFEM2_ADVECT_SPLIT_MIN"""
     sp = spec_2d(dt=0.02)
     outs = []
     for split_min in ("0", str(1 << 40)):
