@@ -27,12 +27,15 @@ namespace pfem2 {
 constexpr int kRebinWarps = 8;
 constexpr int kMaxBuckets = 256;
 // resident rebin blocks per SM the registers are capped for: the kernel is
-// bound by dependent loads; in 2D FP32 six blocks (48 warps) measured 17%
-// faster than the four that 64 registers allowed, in 3D FP32 four blocks 36%
-// faster than uncapped, each at a few spilled bytes; FP64 is not capped
+// bound by dependent loads, so resident warps pay more than registers; in 2D
+// FP32 six blocks (48 warps) measured 17% faster than the four that 64
+// registers allowed, in 3D FP32 four blocks 36% faster than uncapped; with
+// FP64 particles five blocks in 2D (0.186 -> 0.110 ms on the 52k-cell
+// channel against two uncapped, 96 registers) and three in 3D (3.15 -> 1.61
+// ms on the 442k-cell pipe against one, 181 registers)
 template <int DIM, typename R>
 struct RebinMinBlocks {
-  static constexpr int value = sizeof(R) == 4 ? (DIM == 2 ? 6 : 4) : 1;
+  static constexpr int value = sizeof(R) == 4 ? (DIM == 2 ? 6 : 4) : (DIM == 2 ? 5 : 3);
 };
 
 // ------------------------------------------------------------------ seed
@@ -192,10 +195,13 @@ pfem2_status launch_correct(Ctx& c) {
 // particle found nowhere is deleted (newcell = -1).
 // resident 256-thread blocks per SM the advection kernel is compiled for:
 // it is latency-bound, so the FP32 2D variant trades its few extra
-// registers for four blocks (32 warps) per SM
+// registers for four blocks (32 warps) per SM, and the FP64 3D variant
+// (240 registers uncapped, one block) runs two at 128 registers in spite of
+// its spills (2.72 -> 2.40 ms on the 442k-cell pipe; three: 4.0 ms); the
+// FP64 2D variant measured slower with three than with two
 template <int DIM, typename R>
 struct AdvectMinBlocks {
-  static constexpr int value = DIM == 2 ? (sizeof(R) == 4 ? 4 : 2) : (sizeof(R) == 4 ? 2 : 1);
+  static constexpr int value = DIM == 2 ? (sizeof(R) == 4 ? 4 : 2) : 2;
 };
 
 
