@@ -266,8 +266,11 @@ template <typename R, bool MG, int MINB>
 __global__ void __launch_bounds__(kSolveThreads, MINB) k_krylov(SolveArgs<R> a) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   // entries of a SELL row (and of a long restriction row) whose loads are
-  // issued together: more with one block per SM, which has the registers
-  constexpr int CH = MINB == 1 ? 16 : 8;
+  // issued together: more with one block per SM, which has the registers;
+  // with two, nine: a Q1 row of 9 entries (2D) in one round of loads and one
+  // of 27 (3D) in three (eight took two and four: channel velocity solves
+  // 0.64 -> 0.61 ms, pipe 31.0 -> 26.9 ms per step)
+  constexpr int CH = MINB == 1 ? 16 : 9;
   // partial sums per work item: the multigrid path (CG) needs 2
   constexpr int NSMAX = MG ? 2 : kMaxSums;
   const int NS = MG ? 2 : a.nsum;
