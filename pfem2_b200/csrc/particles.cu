@@ -8,7 +8,8 @@
 //   k_seed          seed_particles / seed_particles_into_cell
 //                   (TurekBenchmark/pfem2particle.cpp:701-721,774-790)
 //   k_correct       correct_particles_velocities (:792-811)
-//   k_advect        move_particles sub-steps (:813-848) + point location
+//   k_advect_q,     move_particles sub-steps (:813-848) + point location
+//   k_advect_one
 //                   sort_particles_into_subdomains_and_cells (:276-507),
 //                   find_closest_vertex_of_cell (:142-166),
 //                   compare_particle_association (:268-274)
@@ -431,9 +432,9 @@ __device__ __forceinline__ void advect_record(int p, int c0, int c, const int* _
   }
 }
 
-// Advection in one kernel (used below a particle count where the two-kernel
-// split does not pay for its second pass): correction, every sub-step with
-// the full point location. Same arithmetic as the split.
+// Advection in one pass (selectable with advect_split = 1 or below
+// PFEM2_ADVECT_SPLIT_MIN slots): correction, every sub-step with the full
+// point location in line. Same arithmetic as the two-phase form.
 template <int DIM, typename R, bool FUSE>
 __global__ void __launch_bounds__(256, AdvectMinBlocks<DIM, R>::value) k_advect_one(
     const int* __restrict__ cell, R* __restrict__ xi, R* __restrict__ u, int* __restrict__ newcell, size_t cap,

@@ -144,3 +144,41 @@ def test_tuning_cache_reader_accepts_both_line_forms(tmp_path):
     assert c["DEV 2 4 15 0"] == (dict(zip(A.TUNING_FIELDS, [16, 2, 8, 16, 1, 0])), 2.5656)
     assert c["DEV 2 -1 15 0"] == (dict(zip(A.TUNING_FIELDS, [16, 2, 6, 16, 1, 1])), 2.6834)
     assert c["DEV 3 4 20 0"] == (dict(zip(A.TUNING_FIELDS, [8, 1, 4, 8, 2, 0])), None)
+
+
+def test_tuner_searches_coupled_knobs_together(monkeypatch):
+    """the advection grid and its one- or two-phase form (and the velocity
+    tile and blocks per SM) are tried over all their combinations, the other
+    knobs one at a time; measured here with a stand-in for the GPU timing"""
+    from pfem2_b200 import autotune
+
+    space = {"advect_blocks_per_sm": [2, 16], "advect_split": [1, 2], "rebin_blocks_per_sm": [4, 8]}
+    assert autotune._groups(space) == [("advect_blocks_per_sm", "advect_split"), ("rebin_blocks_per_sm",)]
+
+    # a landscape with a coupled optimum: one pass is best at 2 blocks per
+    # SM, two phases at 16 blocks per SM and overall
+    cost = {(2, 1): 3.0, (16, 1): 4.0, (2, 2): 5.0, (16, 2): 1.0}
+    tried = []
+
+    def fake_measure(specs, tuning, steps, warmup, prepare=None, **kw):
+        t = dict({"advect_blocks_per_sm": 2, "advect_split": 1, "rebin_blocks_per_sm": 8}, **(tuning or {}))
+        tried.append((t["advect_blocks_per_sm"], t["advect_split"], t["rebin_blocks_per_sm"]))
+        ms = cost[(t["advect_blocks_per_sm"], t["advect_split"])] + (0.1 if t["rebin_blocks_per_sm"] == 8 else 0.0)
+        return ms, dict(t, vel_tile_slices=0, p_blocks_per_sm=0, vel_blocks_per_sm=0)
+
+    class FakeSolver:
+        def __init__(self, *a, **k):
+            pass
+
+        def tuning_key(self):
+            return "DEV 2 4 15 0"
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(autotune, "measure", fake_measure)
+    monkeypatch.setattr(autotune, "Solver", FakeSolver)
+    res = autotune.tune([None], space=space, steps=1, warmup=0)
+    assert res["tuning"]["advect_blocks_per_sm"] == 16 and res["tuning"]["advect_split"] == 2
+    assert res["tuning"]["rebin_blocks_per_sm"] == 4
+    assert (16, 2, 8) in tried  # the coupled corner one knob at a time would not reach
