@@ -757,7 +757,11 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": threads, "kind": "port",
                          "sample": f"{n} whole time steps (of {args.steps} requested, 120 s cap) after "
                                    f"{warm} warm-up steps (of {args.warmup} requested); deal.II, which the "
-                                   f"reference needs, is not installed, so its FP64 CPU restatement runs"},
+                                   f"reference needs, is not installed, so its FP64 CPU restatement runs",
+                         "parallel_parts": "OpenMP over particle advection, right-hand sides, SpMV and the Krylov "
+                                           "vector operations; the pressure's SSOR preconditioner is sequential "
+                                           "(as deal.II's), which bounds the scaling (8-core host: 0.45 "
+                                           "timesteps/s on 1 thread, 0.90 on 4, 0.95 on 8)"},
         "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(res), flush=True)

@@ -933,13 +933,29 @@ void or_assemble_matrices(omodel* m) {
   m->assembled = 1;
 }
 
+/* The right-hand sides are assembled cell by cell. Each cell's local vector
+ * goes to a per-cell buffer (cells in parallel), and each vertex then sums
+ * its cells' entries in ascending cell order (vertices in parallel): the
+ * additions of the serial scatter rhs[cv[c][i]] += loc[i] over ascending c,
+ * in the same order, so the result does not depend on the thread count. */
+static double* cell_buffer(const omodel* m) { return (double*)xcalloc((size_t)m->nc * m->nvc, sizeof(double)); }
+static void gather_cells(const omodel* m, const double* lbuf, double* rhs) {
+#pragma omp parallel for schedule(static) num_threads(m->threads)
+  for (int v = 0; v < m->nv; ++v) {
+    double s = 0.0;
+    for (int k = m->v2c_ptr[v]; k < m->v2c_ptr[v + 1]; ++k) s += lbuf[(size_t)m->v2c_cell[k] * m->nvc + m->v2c_loc[k]];
+    rhs[v] = s;
+  }
+}
+
 /* prediction rhs of component comp */
 static void rhs_prediction(const omodel* m, int comp, const double* const* old, const double* const* inner, double* rhs) {
   int dim = m->dim, nvc = m->nvc;
   double mu = m->cs.mu, rho = m->cs.rho, dt = m->cs.dt;
-  memset(rhs, 0, sizeof(double) * m->nv);
-  qpoint qs[8];
+  double* lbuf = cell_buffer(m);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
   for (int c = 0; c < m->nc; ++c) {
+    qpoint qs[8];
     const int* cvv = m->cv + (size_t)c * nvc;
     double loc[MAXV] = {0};
     int nq = cell_qpoints(m, c, qs);
@@ -981,16 +997,19 @@ static void rhs_prediction(const omodel* m, int comp, const double* const* old, 
         for (int i = 0; i < nvc; ++i) loc[i] += mu * dt * q->N[i] * T * q->n[0] * q->JxW;
       }
     }
-    for (int i = 0; i < nvc; ++i) rhs[cvv[i]] += loc[i];
+    for (int i = 0; i < nvc; ++i) lbuf[(size_t)c * nvc + i] = loc[i];
   }
+  gather_cells(m, lbuf, rhs);
+  free(lbuf);
 }
 
 static void rhs_pressure(const omodel* m, const double* const* pred, double* rhs) {
   int dim = m->dim, nvc = m->nvc;
   double rho = m->cs.rho, dt = m->cs.dt, G = m->cs.open_boundary_pressure_flux;
-  memset(rhs, 0, sizeof(double) * m->nv);
-  qpoint qs[8];
+  double* lbuf = cell_buffer(m);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
   for (int c = 0; c < m->nc; ++c) {
+    qpoint qs[8];
     const int* cvv = m->cv + (size_t)c * nvc;
     double loc[MAXV] = {0};
     int nq = cell_qpoints(m, c, qs);
@@ -1017,16 +1036,19 @@ static void rhs_pressure(const omodel* m, const double* const* pred, double* rhs
         }
       }
     }
-    for (int i = 0; i < nvc; ++i) rhs[cvv[i]] += loc[i];
+    for (int i = 0; i < nvc; ++i) lbuf[(size_t)c * nvc + i] = loc[i];
   }
+  gather_cells(m, lbuf, rhs);
+  free(lbuf);
 }
 
 static void rhs_correction(const omodel* m, int comp, const double* p, double* rhs) {
   int dim = m->dim, nvc = m->nvc;
   double rho = m->cs.rho, dt = m->cs.dt;
-  memset(rhs, 0, sizeof(double) * m->nv);
-  qpoint qs[8];
+  double* lbuf = cell_buffer(m);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
   for (int c = 0; c < m->nc; ++c) {
+    qpoint qs[8];
     const int* cvv = m->cv + (size_t)c * nvc;
     double loc[MAXV] = {0};
     int nq = cell_qpoints(m, c, qs);
@@ -1036,8 +1058,10 @@ static void rhs_correction(const omodel* m, int comp, const double* p, double* r
         for (int j = 0; j < nvc; ++j)
           loc[i] -= dt / rho * q->N[i] * q->G[j * dim + comp] * p[cvv[j]] * q->JxW;
     }
-    for (int i = 0; i < nvc; ++i) rhs[cvv[i]] += loc[i];
+    for (int i = 0; i < nvc; ++i) lbuf[(size_t)c * nvc + i] = loc[i];
   }
+  gather_cells(m, lbuf, rhs);
+  free(lbuf);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1056,14 +1080,38 @@ static double dot(int n, const double* a, const double* b) {
   for (int i = 0; i < n; ++i) s += a[i] * b[i];
   return s;
 }
+/* the Krylov solvers' dot product: in index order with one thread; with
+ * more, chunks of 4096 entries summed in parallel (each in index order) and
+ * then in chunk order, so that the result is the same for every thread
+ * count above one */
+enum { kDotChunk = 4096 };
+static double dot_m(const omodel* m, int n, const double* a, const double* b) {
+  if (m->threads <= 1) return dot(n, a, b);
+  const int nch = (n + kDotChunk - 1) / kDotChunk;
+  double* part = (double*)xcalloc(nch > 0 ? nch : 1, sizeof(double));
+#pragma omp parallel for schedule(static) num_threads(m->threads)
+  for (int ch = 0; ch < nch; ++ch) {
+    const int i1 = (ch + 1) * kDotChunk < n ? (ch + 1) * kDotChunk : n;
+    double s = 0.0;
+    for (int i = ch * kDotChunk; i < i1; ++i) s += a[i] * b[i];
+    part[ch] = s;
+  }
+  double s = 0.0;
+  for (int ch = 0; ch < nch; ++ch) s += part[ch];
+  free(part);
+  return s;
+}
 
 /* precond: 0 = Jacobi, 1 = SSOR (omega 1, symmetric Gauss-Seidel) */
 static void precond(const omodel* m, int kind, const double* A, const double* r, double* z) {
   int n = m->nv;
   if (kind == 0) {
+#pragma omp parallel for schedule(static) num_threads(m->threads)
     for (int i = 0; i < n; ++i) z[i] = r[i] / A[m->diag[i]];
     return;
   }
+  /* symmetric Gauss-Seidel: sequential by construction, as deal.II's
+   * PreconditionSSOR */
   for (int i = 0; i < n; ++i) {
     double s = r[i];
     for (int k = m->rp[i]; k < m->diag[i]; ++k) s -= A[k] * z[m->ci[k]];
@@ -1081,23 +1129,26 @@ static int solve_cg(const omodel* m, const double* A, double* x, const double* b
   int n = m->nv;
   double *r = xcalloc(n, 8), *z = xcalloc(n, 8), *p = xcalloc(n, 8), *q = xcalloc(n, 8);
   spmv(m, A, x, q);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
   for (int i = 0; i < n; ++i) r[i] = b[i] - q[i];
-  double res = sqrt(dot(n, r, r));
+  double res = sqrt(dot_m(m, n, r, r));
   int it = 0;
   if (res > tol) {
     precond(m, pk, A, r, z);
     memcpy(p, z, sizeof(double) * n);
-    double rho = dot(n, r, z);
+    double rho = dot_m(m, n, r, z);
     for (it = 1; it <= maxit; ++it) {
       spmv(m, A, p, q);
-      double alpha = rho / dot(n, p, q);
+      double alpha = rho / dot_m(m, n, p, q);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
       for (int i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
-      res = sqrt(dot(n, r, r));
+      res = sqrt(dot_m(m, n, r, r));
       if (res <= tol) break;
       precond(m, pk, A, r, z);
-      double rn = dot(n, r, z);
+      double rn = dot_m(m, n, r, z);
       double beta = rn / rho;
       rho = rn;
+#pragma omp parallel for schedule(static) num_threads(m->threads)
       for (int i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     }
     if (it > maxit) it = maxit;
@@ -1112,35 +1163,40 @@ static int solve_bicgstab(const omodel* m, const double* A, double* x, const dou
   double *r = xcalloc(n, 8), *rb = xcalloc(n, 8), *p = xcalloc(n, 8), *v = xcalloc(n, 8);
   double *y = xcalloc(n, 8), *z = xcalloc(n, 8), *t = xcalloc(n, 8);
   spmv(m, A, x, v);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
   for (int i = 0; i < n; ++i) r[i] = b[i] - v[i];
   memset(v, 0, sizeof(double) * n);
-  double res = sqrt(dot(n, r, r));
+  double res = sqrt(dot_m(m, n, r, r));
   int it = 0;
   if (res > tol) {
     memcpy(rb, r, sizeof(double) * n);
     double alpha = 1.0, rho = 1.0, omega = 1.0;
     for (it = 1; it <= maxit; ++it) {
-      double rhobar = dot(n, r, rb);
+      double rhobar = dot_m(m, n, r, rb);
       double beta = rhobar * alpha / (rho * omega);
       rho = rhobar;
+#pragma omp parallel for schedule(static) num_threads(m->threads)
       for (int i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
       precond(m, pk, A, p, y);
       spmv(m, A, y, v);
-      alpha = rho / dot(n, rb, v);
+      alpha = rho / dot_m(m, n, rb, v);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
       for (int i = 0; i < n; ++i) r[i] -= alpha * v[i];
-      res = sqrt(dot(n, r, r));
+      res = sqrt(dot_m(m, n, r, r));
       if (res <= tol) {
+#pragma omp parallel for schedule(static) num_threads(m->threads)
         for (int i = 0; i < n; ++i) x[i] += alpha * y[i];
         break;
       }
       precond(m, pk, A, r, z);
       spmv(m, A, z, t);
-      omega = dot(n, t, r) / dot(n, t, t);
+      omega = dot_m(m, n, t, r) / dot_m(m, n, t, t);
+#pragma omp parallel for schedule(static) num_threads(m->threads)
       for (int i = 0; i < n; ++i) {
         x[i] += alpha * y[i] + omega * z[i];
         r[i] -= omega * t[i];
       }
-      res = sqrt(dot(n, r, r));
+      res = sqrt(dot_m(m, n, r, r));
       if (res <= tol) break;
     }
     if (it > maxit) it = maxit;
@@ -1156,7 +1212,7 @@ static int solve(omodel* m, int slot, const double* A, double* x, const double* 
                  double rtol) {
   double res = 0.0;
   if (rtol > 0.0) {
-    const double bn = sqrt(dot(m->nv, b, b));
+    const double bn = sqrt(dot_m(m, m->nv, b, b));
     if (rtol * bn > tol) tol = rtol * bn;
   }
   int it = kind == PFEM2_SOLVER_CG ? solve_cg(m, A, x, b, pk, tol, m->cs.max_iter, &res)
