@@ -176,7 +176,7 @@ typedef struct {
   int32_t dim;                     /* 2 or 3 */
   int32_t precision;               /* pfem2_precision */
   int32_t device;                  /* CUDA ordinal */
-  int32_t movement_steps;          /* PARTICLES_MOVEMENT_STEPS (pfem2particle.h:4) */
+  int32_t movement_steps;          /* PARTICLES_MOVEMENT_STEPS (pfem2particle.h:4), 1 .. 65535 */
   int32_t max_particles_per_cell_part; /* MAX_PARTICLES_PER_CELL_PART (pfem2particle.h:5) */
   int32_t particles_per_cell_max;  /* per-cell capacity of the rebin pass (0 = auto) */
   double particle_capacity_factor; /* particle storage = factor * seeded count (0 = 2.0) */

@@ -728,6 +728,10 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
     set_error("movement_steps and max_particles_per_cell_part must be >= 1");
     return PFEM2_INVALID_ARG;
   }
+  if (cfg->movement_steps > 65535) {
+    set_error("movement_steps must be <= 65535");
+    return PFEM2_INVALID_ARG;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("no CUDA device");

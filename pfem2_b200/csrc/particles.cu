@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(kAdvThreads, AdvectMinBlocks<DIM, R>::value) k
   constexpr int QN = 64;  // below 32 left over + 32 appended
   __shared__ int q_p[NW][QN], q_c[NW][QN];
   __shared__ R q_x[NW][DIM][QN];
-  __shared__ unsigned char q_s[NW][QN];
+  __shared__ unsigned short q_s[NW][QN];  // sub-step index (movement_steps <= 65535)
   const int n = min(*d_np, (int)cap);
   const int chunk = (n + gridDim.x - 1) / gridDim.x;
   const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(kAdvThreads, AdvectMinBlocks<DIM, R>::value) k
         const int k = nq + __popc(m & lanemask_lt());
         q_p[warp][k] = p;
         q_c[warp][k] = c0;
-        q_s[warp][k] = (unsigned char)s_left;
+        q_s[warp][k] = (unsigned short)s_left;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) q_x[warp][d][k] = x[d];
       }

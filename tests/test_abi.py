@@ -182,3 +182,15 @@ def test_tuner_searches_coupled_knobs_together(monkeypatch):
     assert res["tuning"]["advect_blocks_per_sm"] == 16 and res["tuning"]["advect_split"] == 2
     assert res["tuning"]["rebin_blocks_per_sm"] == 4
     assert (16, 2, 8) in tried  # the coupled corner one knob at a time would not reach
+
+
+@pytest.mark.parametrize("steps", [0, 65536])
+def test_movement_steps_range_checked_before_device(steps):
+    """movement_steps outside 1 .. 65535 is refused at pfem2_create, before
+    the device is looked at (the advection queues store the sub-step index
+    in 16 bits)"""
+    from pfem2_b200 import cases
+    sp = cases.poiseuille_2d(nx=4, ny=2)
+    with pytest.raises(solver.Pfem2Error) as e:
+        solver.Solver(sp, movement_steps=steps)
+    assert e.value.status == A.INVALID_ARG
