@@ -767,6 +767,7 @@ pfem2_status pfem2_create(const pfem2_config* cfg, pfem2_ctx** out) {
   c.moving = cfg->moving_mesh != 0;
   if (const char* v = getenv("PFEM2_ADVECT_SPLIT_MIN")) c.adv_split_min = atoll(v);
   if (const char* v = getenv("PFEM2_MG_WIDE_MIN")) c.mg_wide_min = atoll(v);
+  if (const char* v = getenv("PFEM2_MG_SPLIT_MIN")) c.mg_split_min = atoll(v);
   if (const char* v = getenv("PFEM2_SPIN_LIMIT")) c.spin_limit = (unsigned)std::min(atoll(v), (long long)c.spin_limit);
   PFEM2_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   for (int k = 0; k < 8; ++k) PFEM2_CUDA(cudaEventCreate(&c.ev[k]));

@@ -176,6 +176,14 @@ struct Ctx {
   int solve_threads = 256;
   int solve_blocks_per_sm = 1;  // persistent Krylov grid: blocks per SM
   long long mg_wide_min = 262144;  // rows from which one pressure system runs two blocks per SM
+  // rows of the largest pressure system from which the restriction to
+  // level 2 is a phase of its own (b2 = Pt1^T b1 after b1 is complete)
+  // instead of the composite R02 in phase B: from every size, since the
+  // composite's rows reach far beyond a block's own rows (on the 52k-row
+  // channel 1,981 other rows per block against 381 own) and the extra phase
+  // costs less (channel pressure solve 1.29 -> 1.15 ms, 64-instance batch
+  // 27.0 -> 21.5 ms); PFEM2_MG_SPLIT_MIN overrides it at creation
+  long long mg_split_min = 0;
   bool two_level = true;        // pressure: multigrid preconditioner (else Jacobi)
   bool vel_bicg = false;        // velocity systems solved by BiCGStab (else CG)
   bool p_bicg = false;          // pressure solved by BiCGStab with Jacobi (else CG with multigrid)

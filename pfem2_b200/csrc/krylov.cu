@@ -24,11 +24,14 @@
 //   A  p' = z + beta p ; q = A p'                 (p double buffered) | (p', q)
 //   B  e += alpha p' ; r -= alpha q ; z = D^-1 r                     | (r, z), (r, r)
 // The pressure systems are preconditioned with one multigrid V(1,1) cycle
-// in additive form (amg.h) and take three:
+// in additive form (amg.h) and take four:
 //   B   e += alpha p' ; r' = r - alpha q (r double buffered) ;
-//       b_l = R0l r' on the block's own level-l rows, l = 1, 2, with r'
-//       formed on the fly from r and q                              | (r', r')
-//       and the own level-2 rows' contributions to b3 = Pt2^T b2
+//       b1 = R01 r' on the block's own level-1 rows, with r' formed on
+//       the fly from r and q                                        | (r', r')
+//   B2  b2 = Pt1^T b1 on the own level-2 rows (b1 of the whole system)
+//       and their contributions to b3 = Pt2^T b2
+//       (below mg_split_min rows, b2 = R02 r' with the composite R02 in
+//       phase B instead, and no B2)
 //   UZ  first every global read: b2 of the block's systems, b3 (summing
 //       the blocks' contributions), J1 b1 on its level-1 list, J0 r on
 //       its own rows; then in shared memory J2 b2, x3 = E^-1 b3,
@@ -1589,7 +1592,7 @@ pfem2_status krylov_setup_precond(Ctx& c) {
   // synchronisation costs (3D pipe: 52M entries against Pt1's few million)
   long long nvmax = 0;
   for (const HostInst& in : c.inst) nvmax = std::max<long long>(nvmax, in.nv);
-  w->split = nvmax >= c.mg_wide_min;
+  w->split = nvmax >= c.mg_split_min;
   // the dense level-3 inverse rows of a block (up to coarse_max^2 floats)
   // must leave room in the two-blocks-per-SM shared-memory budget
   const int coarse_max = w->mg_minb == 1 ? 160 : 128;

@@ -52,9 +52,19 @@ def test_library_matches_golden(name, prec):
 @pytest.mark.parametrize("name", CASES)
 def test_library_matches_golden_wide_multigrid(name, prec, monkeypatch):
     """the pressure multigrid of one large system (from PFEM2_MG_WIDE_MIN rows
-    on: two blocks per SM, a tile per block, the restriction to level 2 in a
-    phase of its own), forced on the small cases"""
+    on: two blocks per SM, a tile per block), forced on the small cases"""
     monkeypatch.setenv("PFEM2_MG_WIDE_MIN", "0")
+    _check_library(name, prec)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", MODES)
+@pytest.mark.parametrize("name", CASES)
+def test_library_matches_golden_composite_restriction(name, prec, monkeypatch):
+    """the restriction to level 2 through the composite R02 inside phase B
+    (the form below PFEM2_MG_SPLIT_MIN rows; by default every system uses the
+    separate phase b2 = Pt1^T b1)"""
+    monkeypatch.setenv("PFEM2_MG_SPLIT_MIN", str(1 << 40))
     _check_library(name, prec)
 
 
