@@ -371,7 +371,7 @@ def run_ours(args, rank, world, local):
 # launches. Under ncu every launch starts with a flushed L2, so this is one
 # cold read of the solve's working set, which then stays in L2: it does
 # not grow with the iteration count.
-KRYLOV_TRAFFIC_PER_LAUNCH = 0.5 * ((33012736 + 103168) + (33008128 + 21760))
+KRYLOV_TRAFFIC_PER_LAUNCH = 0.5 * ((27532032 + 54272) + (27526400 + 10240))
 KRYLOV_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_krylov<float, MG> launches "
                          "of steps 5-6 (31 and 30 iterations) of `bench.py --only channel --steps 3 --warmup 4`; "
                          "per launch = per step")
